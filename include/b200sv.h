@@ -1,0 +1,274 @@
+/*
+ * b200sv.h — C ABI of the B200 state-vector engine (libb200sv.so).
+ *
+ * This is the drop-in boundary for the hot path of lightning.qubit: state-vector
+ * gate application, measurements and adjoint differentiation.  Every entry point
+ * is `extern "C"`, takes plain pointers and sizes, returns an int status
+ * (B200SV_OK == 0) and leaves a thread-local message for b200sv_last_error().
+ *
+ * Conventions kept from the reference (paths relative to the reference project,
+ * pennylane_lightning/core/src = CS/, CS/simulators/lightning_qubit = LQ/):
+ *   - wire 0 is the most significant bit of the basis index
+ *     (rev_wire = n - 1 - wire, LQ/gates/cpu_kernels/GateImplementationsLM.hpp:210);
+ *   - matrices are row-major complex<T>, wires[0] is the most significant bit of
+ *     the matrix index; `inverse` means conjugate transpose
+ *     (GateImplementationsLM.hpp:204-387);
+ *   - gate and generator ids are the enum values of CS/gates/GateOperation.hpp:27-111;
+ *   - Jacobians are laid out [observable][trainable parameter]
+ *     (LQ/algorithms/AdjointJacobianLQubit.hpp:331-334).
+ *
+ * All device work of a handle runs on that handle's CUDA stream and is ordered
+ * there; calls that return host data synchronise that stream.  No call falls back
+ * to the CPU: when no CUDA device is usable, b200sv_create fails.
+ */
+#ifndef B200SV_H
+#define B200SV_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+enum b200sv_status {
+    B200SV_OK = 0,
+    B200SV_ERR_ARGUMENT = 1,    /* bad wires, sizes, ids, parameter counts   */
+    B200SV_ERR_CUDA = 2,        /* a CUDA runtime call failed                */
+    B200SV_ERR_ALLOC = 3,       /* device or pinned allocation failed        */
+    B200SV_ERR_UNSUPPORTED = 4, /* valid request this build does not handle  */
+    B200SV_ERR_TIMEOUT = 5,     /* a bounded device wait ran out             */
+    B200SV_ERR_CANCELLED = 6    /* a batch was cancelled before completion   */
+};
+
+/* ---- precisions -------------------------------------------------------- */
+enum b200sv_dtype {
+    B200SV_C64 = 0,  /* complex<float>  amplitudes, FP64 reductions          */
+    B200SV_C128 = 1  /* complex<double> amplitudes                           */
+};
+
+/* ---- gate ids: CS/gates/GateOperation.hpp:27-70 (same numeric values) --- */
+enum b200sv_gate {
+    B200SV_Identity = 0, B200SV_PauliX, B200SV_PauliY, B200SV_PauliZ,
+    B200SV_Hadamard, B200SV_S, B200SV_T, B200SV_PhaseShift, B200SV_RX,
+    B200SV_RY, B200SV_RZ, B200SV_Rot,
+    B200SV_CNOT, B200SV_CY, B200SV_CZ, B200SV_SWAP, B200SV_IsingXX,
+    B200SV_IsingXY, B200SV_IsingYY, B200SV_IsingZZ,
+    B200SV_ControlledPhaseShift, B200SV_CRX, B200SV_CRY, B200SV_CRZ,
+    B200SV_CRot, B200SV_SingleExcitation, B200SV_SingleExcitationMinus,
+    B200SV_SingleExcitationPlus,
+    B200SV_Toffoli, B200SV_CSWAP,
+    B200SV_DoubleExcitation, B200SV_DoubleExcitationMinus,
+    B200SV_DoubleExcitationPlus,
+    B200SV_MultiRZ,
+    B200SV_GATE_END,
+    /* ids outside the reference enum used in operation lists */
+    B200SV_OP_MATRIX = 1000, /* dense matrix given in b200sv_op.matrix       */
+    B200SV_OP_SKIP = 1001    /* state-preparation ops the adjoint ignores
+                                ("QubitStateVector", "BasisState":
+                                AdjointJacobianLQubit.hpp:287-290)          */
+};
+
+/* ---- generator ids: CS/gates/GateOperation.hpp:75-98 -------------------- */
+enum b200sv_generator {
+    B200SV_GEN_PhaseShift = 0, B200SV_GEN_RX, B200SV_GEN_RY, B200SV_GEN_RZ,
+    B200SV_GEN_IsingXX, B200SV_GEN_IsingXY, B200SV_GEN_IsingYY,
+    B200SV_GEN_IsingZZ, B200SV_GEN_CRX, B200SV_GEN_CRY, B200SV_GEN_CRZ,
+    B200SV_GEN_ControlledPhaseShift, B200SV_GEN_SingleExcitation,
+    B200SV_GEN_SingleExcitationMinus, B200SV_GEN_SingleExcitationPlus,
+    B200SV_GEN_DoubleExcitation, B200SV_GEN_DoubleExcitationMinus,
+    B200SV_GEN_DoubleExcitationPlus, B200SV_GEN_MultiRZ,
+    B200SV_GEN_END
+};
+
+typedef struct b200sv_state *b200sv_handle;
+
+/* One operation of a gate list (CS/algorithms/JacobianData.hpp:40-197 OpsData:
+ * name, params, wires, inverse, matrix).  `matrix` is complex<T> row-major of
+ * size 4^nwires, read only when gate == B200SV_OP_MATRIX. */
+typedef struct b200sv_op {
+    uint32_t gate;
+    uint32_t nwires;
+    const uint32_t *wires;
+    int32_t inverse;
+    uint32_t nparams;
+    const double *params;
+    const void *matrix;
+} b200sv_op;
+
+/* One factor of an observable term: a named operator (a gate id applied as an
+ * operator, e.g. PauliX/Y/Z, Hadamard, Identity — CS/observables/Observables.hpp:101-143)
+ * or a Hermitian matrix (Observables.hpp:151-198). */
+enum b200sv_factor_kind { B200SV_FACTOR_NAMED = 0, B200SV_FACTOR_MATRIX = 1 };
+typedef struct b200sv_factor {
+    uint32_t kind;
+    uint32_t gate;          /* for B200SV_FACTOR_NAMED                       */
+    uint32_t nwires;
+    const uint32_t *wires;
+    const void *matrix;     /* for B200SV_FACTOR_MATRIX: complex<T>[4^nwires] */
+} b200sv_factor;
+
+/* A term: coeff * (tensor product of factors on disjoint wires). */
+typedef struct b200sv_term {
+    double coeff;
+    uint32_t nfactors;
+    const b200sv_factor *factors;
+} b200sv_term;
+
+/* An observable: NamedObs / HermitianObs / TensorProdObs are one term with
+ * coeff 1; a Hamiltonian is a list of terms (Observables.hpp:325-416). */
+typedef struct b200sv_observable {
+    uint32_t nterms;
+    const b200sv_term *terms;
+} b200sv_observable;
+
+/* ---- library ----------------------------------------------------------- */
+/* Last error message of the calling thread ("" when none). */
+const char *b200sv_last_error(void);
+/* ABI version (major*10000 + minor*100 + patch). */
+int b200sv_version(void);
+/* Number of CUDA devices usable by the library (0 when none). */
+int b200sv_device_count(int *count);
+
+/* ---- state lifecycle: LQ/StateVectorLQubitManaged.hpp:72-129 ------------ */
+/* Allocate 2^num_qubits amplitudes on the current device, set to |0...0>. */
+int b200sv_create(uint32_t num_qubits, int dtype, b200sv_handle *out);
+int b200sv_destroy(b200sv_handle h);
+int b200sv_num_qubits(b200sv_handle h, uint32_t *out);
+int b200sv_dtype(b200sv_handle h, int *out);
+/* Run the handle's work on an external stream (e.g. torch's current stream);
+ * pass NULL to return to the handle's own stream. */
+int b200sv_set_stream(b200sv_handle h, void *cuda_stream);
+int b200sv_synchronize(b200sv_handle h);
+/* Device address of the amplitudes (complex<T>[2^n]) for zero-copy interop. */
+int b200sv_device_ptr(b200sv_handle h, void **out);
+/* Copy 2^n complex<T> host amplitudes in / out (updateData, getData). */
+int b200sv_upload(b200sv_handle h, const void *host, uint64_t length);
+int b200sv_download(b200sv_handle h, void *host, uint64_t length);
+/* dst <- src (same size and dtype): the copy constructor. */
+int b200sv_copy(b200sv_handle dst, b200sv_handle src);
+/* |index> (index 0 = |0...0>): setBasisState. */
+int b200sv_set_basis_state(b200sv_handle h, uint64_t index);
+
+/* ---- gates: CS/simulators/base/StateVectorBase.hpp:99-194 ---------------- */
+/* applyOperation(name, wires, inverse, params) with the name resolved to an id
+ * (LQ/StateVectorLQubit.hpp:231-240).  Parameter counts follow
+ * CS/gates/Constant.hpp:234-269; wire counts Constant.hpp:163-197 (MultiRZ: any). */
+int b200sv_apply_gate(b200sv_handle h, uint32_t gate, const uint32_t *wires,
+                      uint32_t nwires, int inverse, const double *params,
+                      uint32_t nparams);
+/* applyMatrix (LQ/StateVectorLQubit.hpp:329-365): complex<T> row-major 4^nwires. */
+int b200sv_apply_matrix(b200sv_handle h, const void *matrix,
+                        const uint32_t *wires, uint32_t nwires, int inverse);
+/* applyOperations: a list applied in order on the handle's stream. */
+int b200sv_apply_ops(b200sv_handle h, const b200sv_op *ops, uint32_t nops);
+/* applyGenerator (LQ/StateVectorLQubit.hpp:250-275): G applied in place (it is
+ * not unitary for projector-type generators); *scale receives the factor of
+ * GateImplementationsLM.hpp:1355-1639 / PauliGenerator.hpp:34-56. */
+int b200sv_apply_generator(b200sv_handle h, uint32_t generator,
+                           const uint32_t *wires, uint32_t nwires, int adj,
+                           double *scale);
+
+/* ---- measurements: LQ/measurements/MeasurementsLQubit.hpp:79-558 --------- */
+/* probs() (nwires == 0 means all wires in order 0..n-1) and probs(wires):
+ * out receives 2^nwires FP64 values, wires[0] the most significant bit. */
+int b200sv_probs(b200sv_handle h, const uint32_t *wires, uint32_t nwires,
+                 double *out);
+/* Device-side variant: writes 2^nwires doubles to a device buffer. */
+int b200sv_probs_device(b200sv_handle h, const uint32_t *wires,
+                        uint32_t nwires, double *out_device);
+/* <psi|O|psi> for an observable (expval(Observable), :248-265). */
+int b200sv_expval(b200sv_handle h, const b200sv_observable *obs, double *out);
+/* <O^2> - <O>^2 as ||O psi||^2 - <psi|O psi>^2 (var(Observable), :273-372). */
+int b200sv_var(b200sv_handle h, const b200sv_observable *obs, double *out);
+/* Pauli-word sums evaluated as read-only fused reductions.  Term t acts with
+ * paulis[off[t]..off[t+1]) ('I','X','Y','Z') on wires[off[t]..off[t+1]).
+ * out_terms (nterms doubles, may be NULL) receives each <P_t>; out_sum (may
+ * be NULL) receives sum_t coeffs[t] <P_t>. */
+int b200sv_expval_pauli(b200sv_handle h, uint32_t nterms, const double *coeffs,
+                        const uint32_t *offsets, const uint32_t *wires,
+                        const char *paulis, double *out_terms, double *out_sum);
+/* Re/Im of <bra|ket> in FP64 (innerProdC, LQ/utils/LinearAlgebra.hpp:190-213). */
+int b200sv_inner_product(b200sv_handle bra, b200sv_handle ket, double *re,
+                         double *im);
+/* ||psi||^2 in FP64. */
+int b200sv_norm2(b200sv_handle h, double *out);
+
+/* Sampling by inverse CDF (the lightning.kokkos rule,
+ * LK/measurements/MeasuresFunctors.hpp:70-103 over an exclusive scan,
+ * LK/measurements/MeasurementsKokkos.hpp:713-722).  p_i = re*re + im*im in FP64
+ * without contraction; the scan order is fixed (see DESIGN), so the indices
+ * are a deterministic function of the state and the uniforms.
+ * uniforms: nshots doubles in [0,1) on the host, or NULL to draw them on the
+ * device from Philox4x32-10 with `seed`.  idx_out: nshots basis indices. */
+int b200sv_sample(b200sv_handle h, uint64_t nshots, const double *uniforms,
+                  uint64_t seed, uint64_t *idx_out);
+/* generate_samples layout: nshots x n bits, MSB (wire 0) first, as uint64. */
+int b200sv_sample_bits(b200sv_handle h, uint64_t nshots, const double *uniforms,
+                       uint64_t seed, uint64_t *bits_out);
+
+/* ---- adjoint Jacobian: LQ/algorithms/AdjointJacobianLQubit.hpp:212-335 ---- */
+/* jac (nobs x ntp doubles, [obs][param]) for the state in `psi` (unchanged).
+ * With apply_operations != 0 the ops are applied to a copy of psi first.
+ * trainable holds sorted indices into the list of parametric operations. */
+int b200sv_adjoint_jacobian(b200sv_handle psi, const b200sv_op *ops,
+                            uint32_t nops, const b200sv_observable *obs,
+                            uint32_t nobs, const uint64_t *trainable,
+                            uint32_t ntrainable, int apply_operations,
+                            double *jac);
+
+/* ---- batched engine ------------------------------------------------------ */
+/* A batch is a packed pool of independent circuits of uneven width, run by one
+ * persistent kernel per step (optionally replayed as a CUDA graph).  Each circuit
+ * is an op list over its own wires 0..n_c-1 starting from |0...0>, followed by
+ * an observable given as a Pauli-word sum.  Parameters live in one device array
+ * so steps can change angles without rebuilding the batch. */
+typedef struct b200sv_batch *b200sv_batch_handle;
+
+typedef struct b200sv_batch_circuit {
+    uint32_t num_qubits;
+    uint32_t nops;
+    const b200sv_op *ops;           /* params of ops index param_index below */
+    const int64_t *param_index;     /* per op: first slot in the batch param
+                                       array (-1: op.params used as constants) */
+    uint32_t nobs;                  /* Pauli-word observables (outputs)        */
+    const uint32_t *obs_nterms;     /* per observable: number of terms        */
+    const double *obs_coeffs;       /* all terms, observable-major             */
+    const uint32_t *obs_offsets;    /* per term: offsets into wires/paulis     */
+    const uint32_t *obs_wires;
+    const char *obs_paulis;
+} b200sv_batch_circuit;
+
+int b200sv_batch_create(int dtype, const b200sv_batch_circuit *circuits,
+                        uint32_t ncircuits, uint64_t nparams,
+                        b200sv_batch_handle *out);
+int b200sv_batch_destroy(b200sv_batch_handle b);
+int b200sv_batch_set_stream(b200sv_batch_handle b, void *cuda_stream);
+/* Forward: params_device (nparams doubles on the device) -> out_device
+ * (sum over circuits of nobs doubles, circuit-major). */
+int b200sv_batch_forward(b200sv_batch_handle b, const double *params_device,
+                         double *out_device);
+/* Adjoint VJP: given dy_device (same layout as the forward outputs), writes
+ * grad_device[p] = sum_c sum_o dy[c,o] d<O_{c,o}>/d param[p] (nparams doubles;
+ * parameters not referenced by any circuit receive 0). */
+int b200sv_batch_vjp(b200sv_batch_handle b, const double *params_device,
+                     const double *dy_device, double *grad_device);
+/* Full Jacobian per circuit: jac_device[c] block of nobs_c x nparams_c
+ * (the circuit's own referenced params in op order), circuit-major. */
+int b200sv_batch_jacobian(b200sv_batch_handle b, const double *params_device,
+                          double *jac_device);
+/* Record the forward / vjp of this batch as CUDA graphs on first use and
+ * replay them afterwards (0 = launch directly). */
+int b200sv_batch_use_graphs(b200sv_batch_handle b, int enable);
+/* Cost model / autotuner: times candidate launch shapes on the batch once and
+ * keeps the fastest; *chosen receives the chosen configuration id. */
+int b200sv_batch_autotune(b200sv_batch_handle b, const double *params_device,
+                          int *chosen);
+/* Number of kernels the last forward / vjp call launched. */
+int b200sv_batch_last_launches(b200sv_batch_handle b, uint32_t *out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* B200SV_H */

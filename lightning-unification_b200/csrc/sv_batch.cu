@@ -1,0 +1,1300 @@
+// sv_batch.cu — batched engine: thousands of independent circuits of uneven width
+// in one persistent launch.
+//
+// Each CTA pulls circuits from an atomic work queue (longest first).  A circuit
+// whose state fits in shared memory (2^n <= 2^kt amplitudes per live state) runs
+// entirely on chip: |0...0> is created in shared memory, every gate is applied
+// there and only the expectation values (or gradients) leave the SM.  Wider
+// circuits run as a host-planned list of segments: each segment is a run of
+// gates whose wires fit in kt local bits, executed as one HBM/L2 pass over the
+// 2^(n-kt) tiles of the state, every tile staged in shared memory.
+//
+// Differentiation is the adjoint method of LQ/algorithms/AdjointJacobianLQubit.hpp:212-335
+// restricted to the vector-Jacobian product (one bra = sum_o dy_o O_o psi, the
+// trick of lightning_qubit.py:747-772): per circuit two live states (lambda and
+// the bra), a reverse sweep applying U^dagger to both and, for each differentiated
+// gate, the FP64 product -2 * scale * Im<bra|G|lambda> accumulated per warp and
+// reduced in a fixed order by a second kernel.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "../../include/b200sv.h"
+#include "sv_device.cuh"
+#include "sv_internal.hpp"
+
+namespace b200sv {
+namespace batch {
+
+enum Form : uint8_t { F_MAT1 = 1, F_MAT2 = 2, F_DIAG = 3, F_SWAP = 4, F_PARITY = 5, F_NOOP = 6 };
+enum GForm : uint8_t { G_NONE = 0, G_MAT = 1, G_PARITY = 2 };
+constexpr uint8_t kConstGate = 255;
+constexpr int kMaxKt = 14;
+constexpr int kMaxObsPerCircuit = 16;
+
+// One gate with bit positions local to its segment's tile.
+struct DOp {
+    uint8_t form, gate, nb, inv;
+    uint8_t nt, gform, gnb, gk;
+    uint16_t low[4];     // insertion masks of the gate bits (ascending)
+    uint16_t glow[2];    // insertion masks of the generator bits
+    uint32_t cmask;      // control bits (must be set)
+    uint32_t off[4];     // row offsets of the targets (row r: bit (nt-1-j) <-> target j)
+    uint32_t goff[4];    // generator row offsets
+    uint32_t pmask;      // parity bits (MultiRZ)
+    int32_t pslot;       // parameter slot, -1 for constant gates
+    int32_t gslot;       // gradient slot, -1 when not differentiated
+    uint32_t cidx;       // constant coefficients (consts[cidx*16..])
+    uint32_t gcidx;      // generator matrix (consts[gcidx*16..])
+    double gscale;       // -2 * generator scale * (inverse ? -1 : 1)
+};
+
+struct DSeg {
+    uint32_t op_begin, nops;
+    uint8_t lbits[kMaxKt];   // tile bit j -> state bit
+    uint8_t gbits[40];       // tile index bit j -> state bit
+    uint8_t nl, ng;
+};
+
+struct DCirc {
+    uint32_t n, kt, resident;
+    uint32_t seg_begin, nseg;
+    uint64_t off_a, off_b;   // offsets into the state pools (amplitudes)
+    uint32_t term_begin, nterms;
+    uint32_t nobs, out_begin;
+};
+
+struct DTerm {
+    uint32_t obs;
+    int32_t ny;
+    double coeff;
+    uint64_t xmask, zmask;
+};
+
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t ins_local(uint32_t g, const uint16_t *low, int nb) {
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        if (j < nb) {
+            const uint32_t lo = g & low[j];
+            g = ((g ^ lo) << 1) | lo;
+        }
+    }
+    return g;
+}
+
+template <typename R>
+__device__ void op_coeffs(const DOp &op, const double *__restrict__ params, const double2 *__restrict__ consts,
+                          bool adj, C<R> *m) {
+    if (op.gate == kConstGate) {
+        const double2 *c = consts + (size_t)op.cidx * 16;
+        if (op.form == F_MAT1 || op.form == F_MAT2) {
+            const int D = op.form == F_MAT1 ? 2 : 4;
+            for (int r = 0; r < D; ++r)
+                for (int q = 0; q < D; ++q) {
+                    const double2 z = adj ? c[q * D + r] : c[r * D + q];
+                    m[r * D + q] = mk<R>((R)z.x, (R)(adj ? -z.y : z.y));
+                }
+        } else {
+            for (int r = 0; r < 4; ++r) m[r] = mk<R>((R)c[r].x, (R)(adj ? -c[r].y : c[r].y));
+        }
+        return;
+    }
+    const double th = params[op.pslot];
+    const double sg = ((op.inv != 0) != adj) ? -1.0 : 1.0;
+    double s, c;
+    sincos(0.5 * th, &s, &c);
+    s *= sg;
+    const R cr = (R)c, sr = (R)s, z = (R)0, one = (R)1;
+    switch (op.gate) {
+    case B200SV_RX: case B200SV_CRX:
+        m[0] = mk<R>(cr, z); m[1] = mk<R>(z, -sr); m[2] = mk<R>(z, -sr); m[3] = mk<R>(cr, z); break;
+    case B200SV_RY: case B200SV_CRY:
+        m[0] = mk<R>(cr, z); m[1] = mk<R>(-sr, z); m[2] = mk<R>(sr, z); m[3] = mk<R>(cr, z); break;
+    case B200SV_RZ: case B200SV_CRZ: case B200SV_MultiRZ:
+        m[0] = mk<R>(cr, -sr); m[1] = mk<R>(cr, sr); break;
+    case B200SV_PhaseShift: case B200SV_ControlledPhaseShift: {
+        double s2, c2;
+        sincos(th, &s2, &c2);
+        m[0] = mk<R>((R)c2, (R)(sg * s2));
+        break;
+    }
+    case B200SV_IsingZZ:
+        m[0] = mk<R>(cr, -sr); m[1] = mk<R>(cr, sr); m[2] = mk<R>(cr, sr); m[3] = mk<R>(cr, -sr); break;
+    default: {
+        for (int i = 0; i < 16; ++i) m[i] = mk<R>(z, z);
+        if (op.gate == B200SV_IsingXX) {
+            m[0] = m[5] = m[10] = m[15] = mk<R>(cr, z);
+            m[3] = m[6] = m[9] = m[12] = mk<R>(z, -sr);
+        } else if (op.gate == B200SV_IsingYY) {
+            m[0] = m[5] = m[10] = m[15] = mk<R>(cr, z);
+            m[3] = m[12] = mk<R>(z, sr);
+            m[6] = m[9] = mk<R>(z, -sr);
+        } else if (op.gate == B200SV_IsingXY) {
+            m[0] = m[15] = mk<R>(one, z);
+            m[5] = m[10] = mk<R>(cr, z);
+            m[6] = m[9] = mk<R>(z, sr);
+        } else {  // SingleExcitation (+/-)
+            m[5] = m[10] = mk<R>(cr, z);
+            m[6] = mk<R>(-sr, z);
+            m[9] = mk<R>(sr, z);
+            C<R> e = mk<R>(one, z);
+            if (op.gate == B200SV_SingleExcitationMinus) e = mk<R>(cr, -sr);
+            if (op.gate == B200SV_SingleExcitationPlus) e = mk<R>(cr, sr);
+            m[0] = m[15] = e;
+        }
+    }
+    }
+}
+
+// apply one gate (or its adjoint, coefficients already conjugated) to NS tiles in shared memory
+template <typename R, int NS>
+__device__ __forceinline__ void apply_tile(C<R> *const (&s)[NS], int kt, const DOp &op, const C<R> *m) {
+    if (op.form == F_NOOP) return;
+    if (op.form == F_PARITY) {
+        const uint32_t n = 1u << kt;
+        for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+            const C<R> f = m[__popc(i & op.pmask) & 1];
+#pragma unroll
+            for (int q = 0; q < NS; ++q) {
+                CAcc<R> a;
+                a.add(f, s[q][i]);
+                s[q][i] = a.get();
+            }
+        }
+        return;
+    }
+    const uint32_t ng = 1u << (kt - op.nb);
+    for (uint32_t g = threadIdx.x; g < ng; g += blockDim.x) {
+        const uint32_t base = ins_local(g, op.low, op.nb) | op.cmask;
+#pragma unroll
+        for (int q = 0; q < NS; ++q) {
+            C<R> *t = s[q];
+            switch (op.form) {
+            case F_MAT1: {
+                const C<R> v0 = t[base + op.off[0]], v1 = t[base + op.off[1]];
+                CAcc<R> a, b;
+                a.add(m[0], v0); a.add(m[1], v1);
+                b.add(m[2], v0); b.add(m[3], v1);
+                t[base + op.off[0]] = a.get();
+                t[base + op.off[1]] = b.get();
+                break;
+            }
+            case F_MAT2: {
+                C<R> v[4];
+#pragma unroll
+                for (int r = 0; r < 4; ++r) v[r] = t[base + op.off[r]];
+#pragma unroll
+                for (int r = 0; r < 4; ++r) {
+                    CAcc<R> a;
+#pragma unroll
+                    for (int c = 0; c < 4; ++c) a.add(m[r * 4 + c], v[c]);
+                    t[base + op.off[r]] = a.get();
+                }
+                break;
+            }
+            case F_DIAG: {
+                const int rows = 1 << op.nt;
+                for (int r = 0; r < rows; ++r) {
+                    CAcc<R> a;
+                    a.add(m[r], t[base + op.off[r]]);
+                    t[base + op.off[r]] = a.get();
+                }
+                break;
+            }
+            case F_SWAP: {
+                const C<R> a = t[base + op.off[0]];
+                t[base + op.off[0]] = t[base + op.off[1]];
+                t[base + op.off[1]] = a;
+                break;
+            }
+            default: break;
+            }
+        }
+    }
+}
+
+// per-thread part of Im<bra|G|ket> on one tile, FP64
+template <typename R>
+__device__ __forceinline__ double gen_inner_tile(const C<R> *bra, const C<R> *ket, int kt, const DOp &op,
+                                                 const double2 *__restrict__ consts) {
+    double acc = 0.0;
+    if (op.gform == G_PARITY) {
+        const uint32_t n = 1u << kt;
+        for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+            const double2 k = widen<R>(ket[i]), b = widen<R>(bra[i]);
+            const double sg = (__popc(i & op.pmask) & 1) ? -1.0 : 1.0;
+            acc += sg * (b.x * k.y - b.y * k.x);
+        }
+        return acc;
+    }
+    const double2 *G = consts + (size_t)op.gcidx * 16;
+    const int D = 1 << op.gk;
+    const uint32_t ng = 1u << (kt - op.gnb);
+    for (uint32_t g = threadIdx.x; g < ng; g += blockDim.x) {
+        const uint32_t base = ins_local(g, op.glow, op.gnb);
+        double2 v[4];
+        for (int r = 0; r < D; ++r) v[r] = widen<R>(ket[base + op.goff[r]]);
+        for (int r = 0; r < D; ++r) {
+            double wr = 0, wi = 0;
+            for (int c = 0; c < D; ++c) {
+                const double2 x = G[r * D + c];
+                wr += x.x * v[c].x - x.y * v[c].y;
+                wi += x.x * v[c].y + x.y * v[c].x;
+            }
+            const double2 b = widen<R>(bra[base + op.goff[r]]);
+            acc += b.x * wi - b.y * wr;
+        }
+    }
+    return acc;
+}
+
+__device__ __forceinline__ uint64_t deposit(uint32_t v, const uint8_t *bits, int nb) {
+    uint64_t r = 0;
+    for (int j = 0; j < nb; ++j)
+        if (v & (1u << j)) r |= uint64_t(1) << bits[j];
+    return r;
+}
+__device__ __forceinline__ uint64_t deposit64(uint64_t v, const uint8_t *bits, int nb) {
+    uint64_t r = 0;
+    for (int j = 0; j < nb; ++j)
+        if (v & (uint64_t(1) << j)) r |= uint64_t(1) << bits[j];
+    return r;
+}
+
+// sum_t coeff_t <psi|P_t|psi> per observable into acc[obs] (per-thread part)
+template <typename R, bool GLOBAL>
+__device__ void expval_terms(const C<R> *psi, uint64_t n_amp, const DTerm *__restrict__ terms, uint32_t nterms,
+                             double (&acc)[kMaxObsPerCircuit]) {
+    for (uint32_t t = 0; t < nterms; ++t) {
+        const DTerm tm = terms[t];
+        double a = 0.0;
+        for (uint64_t i = threadIdx.x; i < n_amp; i += blockDim.x) {
+            // Re conj(psi_{i^X}) i^ny (-1)^{|i&Z|} psi_i
+            const double2 vi = widen<R>(psi[i]), vj = widen<R>(psi[i ^ tm.xmask]);
+            const double zr = vj.x * vi.x + vj.y * vi.y, zi = vj.x * vi.y - vj.y * vi.x;
+            double r;
+            switch (tm.ny & 3) {
+            case 0: r = zr; break;
+            case 1: r = -zi; break;
+            case 2: r = -zr; break;
+            default: r = zi; break;
+            }
+            a += (__popcll(i & tm.zmask) & 1) ? -r : r;
+        }
+        acc[tm.obs] += tm.coeff * a;
+    }
+}
+
+// bra_j = sum_t w_t (P_t psi)_j,  (P psi)_j = i^ny (-1)^{|(j^X)&Z|} psi_{j^X}
+template <typename R>
+__device__ void init_bra(C<R> *bra, const C<R> *psi, uint64_t n_amp, const DTerm *__restrict__ terms,
+                         uint32_t nterms, const double *__restrict__ dy) {
+    for (uint64_t j = threadIdx.x; j < n_amp; j += blockDim.x) {
+        double br = 0.0, bi = 0.0;
+        for (uint32_t t = 0; t < nterms; ++t) {
+            const DTerm tm = terms[t];
+            const double w = tm.coeff * dy[tm.obs];
+            if (w == 0.0) continue;
+            const uint64_t i = j ^ tm.xmask;
+            const double2 v = widen<R>(psi[i]);
+            double fr = (__popcll(i & tm.zmask) & 1) ? -w : w, fi = 0.0;
+            switch (tm.ny & 3) {
+            case 1: fi = fr; fr = 0; break;
+            case 2: fr = -fr; break;
+            case 3: fi = -fr; fr = 0; break;
+            default: break;
+            }
+            br += fr * v.x - fi * v.y;
+            bi += fr * v.y + fi * v.x;
+        }
+        bra[j] = mk<R>((R)br, (R)bi);
+    }
+}
+
+struct KArgs {
+    const DCirc *circs;
+    const DSeg *segs;
+    const DOp *ops;
+    const DTerm *terms;
+    const double2 *consts;
+    const uint32_t *order;
+    uint32_t ncirc;
+    uint32_t *counter;
+    const double *params;
+    const double *dy;     // [sum nobs] (VJP)
+    double *out;          // forward: [sum nobs]
+    double *gradw;        // VJP: [ngslots * nwarps]
+    void *pool_a, *pool_b;
+    int mode;             // 0 forward, 1 vjp
+    int max_kt;
+};
+
+template <typename R> __device__ __forceinline__ void zero_tile(C<R> *s, uint32_t n) {
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) s[i] = mk<R>(0, 0);
+}
+
+template <typename R>
+__device__ void load_tile(C<R> *dst, const C<R> *__restrict__ src, const DSeg &sg, uint64_t tbase, uint32_t nt) {
+    for (uint32_t l = threadIdx.x; l < nt; l += blockDim.x) dst[l] = src[tbase | deposit(l, sg.lbits, sg.nl)];
+}
+template <typename R>
+__device__ void store_tile(C<R> *__restrict__ dst, const C<R> *src, const DSeg &sg, uint64_t tbase, uint32_t nt) {
+    for (uint32_t l = threadIdx.x; l < nt; l += blockDim.x) dst[tbase | deposit(l, sg.lbits, sg.nl)] = src[l];
+}
+
+// one circuit, forward only: state ends in tile 0 (resident) or pool A (global)
+template <typename R>
+__device__ void run_forward(const KArgs &A, const DCirc &c, C<R> *sm, C<R> *pa) {
+    const uint32_t tn = 1u << c.kt;
+    C<R> *tiles[1] = {sm};
+    __shared__ C<R> coef[16];
+    if (c.resident) {
+        zero_tile<R>(sm, tn);
+        __syncthreads();
+        if (threadIdx.x == 0) sm[0] = mk<R>(1, 0);
+        __syncthreads();
+        const DSeg sg = A.segs[c.seg_begin];
+        for (uint32_t o = 0; o < sg.nops; ++o) {
+            const DOp op = A.ops[sg.op_begin + o];
+            if (threadIdx.x == 0) op_coeffs<R>(op, A.params, A.consts, false, coef);
+            __syncthreads();
+            apply_tile<R, 1>(tiles, c.kt, op, coef);
+            __syncthreads();
+        }
+        return;
+    }
+    const uint64_t ntiles = uint64_t(1) << (c.n - c.kt);
+    for (uint32_t si = 0; si < c.nseg; ++si) {
+        const DSeg sg = A.segs[c.seg_begin + si];
+        for (uint64_t t = 0; t < ntiles; ++t) {
+            const uint64_t tbase = deposit64(t, sg.gbits, sg.ng);
+            if (si == 0) {
+                zero_tile<R>(sm, tn);
+                __syncthreads();
+                if (threadIdx.x == 0 && tbase == 0) sm[0] = mk<R>(1, 0);
+            } else {
+                load_tile<R>(sm, pa, sg, tbase, tn);
+            }
+            __syncthreads();
+            for (uint32_t o = 0; o < sg.nops; ++o) {
+                const DOp op = A.ops[sg.op_begin + o];
+                if (threadIdx.x == 0) op_coeffs<R>(op, A.params, A.consts, false, coef);
+                __syncthreads();
+                apply_tile<R, 1>(tiles, c.kt, op, coef);
+                __syncthreads();
+            }
+            store_tile<R>(pa, sm, sg, tbase, tn);
+            __syncthreads();
+        }
+    }
+}
+
+template <typename R>
+__global__ void k_batch(KArgs A) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ uint32_t s_next;
+    __shared__ double s_red[kMaxObsPerCircuit * 32];
+    __shared__ C<R> coef[16];
+    C<R> *sm0 = reinterpret_cast<C<R> *>(smem_raw);
+    C<R> *sm1 = sm0 + (size_t(1) << A.max_kt);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    for (;;) {
+        if (threadIdx.x == 0) s_next = atomicAdd(A.counter, 1u);
+        __syncthreads();
+        const uint32_t pos = s_next;
+        __syncthreads();
+        if (pos >= A.ncirc) break;
+        const DCirc c = A.circs[A.order[pos]];
+        C<R> *pa = static_cast<C<R> *>(A.pool_a) + c.off_a;
+        C<R> *pb = static_cast<C<R> *>(A.pool_b) + c.off_b;
+        const uint64_t namp = uint64_t(1) << c.n;
+        run_forward<R>(A, c, sm0, pa);
+        const C<R> *psi = c.resident ? sm0 : pa;
+        if (A.mode == 0) {
+            double acc[kMaxObsPerCircuit];
+#pragma unroll
+            for (int o = 0; o < kMaxObsPerCircuit; ++o) acc[o] = 0.0;
+            expval_terms<R, false>(psi, namp, A.terms + c.term_begin, c.nterms, acc);
+            block_reduce<kMaxObsPerCircuit>(acc, s_red);
+            if (threadIdx.x == 0)
+                for (uint32_t o = 0; o < c.nobs; ++o) A.out[c.out_begin + o] = acc[o];
+            __syncthreads();
+            continue;
+        }
+        // ---- VJP: bra = sum_o dy_o O_o psi, then the reverse sweep ----
+        C<R> *bra = c.resident ? sm1 : pb;
+        init_bra<R>(bra, psi, namp, A.terms + c.term_begin, c.nterms, A.dy + c.out_begin);
+        __syncthreads();
+        if (c.resident) {
+            C<R> *tiles[2] = {sm0, sm1};
+            const DSeg sg = A.segs[c.seg_begin];
+            for (int32_t o = (int32_t)sg.nops - 1; o >= 0; --o) {
+                const DOp op = A.ops[sg.op_begin + o];
+                if (op.gslot >= 0) {
+                    double p = gen_inner_tile<R>(sm1, sm0, c.kt, op, A.consts);
+#pragma unroll
+                    for (int off = 16; off > 0; off >>= 1) p += __shfl_down_sync(0xffffffffu, p, off);
+                    if (lane == 0) A.gradw[(size_t)op.gslot * nw + warp] = p;
+                }
+                if (threadIdx.x == 0) op_coeffs<R>(op, A.params, A.consts, true, coef);
+                __syncthreads();
+                apply_tile<R, 2>(tiles, c.kt, op, coef);
+                __syncthreads();
+            }
+            continue;
+        }
+        const uint64_t ntiles = uint64_t(1) << (c.n - c.kt);
+        const uint32_t tn = 1u << c.kt;
+        C<R> *tiles[2] = {sm0, sm1};
+        for (int32_t si = (int32_t)c.nseg - 1; si >= 0; --si) {
+            const DSeg sg = A.segs[c.seg_begin + si];
+            for (uint64_t t = 0; t < ntiles; ++t) {
+                const uint64_t tbase = deposit64(t, sg.gbits, sg.ng);
+                load_tile<R>(sm0, pa, sg, tbase, tn);
+                load_tile<R>(sm1, pb, sg, tbase, tn);
+                __syncthreads();
+                for (int32_t o = (int32_t)sg.nops - 1; o >= 0; --o) {
+                    const DOp op = A.ops[sg.op_begin + o];
+                    if (op.gslot >= 0) {
+                        double p = gen_inner_tile<R>(sm1, sm0, c.kt, op, A.consts);
+#pragma unroll
+                        for (int off = 16; off > 0; off >>= 1) p += __shfl_down_sync(0xffffffffu, p, off);
+                        if (lane == 0) {
+                            double *slot = A.gradw + (size_t)op.gslot * nw + warp;
+                            *slot = (t == 0) ? p : *slot + p;
+                        }
+                    }
+                    if (threadIdx.x == 0) op_coeffs<R>(op, A.params, A.consts, true, coef);
+                    __syncthreads();
+                    apply_tile<R, 2>(tiles, c.kt, op, coef);
+                    __syncthreads();
+                }
+                store_tile<R>(pa, sm0, sg, tbase, tn);
+                store_tile<R>(pb, sm1, sg, tbase, tn);
+                __syncthreads();
+            }
+        }
+    }
+}
+
+// grad[p] = sum over ops referencing p (CSR order) of gscale * sum_w gradw[op, w]
+__global__ void k_grad_params(const uint32_t *__restrict__ rowptr, const uint32_t *__restrict__ cols,
+                              const double *__restrict__ gscale, const double *__restrict__ gradw, int nw,
+                              uint64_t nparams, double *__restrict__ grad) {
+    for (uint64_t p = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; p < nparams; p += (uint64_t)gridDim.x * blockDim.x) {
+        double s = 0.0;
+        for (uint32_t k = rowptr[p]; k < rowptr[p + 1]; ++k) {
+            const uint32_t g = cols[k];
+            double v = 0.0;
+            for (int w = 0; w < nw; ++w) v += gradw[(size_t)g * nw + w];
+            s += gscale[g] * v;
+        }
+        grad[p] = s;
+    }
+}
+
+// jac[jac_index[g]] = gscale * sum_w gradw[g, w]  (one observable pass)
+__global__ void k_grad_scatter(const double *__restrict__ gscale, const double *__restrict__ gradw, int nw,
+                               uint32_t ngslots, uint32_t obs, const uint32_t *__restrict__ gslot_circ,
+                               const DCirc *__restrict__ circs, const uint64_t *__restrict__ jac_base,
+                               const uint32_t *__restrict__ gslot_col, const uint32_t *__restrict__ circ_ncols,
+                               double *__restrict__ jac) {
+    for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < ngslots; g += gridDim.x * blockDim.x) {
+        const uint32_t c = gslot_circ[g];
+        if (obs >= circs[c].nobs) continue;
+        double v = 0.0;
+        for (int w = 0; w < nw; ++w) v += gradw[(size_t)g * nw + w];
+        jac[jac_base[c] + (uint64_t)obs * circ_ncols[c] + gslot_col[g]] = gscale[g] * v;
+    }
+}
+
+__global__ void k_onehot_dy(double *dy, const DCirc *circs, uint32_t ncirc, uint32_t obs) {
+    for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < ncirc; c += gridDim.x * blockDim.x)
+        for (uint32_t o = 0; o < circs[c].nobs; ++o) dy[circs[c].out_begin + o] = (o == obs) ? 1.0 : 0.0;
+}
+
+// ---------------------------------------------------------------------------
+// host side
+struct Config {
+    int threads = 512;
+    int kt = 13;
+};
+
+struct HostOp {
+    uint32_t gate;
+    std::vector<uint32_t> bits;  // circuit bit positions, gate order (controls first as in the reference)
+    bool inv;
+    int64_t pslot;
+    std::vector<cd> cmat;  // constant matrix / phases (for constant gates)
+    int form;
+    int nt;                // number of targets (rest are controls)
+    bool diff;             // differentiated (param op)
+    int gen;               // generator id
+};
+
+struct Batch {
+    int dtype = B200SV_C128;
+    int device = 0;
+    cudaStream_t own = nullptr, ext = nullptr;
+    cudaStream_t stream() const { return ext ? ext : own; }
+    uint64_t nparams = 0;
+    uint32_t ncirc = 0;
+    Config cfg;
+    bool use_graphs = false;
+    uint32_t last_launches = 0;
+
+    // circuit descriptions kept for re-planning
+    std::vector<uint32_t> nq;
+    std::vector<std::vector<HostOp>> hops;
+    std::vector<std::vector<DTerm>> hterms;  // masks in circuit bit positions
+    std::vector<uint32_t> nobs;
+    uint32_t total_obs = 0;
+
+    // device program
+    DCirc *d_circs = nullptr;
+    DSeg *d_segs = nullptr;
+    DOp *d_ops = nullptr;
+    DTerm *d_terms = nullptr;
+    double2 *d_consts = nullptr;
+    uint32_t *d_order = nullptr;
+    uint32_t *d_counter = nullptr;
+    void *d_pool_a = nullptr, *d_pool_b = nullptr;
+    size_t pool_a_bytes = 0, pool_b_bytes = 0;
+    double *d_gradw = nullptr;
+    double *d_gscale = nullptr;
+    uint32_t *d_rowptr = nullptr, *d_cols = nullptr;
+    uint32_t *d_gslot_circ = nullptr, *d_gslot_col = nullptr, *d_circ_ncols = nullptr;
+    uint64_t *d_jac_base = nullptr;
+    double *d_dy_tmp = nullptr;
+    double *d_params_in = nullptr, *d_dy_in = nullptr, *d_out = nullptr, *d_grad = nullptr;
+    uint32_t ngslots = 0;
+    size_t smem_bytes = 0;
+    int grid = 0;
+    std::vector<DCirc> h_circs;
+    std::vector<uint32_t> circ_ncols;
+    std::vector<uint64_t> jac_base;
+    uint64_t jac_total = 0;
+
+    cudaGraphExec_t g_forward = nullptr, g_vjp = nullptr;
+
+    std::vector<void *> allocs;
+    ~Batch() {
+        if (g_forward) cudaGraphExecDestroy(g_forward);
+        if (g_vjp) cudaGraphExecDestroy(g_vjp);
+        for (void *p : allocs) cudaFree(p);
+        if (own) cudaStreamDestroy(own);
+    }
+    template <typename T> T *dalloc(size_t count) {
+        void *p = nullptr;
+        B200SV_CUDA(cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T)));
+        allocs.push_back(p);
+        return static_cast<T *>(p);
+    }
+    void free_program() {
+        if (g_forward) { cudaGraphExecDestroy(g_forward); g_forward = nullptr; }
+        if (g_vjp) { cudaGraphExecDestroy(g_vjp); g_vjp = nullptr; }
+        for (void *p : allocs) cudaFree(p);
+        allocs.clear();
+    }
+    size_t amp() const { return dtype == B200SV_C64 ? 8 : 16; }
+};
+
+int popcount64(uint64_t x) { return __builtin_popcountll(x); }
+
+// translate one reference operation into a batch op (circuit bit positions)
+HostOp make_hostop(const b200sv_op &o, int64_t pslot, uint32_t nq, int dtype) {
+    HostOp h{};
+    h.gate = o.gate;
+    h.inv = o.inverse != 0;
+    h.pslot = pslot;
+    h.diff = false;
+    h.gen = -1;
+    std::vector<uint32_t> w(o.wires, o.wires + o.nwires);
+    check_wires(w.data(), (uint32_t)w.size(), nq, "batch op");
+    std::vector<uint32_t> b(w.size());
+    for (size_t i = 0; i < w.size(); ++i) b[i] = bitpos(w[i], nq);
+    if (o.gate == B200SV_OP_MATRIX) {
+        if (o.nwires < 1 || o.nwires > 2 || !o.matrix) throw Unsupported("batch: matrix ops act on 1 or 2 wires");
+        const size_t d = size_t(1) << o.nwires;
+        h.cmat.resize(d * d);
+        for (size_t i = 0; i < d * d; ++i) {
+            if (dtype == B200SV_C64) {
+                const float *f = static_cast<const float *>(o.matrix);
+                h.cmat[i] = cd(f[2 * i], f[2 * i + 1]);
+            } else {
+                const double *f = static_cast<const double *>(o.matrix);
+                h.cmat[i] = cd(f[2 * i], f[2 * i + 1]);
+            }
+        }
+        if (h.inv) h.cmat = dagger(h.cmat, d);
+        h.gate = kConstGate;
+        h.form = o.nwires == 1 ? F_MAT1 : F_MAT2;
+        h.nt = (int)o.nwires;
+        h.bits = b;
+        return h;
+    }
+    if (o.gate >= kNumGates) throw ArgError("batch: unknown gate id");
+    const GateInfo &gi = gate_table()[o.gate];
+    if (gi.nwires >= 0 && (int)o.nwires != gi.nwires) throw ArgError(std::string("batch: wrong wire count for ") + gi.name);
+    const bool param = gi.nparams == 1;
+    if (gi.nparams > 1) throw Unsupported(std::string("batch: ") + gi.name + " must be decomposed into single-parameter gates");
+    if (param && pslot < 0 && o.nparams != 1) throw ArgError(std::string("batch: ") + gi.name + " needs a parameter");
+    h.bits = b;
+    switch (o.gate) {
+    case B200SV_Identity: h.form = F_NOOP; h.nt = 0; h.gate = kConstGate; return h;
+    case B200SV_PauliX: h.form = F_SWAP; h.nt = 1; h.gate = kConstGate; return h;
+    case B200SV_CNOT: h.form = F_SWAP; h.nt = 1; h.gate = kConstGate; return h;
+    case B200SV_Toffoli: h.form = F_SWAP; h.nt = 1; h.gate = kConstGate; return h;
+    case B200SV_SWAP: h.form = F_SWAP; h.nt = 2; h.gate = kConstGate; return h;
+    case B200SV_CSWAP: h.form = F_SWAP; h.nt = 2; h.gate = kConstGate; return h;
+    default: break;
+    }
+    // everything else: dense / diagonal, constant or parameterised
+    auto constant = [&](int form, int nt, std::vector<cd> m) {
+        h.form = form;
+        h.nt = nt;
+        h.gate = kConstGate;
+        h.cmat = std::move(m);
+        return h;
+    };
+    if (!param || pslot < 0) {
+        // constant gate: reuse the plain-path compiler for the coefficients
+        const double th = param ? o.params[0] : 0.0;
+        GateDesc g = compile_gate(o.gate, o.wires, o.nwires, h.inv, param ? &th : nullptr, param ? 1 : 0, nq);
+        switch (g.kind) {
+        case Kind::Dense:
+            if (g.k == 1) return constant(F_MAT1, 1, g.m);
+            if (g.k == 2 && g.cbits.empty()) return constant(F_MAT2, 2, g.m);
+            throw Unsupported("batch: dense gate form not supported");
+        case Kind::Diag: {
+            std::vector<cd> ph = g.m;
+            ph.resize(4, cd(1, 0));
+            return constant(F_DIAG, g.k, ph);
+        }
+        case Kind::Pair: {
+            if (g.k != 2) throw Unsupported("batch: four-wire gates are not supported");
+            std::vector<cd> m(16, 0.0);
+            for (int r = 0; r < 4; ++r) m[r * 4 + r] = g.gamma;
+            m[g.pa * 4 + g.pa] = g.m2[0];
+            m[g.pa * 4 + g.pb] = g.m2[1];
+            m[g.pb * 4 + g.pa] = g.m2[2];
+            m[g.pb * 4 + g.pb] = g.m2[3];
+            return constant(F_MAT2, 2, m);
+        }
+        case Kind::Parity: {
+            h.form = F_PARITY;
+            h.nt = 0;
+            h.gate = kConstGate;
+            h.cmat = {g.pphase[0], g.pphase[1], 1.0, 1.0};
+            return h;
+        }
+        default: throw Unsupported("batch: gate form not supported");
+        }
+    }
+    // parameterised gate with a slot: coefficients synthesised on the device
+    h.diff = true;
+    h.gen = generator_of_gate(o.gate);
+    switch (o.gate) {
+    case B200SV_RX: case B200SV_RY: h.form = F_MAT1; h.nt = 1; break;
+    case B200SV_RZ: h.form = F_DIAG; h.nt = 1; break;
+    case B200SV_PhaseShift: h.form = F_DIAG; h.nt = 0; break;
+    case B200SV_CRX: case B200SV_CRY: h.form = F_MAT1; h.nt = 1; break;
+    case B200SV_CRZ: h.form = F_DIAG; h.nt = 1; break;
+    case B200SV_ControlledPhaseShift: h.form = F_DIAG; h.nt = 0; break;
+    case B200SV_IsingXX: case B200SV_IsingYY: case B200SV_IsingXY: case B200SV_SingleExcitation:
+    case B200SV_SingleExcitationMinus: case B200SV_SingleExcitationPlus: h.form = F_MAT2; h.nt = 2; break;
+    case B200SV_IsingZZ: h.form = F_DIAG; h.nt = 2; break;
+    case B200SV_MultiRZ: h.form = F_PARITY; h.nt = 0; break;
+    default: throw Unsupported(std::string("batch: parameterised gate not supported: ") + gi.name);
+    }
+    return h;
+}
+
+struct Planned {
+    std::vector<DCirc> circs;
+    std::vector<DSeg> segs;
+    std::vector<DOp> ops;
+    std::vector<DTerm> terms;
+    std::vector<double2> consts;
+    std::vector<uint32_t> order;
+    std::vector<double> gscale;
+    std::vector<uint32_t> gslot_circ, gslot_col;
+    std::vector<int64_t> gslot_param;
+    size_t pool_a = 0, pool_b = 0;
+    int max_kt = 1;
+};
+
+uint32_t push_const(Planned &P, const std::vector<cd> &m) {
+    const uint32_t idx = (uint32_t)(P.consts.size() / 16);
+    for (int i = 0; i < 16; ++i) {
+        const cd z = i < (int)m.size() ? m[i] : cd(0, 0);
+        P.consts.push_back(make_double2(z.real(), z.imag()));
+    }
+    return idx;
+}
+
+// lower one host op into a device op with tile-local bit positions
+DOp lower(Planned &P, const HostOp &h, const std::vector<int> &loc /* state bit -> tile bit */) {
+    DOp d{};
+    d.form = (uint8_t)h.form;
+    d.gate = (uint8_t)(h.gate == kConstGate ? kConstGate : h.gate);
+    d.inv = h.inv ? 1 : 0;
+    d.nt = (uint8_t)h.nt;
+    d.pslot = (int32_t)(h.gate == kConstGate ? -1 : h.pslot);
+    d.gslot = -1;
+    std::vector<uint32_t> lb(h.bits.size());
+    for (size_t i = 0; i < h.bits.size(); ++i) lb[i] = (uint32_t)loc[h.bits[i]];
+    // targets are the last nt bits of the reference wire order; the rest are controls
+    const size_t nc = h.form == F_PARITY || h.form == F_NOOP ? 0 : lb.size() - h.nt;
+    std::vector<uint32_t> tgt(lb.begin() + nc, lb.end()), ctl(lb.begin(), lb.begin() + nc);
+    if (h.form == F_DIAG && h.nt == 0) {  // phase on all-ones of the listed bits
+        ctl = lb;
+        tgt.clear();
+    }
+    if (h.form == F_SWAP) {
+        // X-type (nt == 1): swap rows 0/1 of the target; SWAP-type (nt == 2): rows 1/2
+        std::vector<uint32_t> all = lb;
+        std::sort(all.begin(), all.end());
+        d.nb = (uint8_t)all.size();
+        for (size_t j = 0; j < all.size(); ++j) d.low[j] = (uint16_t)((1u << all[j]) - 1);
+        for (auto x : ctl) d.cmask |= 1u << x;
+        if (h.nt == 1) {
+            d.off[0] = 0;
+            d.off[1] = 1u << tgt[0];
+        } else {
+            d.off[0] = 1u << tgt[1];  // row 01
+            d.off[1] = 1u << tgt[0];  // row 10
+        }
+        d.cidx = 0;
+        return d;
+    }
+    if (h.form == F_PARITY) {
+        for (auto x : lb) d.pmask |= 1u << x;
+        d.nb = 0;
+    } else {
+        std::vector<uint32_t> all = lb;
+        std::sort(all.begin(), all.end());
+        d.nb = (uint8_t)all.size();
+        for (size_t j = 0; j < all.size(); ++j) d.low[j] = (uint16_t)((1u << all[j]) - 1);
+        for (auto x : ctl) d.cmask |= 1u << x;
+        const int nt = (int)tgt.size();
+        for (int r = 0; r < (1 << nt); ++r) {
+            uint32_t o = 0;
+            for (int j = 0; j < nt; ++j)
+                if (r & (1 << (nt - 1 - j))) o |= 1u << tgt[j];
+            d.off[r] = o;
+        }
+        d.nt = (uint8_t)nt;
+    }
+    if (h.gate == kConstGate) d.cidx = push_const(P, h.cmat);
+    if (h.diff && h.gen >= 0) {
+        double sc = 0.0;
+        // generator as a matrix on the gate's bits (all of them, controls included)
+        // built with the plain-path compiler on a virtual register whose bits are the tile bits
+        std::vector<uint32_t> vw(lb.size());
+        const uint32_t vq = 32;
+        for (size_t i = 0; i < lb.size(); ++i) vw[i] = vq - 1 - lb[i];
+        GateDesc G = compile_generator((uint32_t)h.gen, vw.data(), (uint32_t)vw.size(), vq, &sc);
+        d.gscale = -2.0 * sc * (h.inv ? -1.0 : 1.0);
+        if (G.kind == Kind::Parity) {
+            d.gform = G_PARITY;
+            d.pmask = (uint32_t)G.pmask;
+        } else {
+            // expand to a dense matrix over G.tbits (k <= 2)
+            const int k = G.k;
+            if (k > 2) throw Unsupported("batch: generator wider than two wires");
+            const int D = 1 << k;
+            std::vector<cd> gm(D * D, 0.0);
+            if (G.kind == Kind::Dense) gm = G.m;
+            else if (G.kind == Kind::Diag) for (int r = 0; r < D; ++r) gm[r * D + r] = G.m[r];
+            else if (G.kind == Kind::Pair) {
+                for (int r = 0; r < D; ++r) gm[r * D + r] = G.gamma;
+                gm[G.pa * D + G.pa] = G.m2[0];
+                gm[G.pa * D + G.pb] = G.m2[1];
+                gm[G.pb * D + G.pa] = G.m2[2];
+                gm[G.pb * D + G.pb] = G.m2[3];
+            }
+            d.gform = G_MAT;
+            d.gk = (uint8_t)k;
+            std::vector<uint32_t> gb = G.tbits;
+            std::vector<uint32_t> sorted = gb;
+            std::sort(sorted.begin(), sorted.end());
+            d.gnb = (uint8_t)sorted.size();
+            for (size_t j = 0; j < sorted.size(); ++j) d.glow[j] = (uint16_t)((1u << sorted[j]) - 1);
+            for (int r = 0; r < D; ++r) {
+                uint32_t o = 0;
+                for (int j = 0; j < k; ++j)
+                    if (r & (1 << (k - 1 - j))) o |= 1u << gb[j];
+                d.goff[r] = o;
+            }
+            d.gcidx = push_const(P, gm);
+        }
+    }
+    return d;
+}
+
+Planned plan(const Batch &B, const Config &cfg, bool vjp) {
+    Planned P;
+    P.consts.reserve(1024);
+    push_const(P, {});  // slot 0 unused
+    const uint32_t nc = B.ncirc;
+    std::vector<double> cost(nc);
+    uint32_t out_begin = 0;
+    for (uint32_t c = 0; c < nc; ++c) {
+        const uint32_t n = B.nq[c];
+        DCirc dc{};
+        dc.n = n;
+        const int live = vjp ? 2 : 1;
+        (void)live;
+        dc.kt = (uint32_t)std::min<int>(cfg.kt, (int)n);
+        dc.resident = n <= (uint32_t)cfg.kt ? 1 : 0;
+        dc.seg_begin = (uint32_t)P.segs.size();
+        dc.nobs = B.nobs[c];
+        dc.out_begin = out_begin;
+        out_begin += B.nobs[c];
+        dc.term_begin = (uint32_t)P.terms.size();
+        for (auto t : B.hterms[c]) P.terms.push_back(t);
+        dc.nterms = (uint32_t)B.hterms[c].size();
+        // segmentation
+        const auto &ops = B.hops[c];
+        size_t i = 0;
+        while (i < ops.size() || (i == 0 && ops.empty())) {
+            uint64_t used = 0;
+            size_t j = i;
+            while (j < ops.size()) {
+                uint64_t b = 0;
+                for (auto x : ops[j].bits) b |= uint64_t(1) << x;
+                if (popcount64(used | b) > (int)dc.kt) break;
+                used |= b;
+                ++j;
+            }
+            if (j == i && i < ops.size()) throw Unsupported("batch: gate wider than the tile");
+            // local bits: used bits plus the lowest unused bits up to kt
+            std::vector<uint32_t> L;
+            for (uint32_t x = 0; x < n; ++x)
+                if (used & (uint64_t(1) << x)) L.push_back(x);
+            for (uint32_t x = 0; x < n && L.size() < dc.kt; ++x)
+                if (!(used & (uint64_t(1) << x))) L.push_back(x);
+            std::sort(L.begin(), L.end());
+            DSeg s{};
+            s.nl = (uint8_t)L.size();
+            std::vector<int> loc(n, -1);
+            for (size_t q = 0; q < L.size(); ++q) {
+                s.lbits[q] = (uint8_t)L[q];
+                loc[L[q]] = (int)q;
+            }
+            uint8_t ng = 0;
+            for (uint32_t x = 0; x < n; ++x)
+                if (loc[x] < 0) s.gbits[ng++] = (uint8_t)x;
+            s.ng = ng;
+            s.op_begin = (uint32_t)P.ops.size();
+            s.nops = (uint32_t)(j - i);
+            for (size_t q = i; q < j; ++q) {
+                DOp d = lower(P, ops[q], loc);
+                if (ops[q].diff && vjp) {
+                    d.gslot = (int32_t)P.gscale.size();
+                    P.gscale.push_back(d.gscale);
+                    P.gslot_circ.push_back(c);
+                    P.gslot_param.push_back(ops[q].pslot);
+                }
+                P.ops.push_back(d);
+            }
+            P.segs.push_back(s);
+            if (ops.empty()) break;
+            i = j;
+        }
+        dc.nseg = (uint32_t)(P.segs.size() - dc.seg_begin);
+        if (!dc.resident) {
+            dc.off_a = P.pool_a;
+            P.pool_a += uint64_t(1) << n;
+            if (vjp) {
+                dc.off_b = P.pool_b;
+                P.pool_b += uint64_t(1) << n;
+            }
+        }
+        P.max_kt = std::max<int>(P.max_kt, (int)dc.kt);
+        cost[c] = double(uint64_t(1) << n) * double(ops.size() + 1);
+        P.circs.push_back(dc);
+    }
+    P.order.resize(nc);
+    std::iota(P.order.begin(), P.order.end(), 0u);
+    std::stable_sort(P.order.begin(), P.order.end(), [&](uint32_t a, uint32_t b) { return cost[a] > cost[b]; });
+    // per gslot column index within its circuit (param ops in op order)
+    std::vector<uint32_t> col_count(nc, 0);
+    P.gslot_col.resize(P.gslot_circ.size());
+    for (size_t g = 0; g < P.gslot_circ.size(); ++g) P.gslot_col[g] = col_count[P.gslot_circ[g]]++;
+    return P;
+}
+
+template <typename T> void upload(Batch &B, T *&dst, const std::vector<T> &src) {
+    dst = B.dalloc<T>(src.size());
+    if (!src.empty())
+        B200SV_CUDA(cudaMemcpy(dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice));
+}
+
+// Build the device program for a configuration (both forward and VJP share it:
+// the VJP layout is a superset).
+void build_program(Batch &B, const Config &cfg) {
+    B.free_program();
+    Planned P = plan(B, cfg, true);
+    B.cfg = cfg;
+    upload(B, B.d_circs, P.circs);
+    upload(B, B.d_segs, P.segs);
+    upload(B, B.d_ops, P.ops);
+    upload(B, B.d_terms, P.terms);
+    upload(B, B.d_consts, P.consts);
+    upload(B, B.d_order, P.order);
+    B.h_circs = P.circs;
+    B.d_counter = B.dalloc<uint32_t>(1);
+    B.pool_a_bytes = P.pool_a * B.amp();
+    B.pool_b_bytes = P.pool_b * B.amp();
+    B.d_pool_a = B.dalloc<unsigned char>(B.pool_a_bytes);
+    B.d_pool_b = B.dalloc<unsigned char>(B.pool_b_bytes);
+    B.ngslots = (uint32_t)P.gscale.size();
+    const int nw = cfg.threads / 32;
+    B.d_gradw = B.dalloc<double>((size_t)B.ngslots * nw);
+    upload(B, B.d_gscale, P.gscale);
+    // CSR param -> gslots
+    std::vector<uint32_t> rowptr(B.nparams + 1, 0), cols;
+    for (size_t g = 0; g < P.gslot_param.size(); ++g) {
+        const int64_t p = P.gslot_param[g];
+        if (p >= 0 && (uint64_t)p < B.nparams) rowptr[p + 1]++;
+    }
+    for (uint64_t p = 0; p < B.nparams; ++p) rowptr[p + 1] += rowptr[p];
+    cols.resize(rowptr[B.nparams]);
+    std::vector<uint32_t> fill(rowptr.begin(), rowptr.end() - 1);
+    for (size_t g = 0; g < P.gslot_param.size(); ++g) {
+        const int64_t p = P.gslot_param[g];
+        if (p >= 0 && (uint64_t)p < B.nparams) cols[fill[p]++] = (uint32_t)g;
+    }
+    upload(B, B.d_rowptr, rowptr);
+    upload(B, B.d_cols, cols);
+    upload(B, B.d_gslot_circ, P.gslot_circ);
+    upload(B, B.d_gslot_col, P.gslot_col);
+    B.circ_ncols.assign(B.ncirc, 0);
+    for (auto c : P.gslot_circ) B.circ_ncols[c]++;
+    B.jac_base.assign(B.ncirc, 0);
+    uint64_t acc = 0;
+    for (uint32_t c = 0; c < B.ncirc; ++c) {
+        B.jac_base[c] = acc;
+        acc += (uint64_t)B.nobs[c] * B.circ_ncols[c];
+    }
+    B.jac_total = acc;
+    upload(B, B.d_circ_ncols, B.circ_ncols);
+    upload(B, B.d_jac_base, B.jac_base);
+    B.d_dy_tmp = B.dalloc<double>(B.total_obs);
+    B.d_params_in = B.dalloc<double>(B.nparams);
+    B.d_dy_in = B.dalloc<double>(B.total_obs);
+    B.d_out = B.dalloc<double>(B.total_obs);
+    B.d_grad = B.dalloc<double>(B.nparams);
+    B.smem_bytes = (size_t)2 * (size_t(1) << P.max_kt) * B.amp();
+    int dev = 0, maxsm = 0, nsm = sm_count();
+    B200SV_CUDA(cudaGetDevice(&dev));
+    B200SV_CUDA(cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    const size_t static_smem = kMaxObsPerCircuit * 32 * 8 + 2 * 16 * 16 + 64;
+    if (B.smem_bytes + static_smem > (size_t)maxsm)
+        throw Unsupported("batch: tile does not fit in shared memory; lower kt");
+    if (B.dtype == B200SV_C64)
+        B200SV_CUDA(cudaFuncSetAttribute(k_batch<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)B.smem_bytes));
+    else
+        B200SV_CUDA(cudaFuncSetAttribute(k_batch<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)B.smem_bytes));
+    int per_sm = 0;
+    if (B.dtype == B200SV_C64)
+        B200SV_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch<float>, cfg.threads, B.smem_bytes));
+    else
+        B200SV_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch<double>, cfg.threads, B.smem_bytes));
+    if (per_sm < 1) throw Unsupported("batch: launch configuration does not fit on an SM");
+    B.grid = std::max(1, std::min<int>((int)B.ncirc, nsm * per_sm));
+    B200SV_CUDA(cudaDeviceSynchronize());
+}
+
+void launch_main(Batch &B, int mode, const double *params, const double *dy, double *out, cudaStream_t st) {
+    KArgs A{};
+    A.circs = B.d_circs;
+    A.segs = B.d_segs;
+    A.ops = B.d_ops;
+    A.terms = B.d_terms;
+    A.consts = B.d_consts;
+    A.order = B.d_order;
+    A.ncirc = B.ncirc;
+    A.counter = B.d_counter;
+    A.params = params;
+    A.dy = dy;
+    A.out = out;
+    A.gradw = B.d_gradw;
+    A.pool_a = B.d_pool_a;
+    A.pool_b = B.d_pool_b;
+    A.mode = mode;
+    int mk = 1;
+    for (auto &c : B.h_circs) mk = std::max<int>(mk, (int)c.kt);
+    A.max_kt = mk;
+    B200SV_CUDA(cudaMemsetAsync(B.d_counter, 0, sizeof(uint32_t), st));
+    if (B.dtype == B200SV_C64) k_batch<float><<<B.grid, B.cfg.threads, B.smem_bytes, st>>>(A);
+    else k_batch<double><<<B.grid, B.cfg.threads, B.smem_bytes, st>>>(A);
+    B200SV_CUDA(cudaGetLastError());
+}
+
+void enqueue_forward(Batch &B, cudaStream_t st) {
+    launch_main(B, 0, B.d_params_in, nullptr, B.d_out, st);
+}
+void enqueue_vjp(Batch &B, cudaStream_t st) {
+    launch_main(B, 1, B.d_params_in, B.d_dy_in, nullptr, st);
+    const int nw = B.cfg.threads / 32;
+    const uint64_t np = std::max<uint64_t>(B.nparams, 1);
+    k_grad_params<<<(unsigned)std::min<uint64_t>((np + 255) / 256, 4096), 256, 0, st>>>(
+        B.d_rowptr, B.d_cols, B.d_gscale, B.d_gradw, nw, B.nparams, B.d_grad);
+    B200SV_CUDA(cudaGetLastError());
+}
+
+template <class F> void run_maybe_graph(Batch &B, cudaGraphExec_t &exec, F &&enqueue) {
+    cudaStream_t st = B.stream();
+    if (!B.use_graphs) {
+        enqueue(st);
+        return;
+    }
+    if (!exec) {
+        cudaGraph_t g = nullptr;
+        B200SV_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        try {
+            enqueue(st);
+        } catch (...) {
+            cudaStreamEndCapture(st, &g);
+            if (g) cudaGraphDestroy(g);
+            throw;
+        }
+        B200SV_CUDA(cudaStreamEndCapture(st, &g));
+        B200SV_CUDA(cudaGraphInstantiate(&exec, g, 0));
+        cudaGraphDestroy(g);
+    }
+    B200SV_CUDA(cudaGraphLaunch(exec, st));
+}
+
+}  // namespace batch
+}  // namespace b200sv
+
+// =============================================================================
+using namespace b200sv;
+using namespace b200sv::batch;
+
+struct b200sv_batch {
+    std::unique_ptr<Batch> b;
+};
+
+extern "C" {
+
+int b200sv_batch_create(int dtype, const b200sv_batch_circuit *circuits, uint32_t ncircuits, uint64_t nparams,
+                        b200sv_batch_handle *out) {
+    return run_guarded([&] {
+        if (!out) throw ArgError("NULL output handle");
+        if (dtype != B200SV_C64 && dtype != B200SV_C128) throw ArgError("dtype must be B200SV_C64 or B200SV_C128");
+        if (ncircuits == 0 || !circuits) throw ArgError("a batch needs at least one circuit");
+        int ndev = 0;
+        if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+            cudaGetLastError();
+            throw CudaError("no CUDA device is available (libb200sv has no CPU path)");
+        }
+        auto B = std::make_unique<Batch>();
+        B->dtype = dtype;
+        B->nparams = nparams;
+        B->ncirc = ncircuits;
+        B200SV_CUDA(cudaGetDevice(&B->device));
+        B200SV_CUDA(cudaStreamCreateWithFlags(&B->own, cudaStreamNonBlocking));
+        for (uint32_t c = 0; c < ncircuits; ++c) {
+            const b200sv_batch_circuit &bc = circuits[c];
+            if (bc.num_qubits < 1 || bc.num_qubits > 30) throw ArgError("batch circuits have 1..30 qubits");
+            if (bc.nops && !bc.ops) throw ArgError("NULL ops");
+            if (bc.nobs > (uint32_t)kMaxObsPerCircuit) throw Unsupported("batch: at most 16 observables per circuit");
+            B->nq.push_back(bc.num_qubits);
+            std::vector<HostOp> hv;
+            for (uint32_t i = 0; i < bc.nops; ++i) {
+                const int64_t ps = bc.param_index ? bc.param_index[i] : -1;
+                if (ps >= 0 && (uint64_t)ps >= nparams) throw ArgError("batch: parameter index out of range");
+                hv.push_back(make_hostop(bc.ops[i], ps, bc.num_qubits, dtype));
+            }
+            B->hops.push_back(std::move(hv));
+            std::vector<DTerm> terms;
+            uint32_t t_global = 0;
+            for (uint32_t o = 0; o < bc.nobs; ++o) {
+                for (uint32_t t = 0; t < bc.obs_nterms[o]; ++t, ++t_global) {
+                    DTerm dt{};
+                    dt.obs = o;
+                    dt.coeff = bc.obs_coeffs[t_global];
+                    uint64_t used = 0;
+                    for (uint32_t q = bc.obs_offsets[t_global]; q < bc.obs_offsets[t_global + 1]; ++q) {
+                        const uint32_t w = bc.obs_wires[q];
+                        if (w >= bc.num_qubits) throw ArgError("batch: observable wire out of range");
+                        const uint64_t bit = uint64_t(1) << bitpos(w, bc.num_qubits);
+                        if (used & bit) throw ArgError("All wires in observables must be disjoint.");
+                        used |= bit;
+                        switch (bc.obs_paulis[q]) {
+                        case 'I': break;
+                        case 'X': dt.xmask |= bit; break;
+                        case 'Y': dt.xmask |= bit; dt.zmask |= bit; dt.ny++; break;
+                        case 'Z': dt.zmask |= bit; break;
+                        default: throw ArgError("Pauli letters must be I, X, Y or Z");
+                        }
+                    }
+                    terms.push_back(dt);
+                }
+            }
+            B->hterms.push_back(std::move(terms));
+            B->nobs.push_back(bc.nobs);
+            B->total_obs += bc.nobs;
+        }
+        Config cfg;
+        cfg.kt = dtype == B200SV_C64 ? 13 : 12;
+        cfg.threads = 512;
+        build_program(*B, cfg);
+        auto *h = new b200sv_batch;
+        h->b = std::move(B);
+        *out = h;
+    });
+}
+
+int b200sv_batch_destroy(b200sv_batch_handle b) {
+    return run_guarded([&] {
+        if (!b) return;
+        cudaStreamSynchronize(b->b->stream());
+        delete b;
+    });
+}
+
+int b200sv_batch_set_stream(b200sv_batch_handle b, void *s) {
+    return run_guarded([&] {
+        if (!b) throw ArgError("NULL batch");
+        if (b->b->ext != static_cast<cudaStream_t>(s)) {
+            b->b->ext = static_cast<cudaStream_t>(s);
+            // graphs are instantiated per stream use; keep them (launchable on any stream)
+        }
+    });
+}
+
+int b200sv_batch_use_graphs(b200sv_batch_handle b, int enable) {
+    return run_guarded([&] {
+        if (!b) throw ArgError("NULL batch");
+        b->b->use_graphs = enable != 0;
+    });
+}
+
+int b200sv_batch_forward(b200sv_batch_handle bh, const double *params, double *out) {
+    return run_guarded([&] {
+        if (!bh) throw ArgError("NULL batch");
+        Batch &B = *bh->b;
+        if (B.nparams && !params) throw ArgError("NULL params");
+        if (!out) throw ArgError("NULL output");
+        cudaStream_t st = B.stream();
+        if (B.nparams)
+            B200SV_CUDA(cudaMemcpyAsync(B.d_params_in, params, B.nparams * sizeof(double), cudaMemcpyDeviceToDevice, st));
+        run_maybe_graph(B, B.g_forward, [&](cudaStream_t s) { enqueue_forward(B, s); });
+        B200SV_CUDA(cudaMemcpyAsync(out, B.d_out, B.total_obs * sizeof(double), cudaMemcpyDeviceToDevice, st));
+        B.last_launches = 1;
+    });
+}
+
+int b200sv_batch_vjp(b200sv_batch_handle bh, const double *params, const double *dy, double *grad) {
+    return run_guarded([&] {
+        if (!bh) throw ArgError("NULL batch");
+        Batch &B = *bh->b;
+        if ((B.nparams && !params) || !dy || (B.nparams && !grad)) throw ArgError("NULL device buffer");
+        cudaStream_t st = B.stream();
+        if (B.nparams)
+            B200SV_CUDA(cudaMemcpyAsync(B.d_params_in, params, B.nparams * sizeof(double), cudaMemcpyDeviceToDevice, st));
+        B200SV_CUDA(cudaMemcpyAsync(B.d_dy_in, dy, B.total_obs * sizeof(double), cudaMemcpyDeviceToDevice, st));
+        run_maybe_graph(B, B.g_vjp, [&](cudaStream_t s) { enqueue_vjp(B, s); });
+        if (B.nparams)
+            B200SV_CUDA(cudaMemcpyAsync(grad, B.d_grad, B.nparams * sizeof(double), cudaMemcpyDeviceToDevice, st));
+        B.last_launches = 2;
+    });
+}
+
+int b200sv_batch_jacobian(b200sv_batch_handle bh, const double *params, double *jac) {
+    return run_guarded([&] {
+        if (!bh) throw ArgError("NULL batch");
+        Batch &B = *bh->b;
+        if ((B.nparams && !params) || !jac) throw ArgError("NULL device buffer");
+        cudaStream_t st = B.stream();
+        if (B.nparams)
+            B200SV_CUDA(cudaMemcpyAsync(B.d_params_in, params, B.nparams * sizeof(double), cudaMemcpyDeviceToDevice, st));
+        uint32_t maxobs = 0;
+        for (auto n : B.nobs) maxobs = std::max(maxobs, n);
+        const int nw = B.cfg.threads / 32;
+        uint32_t launches = 0;
+        for (uint32_t o = 0; o < maxobs; ++o) {
+            k_onehot_dy<<<std::max(1u, (B.ncirc + 255) / 256), 256, 0, st>>>(B.d_dy_in, B.d_circs, B.ncirc, o);
+            launch_main(B, 1, B.d_params_in, B.d_dy_in, nullptr, st);
+            if (B.ngslots)
+                k_grad_scatter<<<std::max(1u, (B.ngslots + 255) / 256), 256, 0, st>>>(
+                    B.d_gscale, B.d_gradw, nw, B.ngslots, o, B.d_gslot_circ, B.d_circs, B.d_jac_base,
+                    B.d_gslot_col, B.d_circ_ncols, jac);
+            B200SV_CUDA(cudaGetLastError());
+            launches += 3;
+        }
+        B.last_launches = launches;
+    });
+}
+
+int b200sv_batch_autotune(b200sv_batch_handle bh, const double *params, int *chosen) {
+    return run_guarded([&] {
+        if (!bh) throw ArgError("NULL batch");
+        Batch &B = *bh->b;
+        cudaStream_t st = B.stream();
+        if (B.nparams)
+            B200SV_CUDA(cudaMemcpyAsync(B.d_params_in, params, B.nparams * sizeof(double), cudaMemcpyDeviceToDevice, st));
+        std::vector<Config> cands;
+        const int kts_c64[] = {11, 12, 13};
+        const int kts_c128[] = {10, 11, 12};
+        for (int th : {256, 512, 1024})
+            for (int i = 0; i < 3; ++i) cands.push_back(Config{th, B.dtype == B200SV_C64 ? kts_c64[i] : kts_c128[i]});
+        float best = 1e30f;
+        int best_i = -1;
+        std::vector<double> saved_params(B.nparams);
+        if (B.nparams)
+            B200SV_CUDA(cudaMemcpy(saved_params.data(), B.d_params_in, B.nparams * sizeof(double), cudaMemcpyDeviceToHost));
+        cudaEvent_t e0, e1;
+        B200SV_CUDA(cudaEventCreate(&e0));
+        B200SV_CUDA(cudaEventCreate(&e1));
+        for (size_t i = 0; i < cands.size(); ++i) {
+            try {
+                build_program(B, cands[i]);
+            } catch (const Unsupported &) {
+                continue;
+            }
+            if (B.nparams)
+                B200SV_CUDA(cudaMemcpy(B.d_params_in, saved_params.data(), B.nparams * sizeof(double), cudaMemcpyHostToDevice));
+            B200SV_CUDA(cudaMemset(B.d_dy_in, 0, B.total_obs * sizeof(double)));
+            enqueue_vjp(B, st);  // warm
+            B200SV_CUDA(cudaEventRecord(e0, st));
+            enqueue_vjp(B, st);
+            B200SV_CUDA(cudaEventRecord(e1, st));
+            B200SV_CUDA(cudaEventSynchronize(e1));
+            float ms = 0;
+            B200SV_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+            if (ms < best) {
+                best = ms;
+                best_i = (int)i;
+            }
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        if (best_i < 0) throw Unsupported("batch autotune: no configuration fits");
+        build_program(B, cands[best_i]);
+        if (B.nparams)
+            B200SV_CUDA(cudaMemcpy(B.d_params_in, saved_params.data(), B.nparams * sizeof(double), cudaMemcpyHostToDevice));
+        if (chosen) *chosen = cands[best_i].threads * 100 + cands[best_i].kt;
+    });
+}
+
+int b200sv_batch_last_launches(b200sv_batch_handle b, uint32_t *out) {
+    return run_guarded([&] {
+        if (!b || !out) throw ArgError("NULL argument");
+        *out = b->b->last_launches;
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,839 @@
+// sv_capi.cu — extern "C" entry points of libb200sv (declared in include/b200sv.h).
+//
+// Host orchestration of the plain form: one state per handle, one gate per
+// launch, all work stream-ordered on the handle's stream; results are read back
+// only where the ABI returns host data.
+#include <algorithm>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/b200sv.h"
+#include "sv_internal.hpp"
+
+using namespace b200sv;
+
+struct b200sv_state {
+    uint32_t nq = 0;
+    int dtype = B200SV_C128;
+    int device = 0;
+    cudaStream_t own = nullptr;
+    cudaStream_t ext = nullptr;
+    void *d_state = nullptr;
+    double *d_partials = nullptr;  // kPartialsCapacity doubles
+    double *d_small = nullptr;     // small results (kSmall doubles)
+    double *h_small = nullptr;     // pinned mirror of d_small
+    void *d_matrix = nullptr;      // dense matrix staging
+    size_t matrix_bytes = 0;
+    void *d_scratch[2] = {nullptr, nullptr};  // two state-sized work buffers (lazy)
+    cudaStream_t stream() const { return ext ? ext : own; }
+    size_t amp_bytes() const { return dtype == B200SV_C64 ? 8 : 16; }
+    size_t state_bytes() const { return amp_bytes() << nq; }
+};
+
+namespace {
+
+constexpr size_t kSmall = 4096;
+thread_local std::string g_last_error;
+
+template <class F> int guard(F &&f) {
+    try {
+        g_last_error.clear();
+        f();
+        return B200SV_OK;
+    } catch (const ArgError &e) {
+        g_last_error = e.what();
+        return B200SV_ERR_ARGUMENT;
+    } catch (const Unsupported &e) {
+        g_last_error = e.what();
+        return B200SV_ERR_UNSUPPORTED;
+    } catch (const AllocError &e) {
+        g_last_error = e.what();
+        return B200SV_ERR_ALLOC;
+    } catch (const CudaError &e) {
+        g_last_error = e.what();
+        return B200SV_ERR_CUDA;
+    } catch (const std::bad_alloc &) {
+        g_last_error = "host allocation failed";
+        return B200SV_ERR_ALLOC;
+    } catch (const std::exception &e) {
+        g_last_error = e.what();
+        return B200SV_ERR_ARGUMENT;
+    }
+}
+
+void need(bool ok, const char *msg) {
+    if (!ok) throw ArgError(msg);
+}
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        cudaGetDevice(&prev);
+        if (prev != dev) B200SV_CUDA(cudaSetDevice(dev));
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        cudaGetDevice(&cur);
+        if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+void ensure_matrix(b200sv_state *h, size_t bytes) {
+    if (bytes <= h->matrix_bytes) return;
+    if (h->d_matrix) {
+        B200SV_CUDA(cudaStreamSynchronize(h->stream()));
+        B200SV_CUDA(cudaFree(h->d_matrix));
+        h->d_matrix = nullptr;
+        h->matrix_bytes = 0;
+    }
+    size_t want = std::max<size_t>(bytes, 64 * 16 * 64);
+    B200SV_CUDA(cudaMalloc(&h->d_matrix, want));
+    h->matrix_bytes = want;
+}
+
+void *scratch(b200sv_state *h, int i) {
+    if (!h->d_scratch[i]) B200SV_CUDA(cudaMalloc(&h->d_scratch[i], h->state_bytes()));
+    return h->d_scratch[i];
+}
+
+void apply_desc(b200sv_state *h, void *const *states, int nstates, const GateDesc &g) {
+    if (g.kind == Kind::Dense && g.k >= 4) {
+        const size_t need_b = h->amp_bytes() * g.m.size();
+        ensure_matrix(h, need_b);
+    }
+    if (h->dtype == B200SV_C64) launch_gate<float>(states, nstates, h->nq, g, h->d_matrix, h->stream());
+    else launch_gate<double>(states, nstates, h->nq, g, h->d_matrix, h->stream());
+}
+
+void apply_desc_multi(b200sv_state *h, const std::vector<void *> &states, const GateDesc &g) {
+    for (size_t i = 0; i < states.size(); i += kMaxStatesPerLaunch) {
+        const int cnt = (int)std::min<size_t>(kMaxStatesPerLaunch, states.size() - i);
+        apply_desc(h, states.data() + i, cnt, g);
+    }
+}
+
+std::vector<cd> read_matrix(const void *m, size_t count, int dtype) {
+    std::vector<cd> r(count);
+    if (dtype == B200SV_C64) {
+        const float *f = static_cast<const float *>(m);
+        for (size_t i = 0; i < count; ++i) r[i] = cd(f[2 * i], f[2 * i + 1]);
+    } else {
+        const double *d = static_cast<const double *>(m);
+        for (size_t i = 0; i < count; ++i) r[i] = cd(d[2 * i], d[2 * i + 1]);
+    }
+    return r;
+}
+
+// ---- operations ------------------------------------------------------------
+struct OpRec {
+    uint32_t gate;
+    std::vector<uint32_t> wires;
+    bool inverse;
+    std::vector<double> params;
+    std::vector<cd> matrix;
+};
+
+std::vector<OpRec> read_ops(const b200sv_op *ops, uint32_t nops, int dtype) {
+    need(nops == 0 || ops != nullptr, "operations pointer is NULL");
+    std::vector<OpRec> r(nops);
+    for (uint32_t i = 0; i < nops; ++i) {
+        const b200sv_op &o = ops[i];
+        need(o.nwires == 0 || o.wires, "operation wires pointer is NULL");
+        need(o.nparams == 0 || o.params, "operation params pointer is NULL");
+        r[i].gate = o.gate;
+        r[i].wires.assign(o.wires, o.wires + o.nwires);
+        r[i].inverse = o.inverse != 0;
+        r[i].params.assign(o.params, o.params + o.nparams);
+        if (o.gate == B200SV_OP_MATRIX) {
+            need(o.matrix != nullptr, "matrix operation without matrix");
+            need(o.nwires > 0 && o.nwires <= 11, "matrix operation needs 1..11 wires");
+            const size_t d = size_t(1) << o.nwires;
+            r[i].matrix = read_matrix(o.matrix, d * d, dtype);
+        }
+    }
+    return r;
+}
+
+GateDesc compile_op(const OpRec &o, bool inverse, uint32_t nq) {
+    if (o.gate == B200SV_OP_SKIP) return GateDesc{};
+    if (o.gate == B200SV_OP_MATRIX)
+        return compile_matrix(o.matrix.data(), o.wires.data(), (uint32_t)o.wires.size(), inverse, nq);
+    return compile_gate(o.gate, o.wires.data(), (uint32_t)o.wires.size(), inverse, o.params.data(),
+                        (uint32_t)o.params.size(), nq);
+}
+
+// ---- observables ---------------------------------------------------------------
+struct FactorRec {
+    bool named;
+    uint32_t gate;
+    std::vector<uint32_t> wires;
+    std::vector<cd> matrix;
+};
+struct TermRec {
+    double coeff;
+    std::vector<FactorRec> f;
+    bool is_pauli = false;
+    PauliWord word;
+};
+struct ObsRec {
+    std::vector<TermRec> terms;
+    bool all_pauli() const {
+        for (auto &t : terms)
+            if (!t.is_pauli) return false;
+        return true;
+    }
+};
+
+ObsRec read_obs(const b200sv_observable &o, uint32_t nq, int dtype) {
+    ObsRec r;
+    need(o.nterms == 0 || o.terms, "observable terms pointer is NULL");
+    for (uint32_t t = 0; t < o.nterms; ++t) {
+        const b200sv_term &bt = o.terms[t];
+        need(bt.nfactors == 0 || bt.factors, "observable factors pointer is NULL");
+        TermRec tr;
+        tr.coeff = bt.coeff;
+        tr.is_pauli = true;
+        std::vector<uint32_t> seen;
+        for (uint32_t f = 0; f < bt.nfactors; ++f) {
+            const b200sv_factor &bf = bt.factors[f];
+            need(bf.nwires == 0 || bf.wires, "observable wires pointer is NULL");
+            FactorRec fr;
+            fr.named = bf.kind == B200SV_FACTOR_NAMED;
+            fr.gate = bf.gate;
+            fr.wires.assign(bf.wires, bf.wires + bf.nwires);
+            check_wires(fr.wires.data(), (uint32_t)fr.wires.size(), nq, "observable");
+            for (auto w : fr.wires) {
+                if (std::find(seen.begin(), seen.end(), w) != seen.end())
+                    throw ArgError("All wires in observables must be disjoint.");
+                seen.push_back(w);
+            }
+            if (!fr.named) {
+                need(bf.matrix != nullptr, "Hermitian observable without matrix");
+                need(bf.nwires > 0 && bf.nwires <= 11, "Hermitian observable needs 1..11 wires");
+                const size_t d = size_t(1) << bf.nwires;
+                fr.matrix = read_matrix(bf.matrix, d * d, dtype);
+                tr.is_pauli = false;
+            } else {
+                need(fr.gate < kNumGates, "unknown observable name");
+                const bool pauli = fr.gate <= 3 && fr.wires.size() == 1;
+                if (!pauli) tr.is_pauli = false;
+                if (pauli) {
+                    const uint64_t bit = uint64_t(1) << bitpos(fr.wires[0], nq);
+                    if (fr.gate == 1) tr.word.xmask |= bit;
+                    if (fr.gate == 2) {
+                        tr.word.xmask |= bit;
+                        tr.word.zmask |= bit;
+                        tr.word.ny++;
+                    }
+                    if (fr.gate == 3) tr.word.zmask |= bit;
+                }
+            }
+            tr.f.push_back(std::move(fr));
+        }
+        r.terms.push_back(std::move(tr));
+    }
+    return r;
+}
+
+void apply_factor(b200sv_state *h, void *state, const FactorRec &f) {
+    GateDesc g = f.named ? compile_gate(f.gate, f.wires.data(), (uint32_t)f.wires.size(), false, nullptr, 0, h->nq)
+                         : compile_matrix(f.matrix.data(), f.wires.data(), (uint32_t)f.wires.size(), false, h->nq);
+    void *s[1] = {state};
+    apply_desc(h, s, 1, g);
+}
+
+// out = O psi (observable applied out of place); tmp is a second work buffer
+void apply_observable(b200sv_state *h, const ObsRec &o, const void *psi, void *out, void *tmp) {
+    const cudaStream_t st = h->stream();
+    const bool single = o.terms.size() == 1 && o.terms[0].coeff == 1.0;
+    if (single) {
+        B200SV_CUDA(cudaMemcpyAsync(out, psi, h->state_bytes(), cudaMemcpyDeviceToDevice, st));
+        for (auto &f : o.terms[0].f) apply_factor(h, out, f);
+        return;
+    }
+    B200SV_CUDA(cudaMemsetAsync(out, 0, h->state_bytes(), st));
+    for (auto &t : o.terms) {
+        if (t.is_pauli) {
+            if (h->dtype == B200SV_C64) axpy_pauli<float>(out, psi, h->nq, t.word, t.coeff, st);
+            else axpy_pauli<double>(out, psi, h->nq, t.word, t.coeff, st);
+        } else {
+            B200SV_CUDA(cudaMemcpyAsync(tmp, psi, h->state_bytes(), cudaMemcpyDeviceToDevice, st));
+            for (auto &f : t.f) apply_factor(h, tmp, f);
+            if (h->dtype == B200SV_C64) axpy<float>(out, tmp, h->nq, t.coeff, st);
+            else axpy<double>(out, tmp, h->nq, t.coeff, st);
+        }
+    }
+}
+
+// per-term Pauli values of an all-Pauli observable (host vector, term order)
+std::vector<double> pauli_term_values(b200sv_state *h, const void *psi, const std::vector<PauliWord> &words) {
+    const cudaStream_t st = h->stream();
+    std::vector<double> vals(words.size(), 0.0);
+    // group by X mask, at most 32 per launch, results into d_small in order
+    std::vector<size_t> order(words.size());
+    for (size_t i = 0; i < order.size(); ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) { return words[a].xmask < words[b].xmask; });
+    size_t done = 0;
+    std::vector<size_t> placed;
+    while (done < order.size()) {
+        size_t batch = 0;
+        std::vector<std::pair<size_t, size_t>> slots;  // (term index, d_small slot)
+        while (done < order.size() && batch < kSmall) {
+            size_t j = done;
+            const uint64_t xm = words[order[j]].xmask;
+            std::vector<PauliWord> grp;
+            while (j < order.size() && words[order[j]].xmask == xm && grp.size() < 32) grp.push_back(words[order[j++]]);
+            if (batch + grp.size() > kSmall) break;
+            if (h->dtype == B200SV_C64)
+                reduce_pauli_group<float>(psi, h->nq, grp.data(), (int)grp.size(), h->d_partials, h->d_small + batch, st);
+            else
+                reduce_pauli_group<double>(psi, h->nq, grp.data(), (int)grp.size(), h->d_partials, h->d_small + batch, st);
+            for (size_t q = 0; q < grp.size(); ++q) slots.emplace_back(order[done + q], batch + q);
+            batch += grp.size();
+            done = j;
+        }
+        B200SV_CUDA(cudaMemcpyAsync(h->h_small, h->d_small, batch * sizeof(double), cudaMemcpyDeviceToHost, st));
+        B200SV_CUDA(cudaStreamSynchronize(st));
+        for (auto &s : slots) vals[s.first] = h->h_small[s.second];
+    }
+    return vals;
+}
+
+double read_small(b200sv_state *h, size_t i) {
+    B200SV_CUDA(cudaMemcpyAsync(h->h_small, h->d_small, (i + 1) * sizeof(double), cudaMemcpyDeviceToHost, h->stream()));
+    B200SV_CUDA(cudaStreamSynchronize(h->stream()));
+    return h->h_small[i];
+}
+
+double norm2_of(b200sv_state *h, const void *a) {
+    if (h->dtype == B200SV_C64) reduce_norm2<float>(a, h->nq, h->d_partials, h->d_small, h->stream());
+    else reduce_norm2<double>(a, h->nq, h->d_partials, h->d_small, h->stream());
+    return read_small(h, 0);
+}
+
+void inner_of(b200sv_state *h, const void *bra, const void *ket, double *re, double *im) {
+    if (h->dtype == B200SV_C64) reduce_inner<float>(bra, ket, h->nq, h->d_partials, h->d_small, h->stream());
+    else reduce_inner<double>(bra, ket, h->nq, h->d_partials, h->d_small, h->stream());
+    read_small(h, 1);
+    *re = h->h_small[0];
+    *im = h->h_small[1];
+}
+
+double expval_impl(b200sv_state *h, const ObsRec &o) {
+    if (o.terms.empty()) return 0.0;
+    if (o.all_pauli()) {
+        std::vector<PauliWord> words;
+        for (auto &t : o.terms) words.push_back(t.word);
+        auto v = pauli_term_values(h, h->d_state, words);
+        double s = 0.0;
+        for (size_t i = 0; i < v.size(); ++i) s += o.terms[i].coeff * v[i];
+        return s;
+    }
+    if (o.terms.size() == 1 && o.terms[0].f.size() == 1 && !o.terms[0].f[0].named &&
+        o.terms[0].f[0].wires.size() <= 4) {
+        const FactorRec &f = o.terms[0].f[0];
+        GateDesc g = compile_matrix(f.matrix.data(), f.wires.data(), (uint32_t)f.wires.size(), false, h->nq);
+        ensure_matrix(h, h->amp_bytes() * g.m.size());
+        if (h->dtype == B200SV_C64)
+            reduce_dense_expval<float>(h->d_state, h->nq, g, h->d_matrix, h->d_partials, h->d_small, h->stream());
+        else
+            reduce_dense_expval<double>(h->d_state, h->nq, g, h->d_matrix, h->d_partials, h->d_small, h->stream());
+        return o.terms[0].coeff * read_small(h, 0);
+    }
+    void *out = scratch(h, 0);
+    void *tmp = o.terms.size() > 1 ? scratch(h, 1) : nullptr;
+    apply_observable(h, o, h->d_state, out, tmp);
+    double re, im;
+    inner_of(h, h->d_state, out, &re, &im);
+    return re;
+}
+
+double var_impl(b200sv_state *h, const ObsRec &o) {
+    if (o.terms.size() == 1 && o.terms[0].is_pauli) {
+        const double c = o.terms[0].coeff;
+        auto v = pauli_term_values(h, h->d_state, {o.terms[0].word});
+        const double n2 = norm2_of(h, h->d_state);
+        return c * c * n2 - (c * v[0]) * (c * v[0]);
+    }
+    void *out = scratch(h, 0);
+    void *tmp = o.terms.size() > 1 ? scratch(h, 1) : nullptr;
+    apply_observable(h, o, h->d_state, out, tmp);
+    const double ms = norm2_of(h, out);
+    double re, im;
+    inner_of(h, h->d_state, out, &re, &im);
+    return ms - re * re;
+}
+
+void check_handle(b200sv_state *h) { need(h != nullptr, "NULL state handle"); }
+
+}  // namespace
+
+int b200sv::run_guarded(const std::function<void()> &f) { return guard(f); }
+
+// =============================================================================
+extern "C" {
+
+const char *b200sv_last_error(void) { return g_last_error.c_str(); }
+int b200sv_version(void) { return 100; }
+
+int b200sv_device_count(int *count) {
+    return guard([&] {
+        need(count != nullptr, "NULL output");
+        int n = 0;
+        if (cudaGetDeviceCount(&n) != cudaSuccess) {
+            cudaGetLastError();
+            n = 0;
+        }
+        *count = n;
+    });
+}
+
+int b200sv_create(uint32_t num_qubits, int dtype, b200sv_handle *out) {
+    return guard([&] {
+        need(out != nullptr, "NULL output handle");
+        need(num_qubits >= 1 && num_qubits <= 36, "number of qubits must be in [1, 36]");
+        need(dtype == B200SV_C64 || dtype == B200SV_C128, "dtype must be B200SV_C64 or B200SV_C128");
+        int ndev = 0;
+        if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+            cudaGetLastError();
+            throw CudaError("no CUDA device is available (libb200sv has no CPU path)");
+        }
+        auto h = std::make_unique<b200sv_state>();
+        h->nq = num_qubits;
+        h->dtype = dtype;
+        B200SV_CUDA(cudaGetDevice(&h->device));
+        try {
+            B200SV_CUDA(cudaStreamCreateWithFlags(&h->own, cudaStreamNonBlocking));
+            B200SV_CUDA(cudaMalloc(&h->d_state, h->state_bytes()));
+            B200SV_CUDA(cudaMalloc(&h->d_partials, kPartialsCapacity * sizeof(double)));
+            B200SV_CUDA(cudaMalloc(&h->d_small, kSmall * sizeof(double)));
+            B200SV_CUDA(cudaMallocHost(&h->h_small, kSmall * sizeof(double)));
+            if (dtype == B200SV_C64) set_basis<float>(h->d_state, num_qubits, 0, h->own);
+            else set_basis<double>(h->d_state, num_qubits, 0, h->own);
+        } catch (...) {
+            if (h->d_state) cudaFree(h->d_state);
+            if (h->d_partials) cudaFree(h->d_partials);
+            if (h->d_small) cudaFree(h->d_small);
+            if (h->h_small) cudaFreeHost(h->h_small);
+            if (h->own) cudaStreamDestroy(h->own);
+            throw;
+        }
+        *out = h.release();
+    });
+}
+
+int b200sv_destroy(b200sv_handle h) {
+    return guard([&] {
+        if (!h) return;
+        DeviceGuard dg(h->device);
+        cudaStreamSynchronize(h->stream());
+        cudaFree(h->d_state);
+        cudaFree(h->d_partials);
+        cudaFree(h->d_small);
+        cudaFreeHost(h->h_small);
+        if (h->d_matrix) cudaFree(h->d_matrix);
+        for (auto &s : h->d_scratch)
+            if (s) cudaFree(s);
+        cudaStreamDestroy(h->own);
+        delete h;
+    });
+}
+
+int b200sv_num_qubits(b200sv_handle h, uint32_t *out) {
+    return guard([&] {
+        check_handle(h);
+        need(out != nullptr, "NULL output");
+        *out = h->nq;
+    });
+}
+int b200sv_dtype(b200sv_handle h, int *out) {
+    return guard([&] {
+        check_handle(h);
+        need(out != nullptr, "NULL output");
+        *out = h->dtype;
+    });
+}
+int b200sv_set_stream(b200sv_handle h, void *s) {
+    return guard([&] {
+        check_handle(h);
+        h->ext = static_cast<cudaStream_t>(s);
+    });
+}
+int b200sv_synchronize(b200sv_handle h) {
+    return guard([&] {
+        check_handle(h);
+        DeviceGuard dg(h->device);
+        B200SV_CUDA(cudaStreamSynchronize(h->stream()));
+    });
+}
+int b200sv_device_ptr(b200sv_handle h, void **out) {
+    return guard([&] {
+        check_handle(h);
+        need(out != nullptr, "NULL output");
+        *out = h->d_state;
+    });
+}
+int b200sv_upload(b200sv_handle h, const void *host, uint64_t length) {
+    return guard([&] {
+        check_handle(h);
+        need(host != nullptr, "NULL host buffer");
+        need(length == (uint64_t(1) << h->nq), "length must equal 2^num_qubits");
+        DeviceGuard dg(h->device);
+        B200SV_CUDA(cudaMemcpyAsync(h->d_state, host, h->state_bytes(), cudaMemcpyHostToDevice, h->stream()));
+        B200SV_CUDA(cudaStreamSynchronize(h->stream()));
+    });
+}
+int b200sv_download(b200sv_handle h, void *host, uint64_t length) {
+    return guard([&] {
+        check_handle(h);
+        need(host != nullptr, "NULL host buffer");
+        need(length == (uint64_t(1) << h->nq), "length must equal 2^num_qubits");
+        DeviceGuard dg(h->device);
+        B200SV_CUDA(cudaMemcpyAsync(host, h->d_state, h->state_bytes(), cudaMemcpyDeviceToHost, h->stream()));
+        B200SV_CUDA(cudaStreamSynchronize(h->stream()));
+    });
+}
+int b200sv_copy(b200sv_handle dst, b200sv_handle src) {
+    return guard([&] {
+        check_handle(dst);
+        check_handle(src);
+        need(dst->nq == src->nq && dst->dtype == src->dtype, "copy needs equal size and dtype");
+        DeviceGuard dg(dst->device);
+        if (src->stream() != dst->stream()) B200SV_CUDA(cudaStreamSynchronize(src->stream()));
+        B200SV_CUDA(cudaMemcpyAsync(dst->d_state, src->d_state, dst->state_bytes(), cudaMemcpyDeviceToDevice,
+                                    dst->stream()));
+    });
+}
+int b200sv_set_basis_state(b200sv_handle h, uint64_t index) {
+    return guard([&] {
+        check_handle(h);
+        need(index < (uint64_t(1) << h->nq), "basis index out of range");
+        DeviceGuard dg(h->device);
+        if (h->dtype == B200SV_C64) set_basis<float>(h->d_state, h->nq, index, h->stream());
+        else set_basis<double>(h->d_state, h->nq, index, h->stream());
+    });
+}
+
+int b200sv_apply_gate(b200sv_handle h, uint32_t gate, const uint32_t *wires, uint32_t nwires, int inverse,
+                      const double *params, uint32_t nparams) {
+    return guard([&] {
+        check_handle(h);
+        need(nwires == 0 || wires, "NULL wires");
+        need(nparams == 0 || params, "NULL params");
+        DeviceGuard dg(h->device);
+        GateDesc g = compile_gate(gate, wires, nwires, inverse != 0, params, nparams, h->nq);
+        void *s[1] = {h->d_state};
+        apply_desc(h, s, 1, g);
+    });
+}
+
+int b200sv_apply_matrix(b200sv_handle h, const void *matrix, const uint32_t *wires, uint32_t nwires, int inverse) {
+    return guard([&] {
+        check_handle(h);
+        need(matrix != nullptr && wires != nullptr, "NULL matrix or wires");
+        need(nwires >= 1 && nwires <= 11, "applyMatrix supports 1..11 wires");
+        DeviceGuard dg(h->device);
+        const size_t d = size_t(1) << nwires;
+        auto m = read_matrix(matrix, d * d, h->dtype);
+        GateDesc g = compile_matrix(m.data(), wires, nwires, inverse != 0, h->nq);
+        void *s[1] = {h->d_state};
+        apply_desc(h, s, 1, g);
+    });
+}
+
+int b200sv_apply_ops(b200sv_handle h, const b200sv_op *ops, uint32_t nops) {
+    return guard([&] {
+        check_handle(h);
+        DeviceGuard dg(h->device);
+        auto rec = read_ops(ops, nops, h->dtype);
+        std::vector<GateDesc> descs;
+        descs.reserve(rec.size());
+        for (auto &o : rec) descs.push_back(compile_op(o, o.inverse, h->nq));  // validate all first
+        void *s[1] = {h->d_state};
+        for (auto &g : descs) apply_desc(h, s, 1, g);
+    });
+}
+
+int b200sv_apply_generator(b200sv_handle h, uint32_t generator, const uint32_t *wires, uint32_t nwires, int adj,
+                           double *scale) {
+    (void)adj;  // generators are Hermitian: adj does not change them (GateImplementationsLM.hpp:1355-1639)
+    return guard([&] {
+        check_handle(h);
+        need(wires != nullptr && scale != nullptr, "NULL wires or scale");
+        DeviceGuard dg(h->device);
+        GateDesc g = compile_generator(generator, wires, nwires, h->nq, scale);
+        void *s[1] = {h->d_state};
+        apply_desc(h, s, 1, g);
+    });
+}
+
+int b200sv_probs_device(b200sv_handle h, const uint32_t *wires, uint32_t nwires, double *out_device) {
+    return guard([&] {
+        check_handle(h);
+        need(out_device != nullptr, "NULL output");
+        DeviceGuard dg(h->device);
+        std::vector<uint32_t> bits;
+        if (nwires == 0) {
+            for (uint32_t w = 0; w < h->nq; ++w) bits.push_back(bitpos(w, h->nq));
+        } else {
+            need(wires != nullptr, "NULL wires");
+            check_wires(wires, nwires, h->nq, "probs");
+            for (uint32_t j = 0; j < nwires; ++j) bits.push_back(bitpos(wires[j], h->nq));
+        }
+        if (h->dtype == B200SV_C64)
+            reduce_probs<float>(h->d_state, h->nq, bits, h->d_partials, kPartialsCapacity, out_device, h->stream());
+        else
+            reduce_probs<double>(h->d_state, h->nq, bits, h->d_partials, kPartialsCapacity, out_device, h->stream());
+    });
+}
+
+int b200sv_probs(b200sv_handle h, const uint32_t *wires, uint32_t nwires, double *out) {
+    return guard([&] {
+        check_handle(h);
+        need(out != nullptr, "NULL output");
+        DeviceGuard dg(h->device);
+        const uint32_t k = nwires == 0 ? h->nq : nwires;
+        const size_t count = size_t(1) << k;
+        double *d_out = nullptr;
+        B200SV_CUDA(cudaMallocAsync((void **)&d_out, count * sizeof(double), h->stream()));
+        int rc = b200sv_probs_device(h, wires, nwires, d_out);
+        if (rc != B200SV_OK) {
+            std::string msg = g_last_error;
+            cudaFreeAsync(d_out, h->stream());
+            throw ArgError(msg);
+        }
+        B200SV_CUDA(cudaMemcpyAsync(out, d_out, count * sizeof(double), cudaMemcpyDeviceToHost, h->stream()));
+        B200SV_CUDA(cudaFreeAsync(d_out, h->stream()));
+        B200SV_CUDA(cudaStreamSynchronize(h->stream()));
+    });
+}
+
+int b200sv_expval(b200sv_handle h, const b200sv_observable *obs, double *out) {
+    return guard([&] {
+        check_handle(h);
+        need(obs != nullptr && out != nullptr, "NULL observable or output");
+        DeviceGuard dg(h->device);
+        *out = expval_impl(h, read_obs(*obs, h->nq, h->dtype));
+    });
+}
+
+int b200sv_var(b200sv_handle h, const b200sv_observable *obs, double *out) {
+    return guard([&] {
+        check_handle(h);
+        need(obs != nullptr && out != nullptr, "NULL observable or output");
+        DeviceGuard dg(h->device);
+        *out = var_impl(h, read_obs(*obs, h->nq, h->dtype));
+    });
+}
+
+int b200sv_expval_pauli(b200sv_handle h, uint32_t nterms, const double *coeffs, const uint32_t *offsets,
+                        const uint32_t *wires, const char *paulis, double *out_terms, double *out_sum) {
+    return guard([&] {
+        check_handle(h);
+        need(nterms == 0 || (offsets && coeffs), "NULL term arrays");
+        DeviceGuard dg(h->device);
+        std::vector<PauliWord> words(nterms);
+        for (uint32_t t = 0; t < nterms; ++t) {
+            need(offsets[t] <= offsets[t + 1], "Pauli offsets must be non-decreasing");
+            uint64_t used = 0;
+            for (uint32_t q = offsets[t]; q < offsets[t + 1]; ++q) {
+                need(wires && paulis, "NULL wires or paulis");
+                need(wires[q] < h->nq, "Pauli wire out of range");
+                const uint64_t bit = uint64_t(1) << bitpos(wires[q], h->nq);
+                need(!(used & bit), "All wires in observables must be disjoint.");
+                used |= bit;
+                switch (paulis[q]) {
+                case 'I': break;
+                case 'X': words[t].xmask |= bit; break;
+                case 'Y': words[t].xmask |= bit; words[t].zmask |= bit; words[t].ny++; break;
+                case 'Z': words[t].zmask |= bit; break;
+                default: throw ArgError("Pauli letters must be I, X, Y or Z");
+                }
+            }
+        }
+        auto v = pauli_term_values(h, h->d_state, words);
+        double s = 0.0;
+        for (uint32_t t = 0; t < nterms; ++t) {
+            if (out_terms) out_terms[t] = v[t];
+            s += coeffs[t] * v[t];
+        }
+        if (out_sum) *out_sum = s;
+    });
+}
+
+int b200sv_inner_product(b200sv_handle bra, b200sv_handle ket, double *re, double *im) {
+    return guard([&] {
+        check_handle(bra);
+        check_handle(ket);
+        need(re && im, "NULL output");
+        need(bra->nq == ket->nq && bra->dtype == ket->dtype, "inner product needs equal size and dtype");
+        DeviceGuard dg(ket->device);
+        if (bra->stream() != ket->stream()) B200SV_CUDA(cudaStreamSynchronize(bra->stream()));
+        inner_of(ket, bra->d_state, ket->d_state, re, im);
+    });
+}
+
+int b200sv_norm2(b200sv_handle h, double *out) {
+    return guard([&] {
+        check_handle(h);
+        need(out != nullptr, "NULL output");
+        DeviceGuard dg(h->device);
+        *out = norm2_of(h, h->d_state);
+    });
+}
+
+static void sample_impl(b200sv_state *h, uint64_t nshots, const double *uniforms, uint64_t seed, uint64_t *idx_host) {
+    const cudaStream_t st = h->stream();
+    const uint64_t N = uint64_t(1) << h->nq;
+    const size_t ws = cdf_workspace_doubles(N);
+    double *cdf = nullptr, *work = nullptr, *u = nullptr;
+    uint64_t *idx = nullptr;
+    B200SV_CUDA(cudaMallocAsync((void **)&cdf, N * sizeof(double), st));
+    B200SV_CUDA(cudaMallocAsync((void **)&work, ws * sizeof(double), st));
+    B200SV_CUDA(cudaMallocAsync((void **)&u, std::max<uint64_t>(1, nshots) * sizeof(double), st));
+    B200SV_CUDA(cudaMallocAsync((void **)&idx, std::max<uint64_t>(1, nshots) * sizeof(uint64_t), st));
+    if (h->dtype == B200SV_C64) build_cdf<float>(h->d_state, h->nq, cdf, work, st);
+    else build_cdf<double>(h->d_state, h->nq, cdf, work, st);
+    if (uniforms) B200SV_CUDA(cudaMemcpyAsync(u, uniforms, nshots * sizeof(double), cudaMemcpyHostToDevice, st));
+    else philox_uniforms(u, nshots, seed, st);
+    sample_from_cdf(cdf, N, u, nshots, idx, st);
+    if (nshots) B200SV_CUDA(cudaMemcpyAsync(idx_host, idx, nshots * sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
+    cudaFreeAsync(cdf, st);
+    cudaFreeAsync(work, st);
+    cudaFreeAsync(u, st);
+    cudaFreeAsync(idx, st);
+    B200SV_CUDA(cudaStreamSynchronize(st));
+}
+
+int b200sv_sample(b200sv_handle h, uint64_t nshots, const double *uniforms, uint64_t seed, uint64_t *idx_out) {
+    return guard([&] {
+        check_handle(h);
+        need(nshots == 0 || idx_out != nullptr, "NULL output");
+        DeviceGuard dg(h->device);
+        sample_impl(h, nshots, uniforms, seed, idx_out);
+    });
+}
+
+int b200sv_sample_bits(b200sv_handle h, uint64_t nshots, const double *uniforms, uint64_t seed, uint64_t *bits_out) {
+    return guard([&] {
+        check_handle(h);
+        need(nshots == 0 || bits_out != nullptr, "NULL output");
+        DeviceGuard dg(h->device);
+        std::vector<uint64_t> idx(nshots);
+        sample_impl(h, nshots, uniforms, seed, idx.data());
+        const uint32_t n = h->nq;
+        // bits MSB (wire 0) first, as MeasurementsLQubit.hpp:549-554
+        for (uint64_t s = 0; s < nshots; ++s)
+            for (uint32_t j = 0; j < n; ++j) bits_out[s * n + (n - 1 - j)] = (idx[s] >> j) & 1u;
+    });
+}
+
+// ---- adjoint Jacobian: LQ/algorithms/AdjointJacobianLQubit.hpp:212-335 --------
+int b200sv_adjoint_jacobian(b200sv_handle psi, const b200sv_op *ops, uint32_t nops, const b200sv_observable *obs,
+                            uint32_t nobs, const uint64_t *trainable, uint32_t ntp, int apply_operations,
+                            double *jac) {
+    return guard([&] {
+        check_handle(psi);
+        need(nobs == 0 || obs != nullptr, "NULL observables");
+        need(ntp == 0 || trainable != nullptr, "NULL trainable parameter list");
+        need(ntp == 0 || nobs == 0 || jac != nullptr, "NULL jacobian output");
+        if (ntp == 0) return;  // nothing to do (AdjointJacobianLQubit.hpp:229-231)
+        for (uint32_t i = 1; i < ntp; ++i) need(trainable[i - 1] < trainable[i], "trainable parameters must be sorted");
+        DeviceGuard dg(psi->device);
+        b200sv_state *h = psi;
+        const cudaStream_t st = h->stream();
+        auto rec = read_ops(ops, nops, h->dtype);
+        std::vector<ObsRec> orec;
+        for (uint32_t o = 0; o < nobs; ++o) orec.push_back(read_obs(obs[o], h->nq, h->dtype));
+        size_t num_param_ops = 0;
+        for (auto &o : rec)
+            if (!o.params.empty()) ++num_param_ops;
+
+        // workspace: lambda, one bra per observable, a tmp, the jacobian [tp][obs]
+        std::vector<void *> bufs;
+        auto alloc_state = [&]() {
+            void *p = nullptr;
+            B200SV_CUDA(cudaMallocAsync(&p, h->state_bytes(), st));
+            bufs.push_back(p);
+            return p;
+        };
+        double *d_jac = nullptr;
+        struct Cleanup {
+            std::vector<void *> &b;
+            double *&j;
+            cudaStream_t s;
+            ~Cleanup() {
+                for (auto p : b) cudaFreeAsync(p, s);
+                if (j) cudaFreeAsync(j, s);
+                cudaStreamSynchronize(s);
+            }
+        } cleanup{bufs, d_jac, st};
+        void *lambda = alloc_state();
+        std::vector<void *> bras;
+        for (uint32_t o = 0; o < nobs; ++o) bras.push_back(alloc_state());
+        bool need_tmp = false;
+        for (auto &o : orec) need_tmp |= o.terms.size() > 1;
+        void *tmp = need_tmp ? alloc_state() : nullptr;
+        B200SV_CUDA(cudaMallocAsync((void **)&d_jac, sizeof(double) * ntp * std::max<uint32_t>(1, nobs), st));
+        B200SV_CUDA(cudaMemsetAsync(d_jac, 0, sizeof(double) * ntp * std::max<uint32_t>(1, nobs), st));
+
+        B200SV_CUDA(cudaMemcpyAsync(lambda, h->d_state, h->state_bytes(), cudaMemcpyDeviceToDevice, st));
+        if (apply_operations) {
+            for (auto &o : rec) {
+                void *s[1] = {lambda};
+                apply_desc(h, s, 1, compile_op(o, o.inverse, h->nq));
+            }
+        }
+        for (uint32_t o = 0; o < nobs; ++o) apply_observable(h, orec[o], lambda, bras[o], tmp);
+
+        int64_t tp_pos = (int64_t)ntp - 1;  // reverse iterator over trainable
+        int64_t trainable_number = (int64_t)ntp - 1;
+        int64_t current_param_idx = (int64_t)num_param_ops - 1;
+        for (int64_t op_idx = (int64_t)rec.size() - 1; op_idx >= 0; --op_idx) {
+            const OpRec &op = rec[op_idx];
+            if (op.params.size() > 1)
+                throw ArgError("The operation is not supported using the adjoint differentiation method");
+            if (op.gate == B200SV_OP_SKIP) continue;
+            if (tp_pos < 0) break;
+            if (!op.params.empty()) {
+                if ((uint64_t)current_param_idx == trainable[tp_pos]) {
+                    const int gen = generator_of_gate(op.gate);
+                    if (gen < 0)
+                        throw ArgError("The operation is not supported using the adjoint differentiation method");
+                    double sc = 0.0;
+                    GateDesc G = compile_generator((uint32_t)gen, op.wires.data(), (uint32_t)op.wires.size(), h->nq, &sc);
+                    const double scaling = sc * (op.inverse ? -1.0 : 1.0);
+                    for (uint32_t o0 = 0; o0 < nobs; o0 += 16) {
+                        const int cnt = (int)std::min<uint32_t>(16, nobs - o0);
+                        double *dst = d_jac + (size_t)trainable_number * nobs + o0;
+                        if (h->dtype == B200SV_C64)
+                            reduce_generator_inner<float>(bras.data() + o0, cnt, lambda, h->nq, G, -2.0 * scaling,
+                                                          h->d_partials, dst, 1, st);
+                        else
+                            reduce_generator_inner<double>(bras.data() + o0, cnt, lambda, h->nq, G, -2.0 * scaling,
+                                                           h->d_partials, dst, 1, st);
+                    }
+                    --trainable_number;
+                    --tp_pos;
+                }
+                --current_param_idx;
+            }
+            GateDesc adj = compile_op(op, !op.inverse, h->nq);
+            void *s[1] = {lambda};
+            apply_desc(h, s, 1, adj);
+            apply_desc_multi(h, bras, adj);
+        }
+        std::vector<double> jt((size_t)ntp * nobs);
+        if (!jt.empty())
+            B200SV_CUDA(cudaMemcpyAsync(jt.data(), d_jac, jt.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+        B200SV_CUDA(cudaStreamSynchronize(st));
+        // [tp][obs] -> [obs][tp]  (AdjointJacobianLQubit.hpp:331-334)
+        for (uint32_t p = 0; p < ntp; ++p)
+            for (uint32_t o = 0; o < nobs; ++o) jac[(size_t)o * ntp + p] = jt[(size_t)p * nobs + o];
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,97 @@
+// sv_internal.hpp — declarations shared by the .cu files of libb200sv (not part of the ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <complex>
+#include <cstdint>
+#include <functional>
+#include <string>
+#include <vector>
+
+#include "gate_compiler.hpp"
+
+namespace b200sv {
+
+struct CudaError : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+struct AllocError : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+
+void cuda_check(cudaError_t e, const char *what);
+
+// Runs f, maps exceptions to a b200sv_status code and records the message for
+// b200sv_last_error() (defined in sv_capi.cu, shared by every entry point).
+int run_guarded(const std::function<void()> &f);
+#define B200SV_CUDA(x) ::b200sv::cuda_check((x), #x)
+
+// Number of SMs of the current device (cached per device).
+int sm_count();
+
+constexpr int kMaxStatesPerLaunch = 32;
+
+// Apply a compiled gate to `nstates` states of 2^nq amplitudes of precision R
+// (R = float or double).  `dev_scratch` must hold 4^k complex<R> when the
+// descriptor is Dense with k >= 4 (used for the matrix); it is written with a
+// stream-ordered copy before the launch.
+template <typename R>
+void launch_gate(void *const *states, int nstates, uint32_t nq, const GateDesc &g,
+                 void *dev_matrix_scratch, cudaStream_t st);
+
+// ---- reductions (sv_reduce.cu) -------------------------------------------
+// All reductions are two-pass and deterministic: per-block partials into
+// `partials` (kPartialsCapacity doubles), then one block finalises into a
+// device array.  Results stay on the device unless noted.
+constexpr int kMaxRedBlocks = 1184;     // 148 SMs x 8
+constexpr size_t kPartialsCapacity = size_t(kMaxRedBlocks) * 64;
+
+// out_dev[0] = ||a||^2
+template <typename R>
+void reduce_norm2(const void *a, uint32_t nq, double *partials, double *out_dev, cudaStream_t st);
+// out_dev[0..1] = <bra|ket> (re, im)
+template <typename R>
+void reduce_inner(const void *bra, const void *ket, uint32_t nq, double *partials, double *out_dev,
+                  cudaStream_t st);
+// Pauli words sharing one X-mask.  out_dev[t] = <psi|P_t|psi> for t < nterms (<= 32).
+struct PauliWord {
+    uint64_t xmask = 0, zmask = 0;
+    int ny = 0;  // number of Y factors (phase i^ny)
+};
+template <typename R>
+void reduce_pauli_group(const void *psi, uint32_t nq, const PauliWord *terms, int nterms,
+                        double *partials, double *out_dev, cudaStream_t st);
+// out_dev[0] = Re <psi| M |psi> for a dense Hermitian M on k <= 4 bits (matrix on device).
+template <typename R>
+void reduce_dense_expval(const void *psi, uint32_t nq, const GateDesc &g, const void *dev_matrix,
+                         double *partials, double *out_dev, cudaStream_t st);
+// out_dev[o * out_stride] = alpha * Im <bra_o| G |ket>, o < nbra (<= 16).
+template <typename R>
+void reduce_generator_inner(void *const *bras, int nbra, const void *ket, uint32_t nq,
+                            const GateDesc &g, double alpha, double *partials, double *out_dev,
+                            int out_stride, cudaStream_t st);
+// Marginal probabilities over `bits` (bits[0] = MSB of the output index).
+template <typename R>
+void reduce_probs(const void *psi, uint32_t nq, const std::vector<uint32_t> &bits, double *partials,
+                  size_t partials_cap, double *out_dev, cudaStream_t st);
+
+// ---- elementwise helpers (sv_reduce.cu) ----------------------------------
+template <typename R> void set_basis(void *psi, uint32_t nq, uint64_t index, cudaStream_t st);
+// acc += c * P psi for one Pauli word (no aliasing between acc and psi)
+template <typename R>
+void axpy_pauli(void *acc, const void *psi, uint32_t nq, const PauliWord &w, double c,
+                cudaStream_t st);
+// acc += c * x
+template <typename R> void axpy(void *acc, const void *x, uint32_t nq, double c, cudaStream_t st);
+
+// ---- sampling (sv_sample.cu) ---------------------------------------------
+// Number of doubles of workspace needed besides the N-double CDF.
+size_t cdf_workspace_doubles(uint64_t N);
+template <typename R>
+void build_cdf(const void *psi, uint32_t nq, double *cdf, double *work, cudaStream_t st);
+void philox_uniforms(double *u, uint64_t n, uint64_t seed, cudaStream_t st);
+void sample_from_cdf(const double *cdf, uint64_t N, const double *u, uint64_t nshots, uint64_t *idx,
+                     cudaStream_t st);
+
+}  // namespace b200sv

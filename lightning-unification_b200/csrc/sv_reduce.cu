@@ -1,0 +1,548 @@
+// sv_reduce.cu — read-only FP64 reductions over a state vector.
+//
+// The reference computes every expectation value by copying the state, applying
+// the observable and taking innerProdC (LQ/measurements/MeasurementsLQubit.hpp:145-180,
+// :248-265; LQ/utils/LinearAlgebra.hpp:151-213): three full passes per term.
+// Here a Pauli word is evaluated in one read-only pass (all words sharing an
+// X-mask together), a Hermitian matrix as v^dagger M v per group, and the
+// adjoint method's -2 Im<H lambda| G |mu> (LQ/algorithms/AdjointJacobianLQubit.hpp:68-77,
+// :301-323) without materialising G|mu>.  All accumulators are FP64 (complex64
+// amplitudes are widened on load) and every reduction is two-pass with a fixed
+// association order, so results are reproducible.
+#include <algorithm>
+#include <vector>
+
+#include "sv_device.cuh"
+#include "sv_internal.hpp"
+
+namespace b200sv {
+namespace {
+
+constexpr int kRT = 256;  // reduction block size
+
+int red_blocks(uint64_t work) {
+    uint64_t b = (work + kRT * 4 - 1) / (kRT * 4);
+    b = std::max<uint64_t>(1, std::min<uint64_t>(b, kMaxRedBlocks));
+    return (int)b;
+}
+
+// out[v * stride] = alpha * sum_b partials[v * nb + b]  (one block per value)
+__global__ void k_finalize(const double *__restrict__ partials, int nb, double *__restrict__ out,
+                           int stride, double alpha) {
+    __shared__ double sm[32];
+    const int v = blockIdx.x;
+    double s[1] = {0.0};
+    for (int b = threadIdx.x; b < nb; b += blockDim.x) s[0] += partials[(size_t)v * nb + b];
+    block_reduce<1>(s, sm);
+    if (threadIdx.x == 0) out[(size_t)v * stride] = alpha * s[0];
+}
+
+void finalize(const double *partials, int nb, int nv, double *out, int stride, double alpha,
+              cudaStream_t st) {
+    k_finalize<<<nv, 128, 0, st>>>(partials, nb, out, stride, alpha);
+    B200SV_CUDA(cudaGetLastError());
+}
+
+template <typename R>
+__global__ void __launch_bounds__(kRT) k_norm2(const C<R> *__restrict__ a, uint64_t n, double *partials) {
+    __shared__ double sm[32];
+    double acc[1] = {0.0};
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const double2 z = widen<R>(a[i]);
+        acc[0] += z.x * z.x + z.y * z.y;
+    }
+    block_reduce<1>(acc, sm);
+    if (threadIdx.x == 0) partials[blockIdx.x] = acc[0];
+}
+
+template <typename R>
+__global__ void __launch_bounds__(kRT) k_inner(const C<R> *__restrict__ b, const C<R> *__restrict__ k,
+                                               uint64_t n, double *partials) {
+    __shared__ double sm[64];
+    double acc[2] = {0.0, 0.0};
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const double2 x = widen<R>(b[i]), y = widen<R>(k[i]);
+        acc[0] += x.x * y.x + x.y * y.y;  // Re conj(x) y
+        acc[1] += x.x * y.y - x.y * y.x;  // Im conj(x) y
+    }
+    block_reduce<2>(acc, sm);
+    if (threadIdx.x == 0) {
+        partials[blockIdx.x] = acc[0];
+        partials[gridDim.x + blockIdx.x] = acc[1];
+    }
+}
+
+// ---- Pauli words sharing an X mask -----------------------------------------
+// P|i> = i^ny (-1)^popcount(i & zmask) |i ^ xmask>  (zmask covers Z and Y factors)
+struct PauliGroupP {
+    uint64_t xmask, hb_low;  // hb_low: (1 << highest X bit) - 1, or 0 when xmask == 0
+    uint64_t npairs;
+    int nterms;
+    uint64_t zmask[32];
+    int ny[32];
+};
+template <typename R, int NT>
+__global__ void __launch_bounds__(kRT) k_pauli(const C<R> *__restrict__ a, PauliGroupP p, double *partials) {
+    __shared__ double sm[NT * 32];
+    double acc[NT];
+#pragma unroll
+    for (int t = 0; t < NT; ++t) acc[t] = 0.0;
+    for (uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < p.npairs;
+         g += (uint64_t)gridDim.x * blockDim.x) {
+        if (p.xmask == 0) {
+            const double2 z = widen<R>(a[g]);
+            const double pr = z.x * z.x + z.y * z.y;
+#pragma unroll
+            for (int t = 0; t < NT; ++t)
+                if (t < p.nterms) acc[t] += (__popcll(g & p.zmask[t]) & 1) ? -pr : pr;
+        } else {
+            const uint64_t lo = g & p.hb_low;
+            const uint64_t i = ((g ^ lo) << 1) | lo;  // highest X bit cleared
+            const uint64_t j = i ^ p.xmask;
+            const double2 vi = widen<R>(a[i]), vj = widen<R>(a[j]);
+            const double zr = vj.x * vi.x + vj.y * vi.y;  // conj(vj) vi
+            const double zi = vj.x * vi.y - vj.y * vi.x;
+#pragma unroll
+            for (int t = 0; t < NT; ++t) {
+                if (t < p.nterms) {
+                    double r;
+                    switch (p.ny[t] & 3) {
+                    case 0: r = zr; break;
+                    case 1: r = -zi; break;
+                    case 2: r = -zr; break;
+                    default: r = zi; break;
+                    }
+                    r *= 2.0;
+                    acc[t] += (__popcll(i & p.zmask[t]) & 1) ? -r : r;
+                }
+            }
+        }
+    }
+    block_reduce<NT>(acc, sm);
+    if (threadIdx.x == 0)
+        for (int t = 0; t < p.nterms; ++t) partials[(size_t)t * gridDim.x + blockIdx.x] = acc[t];
+}
+
+// ---- generator products ----------------------------------------------------
+// A generator acts on a group of 2^k rows (Dense k<=2, Diag k<=2, Pair k in {1,2,4})
+// or on single amplitudes by parity; w = G v is formed in registers.
+template <typename R> struct GenP {
+    int kind, k;
+    Insert ins;
+    uint64_t ngroups;
+    uint64_t off[16];
+    C<R> m[16];     // Dense 4x4 (k<=2) or Diag phases
+    C<R> m2[4], gamma;
+    int pa, pb;
+    uint64_t pmask;
+    C<R> pph[2];
+};
+template <typename R> struct Bras {
+    const C<R> *p[16];
+};
+template <typename R>
+__device__ __forceinline__ int gen_apply(const GenP<R> &p, uint64_t g, const C<R> *__restrict__ ket,
+                                         uint64_t &base, double2 (&w)[16]) {
+    if (p.kind == (int)Kind::Parity) {
+        base = g;
+        const double2 v = widen<R>(ket[g]);
+        const C<R> f = p.pph[__popcll(g & p.pmask) & 1];
+        w[0] = make_double2(f.x * v.x - f.y * v.y, f.x * v.y + f.y * v.x);
+        return 1;
+    }
+    base = p.ins(g);
+    const int D = 1 << p.k;
+    double2 v[16];
+    for (int r = 0; r < D; ++r) v[r] = widen<R>(ket[base + p.off[r]]);
+    if (p.kind == (int)Kind::Dense) {
+        for (int r = 0; r < D; ++r) {
+            double re = 0, im = 0;
+            for (int c = 0; c < D; ++c) {
+                const double mr = p.m[r * D + c].x, mi = p.m[r * D + c].y;
+                re += mr * v[c].x - mi * v[c].y;
+                im += mr * v[c].y + mi * v[c].x;
+            }
+            w[r] = make_double2(re, im);
+        }
+    } else if (p.kind == (int)Kind::Diag) {
+        for (int r = 0; r < D; ++r) {
+            const double mr = p.m[r].x, mi = p.m[r].y;
+            w[r] = make_double2(mr * v[r].x - mi * v[r].y, mr * v[r].y + mi * v[r].x);
+        }
+    } else {  // Pair
+        for (int r = 0; r < D; ++r) {
+            const double gr = p.gamma.x, gi = p.gamma.y;
+            w[r] = make_double2(gr * v[r].x - gi * v[r].y, gr * v[r].y + gi * v[r].x);
+        }
+        const double2 va = v[p.pa], vb = v[p.pb];
+        const C<R> *m = p.m2;
+        w[p.pa] = make_double2(m[0].x * va.x - m[0].y * va.y + m[1].x * vb.x - m[1].y * vb.y,
+                               m[0].x * va.y + m[0].y * va.x + m[1].x * vb.y + m[1].y * vb.x);
+        w[p.pb] = make_double2(m[2].x * va.x - m[2].y * va.y + m[3].x * vb.x - m[3].y * vb.y,
+                               m[2].x * va.y + m[2].y * va.x + m[3].x * vb.y + m[3].y * vb.x);
+    }
+    return D;
+}
+
+template <typename R, int NB>
+__global__ void __launch_bounds__(kRT) k_gen_inner(Bras<R> bras, int nbra, const C<R> *__restrict__ ket,
+                                                   GenP<R> p, double *partials) {
+    __shared__ double sm[NB * 32];
+    double acc[NB];
+#pragma unroll
+    for (int o = 0; o < NB; ++o) acc[o] = 0.0;
+    for (uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < p.ngroups;
+         g += (uint64_t)gridDim.x * blockDim.x) {
+        uint64_t base;
+        double2 w[16];
+        const int D = gen_apply<R>(p, g, ket, base, w);
+        for (int r = 0; r < D; ++r) {
+            const uint64_t idx = (p.kind == (int)Kind::Parity) ? base : base + p.off[r];
+#pragma unroll
+            for (int o = 0; o < NB; ++o) {
+                if (o < nbra) {
+                    const double2 b = widen<R>(bras.p[o][idx]);
+                    acc[o] += b.x * w[r].y - b.y * w[r].x;  // Im conj(b) w
+                }
+            }
+        }
+    }
+    block_reduce<NB>(acc, sm);
+    if (threadIdx.x == 0)
+        for (int o = 0; o < nbra; ++o) partials[(size_t)o * gridDim.x + blockIdx.x] = acc[o];
+}
+
+// ---- Hermitian sandwich ------------------------------------------------------
+template <typename R> struct DenseEvP {
+    Insert ins;
+    uint64_t ngroups;
+    uint64_t off[16];
+    int k;
+};
+template <typename R>
+__global__ void __launch_bounds__(kRT) k_dense_ev(const C<R> *__restrict__ a, DenseEvP<R> p,
+                                                  const C<R> *__restrict__ m, double *partials) {
+    __shared__ double sm[32];
+    double acc[1] = {0.0};
+    const int D = 1 << p.k;
+    for (uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < p.ngroups;
+         g += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t base = p.ins(g);
+        double2 v[16];
+        for (int r = 0; r < D; ++r) v[r] = widen<R>(a[base + p.off[r]]);
+        for (int r = 0; r < D; ++r) {
+            double re = 0, im = 0;
+            for (int c = 0; c < D; ++c) {
+                const C<R> x = m[r * D + c];
+                re += (double)x.x * v[c].x - (double)x.y * v[c].y;
+                im += (double)x.x * v[c].y + (double)x.y * v[c].x;
+            }
+            acc[0] += v[r].x * re + v[r].y * im;  // Re conj(v_r) (M v)_r
+        }
+    }
+    block_reduce<1>(acc, sm);
+    if (threadIdx.x == 0) partials[blockIdx.x] = acc[0];
+}
+
+// ---- marginal probabilities --------------------------------------------------
+struct ProbsP {
+    Insert others;        // inserts zeros at the measured bits
+    uint64_t nothers;
+    uint64_t binmask[64];  // bin bit (k-1-j) -> state bit bits[j]
+    int k;
+    uint64_t nbins;
+};
+__device__ __forceinline__ uint64_t deposit_bin(const ProbsP &p, uint64_t m) {
+    uint64_t o = 0;
+    for (int j = 0; j < p.k; ++j)
+        if (m & (uint64_t(1) << (p.k - 1 - j))) o |= p.binmask[j];
+    return o;
+}
+// 8 bins per block row (blockIdx.y), blocks along x split the other indices
+template <typename R>
+__global__ void __launch_bounds__(kRT) k_probs_hist(const C<R> *__restrict__ a, ProbsP p, double *partials) {
+    __shared__ double sm[8 * 32];
+    double acc[8];
+    uint64_t bo[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        acc[q] = 0.0;
+        const uint64_t m = (uint64_t)blockIdx.y * 8 + q;
+        bo[q] = m < p.nbins ? deposit_bin(p, m) : 0;
+    }
+    for (uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; r < p.nothers;
+         r += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t base = p.others(r);
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            if ((uint64_t)blockIdx.y * 8 + q < p.nbins) {
+                const double2 z = widen<R>(a[base | bo[q]]);
+                acc[q] += z.x * z.x + z.y * z.y;
+            }
+        }
+    }
+    block_reduce<8>(acc, sm);
+    if (threadIdx.x == 0) {
+        for (int q = 0; q < 8; ++q) {
+            const uint64_t m = (uint64_t)blockIdx.y * 8 + q;
+            if (m < p.nbins) partials[m * gridDim.x + blockIdx.x] = acc[q];
+        }
+    }
+}
+template <typename R>
+__global__ void __launch_bounds__(kRT) k_probs_perbin(const C<R> *__restrict__ a, ProbsP p, double *out) {
+    for (uint64_t m = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; m < p.nbins;
+         m += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t bo = deposit_bin(p, m);
+        double s = 0.0;
+        for (uint64_t r = 0; r < p.nothers; ++r) {
+            const double2 z = widen<R>(a[p.others(r) | bo]);
+            s += z.x * z.x + z.y * z.y;
+        }
+        out[m] = s;
+    }
+}
+template <typename R>
+__global__ void __launch_bounds__(kRT) k_probs_all(const C<R> *__restrict__ a, uint64_t n, double *out) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const double2 z = widen<R>(a[i]);
+        out[i] = z.x * z.x + z.y * z.y;
+    }
+}
+
+// ---- elementwise -------------------------------------------------------------
+template <typename R> __global__ void k_set_one(C<R> *a, uint64_t idx) { a[idx] = mk<R>(1, 0); }
+
+template <typename R>
+__global__ void __launch_bounds__(kRT) k_axpy_pauli(C<R> *__restrict__ acc, const C<R> *__restrict__ x, uint64_t n,
+                                                    uint64_t xmask, uint64_t zmask, int ny, double cr) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const double2 v = widen<R>(x[i]);
+        double fr = (__popcll(i & zmask) & 1) ? -cr : cr, fi = 0.0;
+        switch (ny & 3) {  // multiply by i^ny
+        case 1: fi = fr; fr = 0; break;
+        case 2: fr = -fr; break;
+        case 3: fi = -fr; fr = 0; break;
+        default: break;
+        }
+        const uint64_t j = i ^ xmask;
+        const double2 a = widen<R>(acc[j]);
+        acc[j] = mk<R>((R)(a.x + fr * v.x - fi * v.y), (R)(a.y + fr * v.y + fi * v.x));
+    }
+}
+template <typename R>
+__global__ void __launch_bounds__(kRT) k_axpy(C<R> *__restrict__ acc, const C<R> *__restrict__ x, uint64_t n, double c) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const double2 v = widen<R>(x[i]), a = widen<R>(acc[i]);
+        acc[i] = mk<R>((R)(a.x + c * v.x), (R)(a.y + c * v.y));
+    }
+}
+
+dim3 ew_grid(uint64_t n) {
+    uint64_t b = (n + kRT - 1) / kRT;
+    const uint64_t cap = uint64_t(sm_count()) * 16;
+    return dim3((unsigned)std::max<uint64_t>(1, std::min(b, cap)));
+}
+
+Insert insert_of(std::vector<uint32_t> bits) {
+    std::sort(bits.begin(), bits.end());
+    Insert ins{};
+    ins.nb = (int)bits.size();
+    if (ins.nb > kMaxInsert) throw Unsupported("too many inserted bits");
+    for (int j = 0; j < ins.nb; ++j) ins.low[j] = (uint64_t(1) << bits[j]) - 1;
+    return ins;
+}
+
+template <typename R> C<R> cvt(const cd &z) { return mk<R>((R)z.real(), (R)z.imag()); }
+
+}  // namespace
+
+template <typename R>
+void reduce_norm2(const void *a, uint32_t nq, double *partials, double *out, cudaStream_t st) {
+    const uint64_t n = uint64_t(1) << nq;
+    const int nb = red_blocks(n);
+    k_norm2<R><<<nb, kRT, 0, st>>>(static_cast<const C<R> *>(a), n, partials);
+    B200SV_CUDA(cudaGetLastError());
+    finalize(partials, nb, 1, out, 1, 1.0, st);
+}
+
+template <typename R>
+void reduce_inner(const void *bra, const void *ket, uint32_t nq, double *partials, double *out,
+                  cudaStream_t st) {
+    const uint64_t n = uint64_t(1) << nq;
+    const int nb = red_blocks(n);
+    k_inner<R><<<nb, kRT, 0, st>>>(static_cast<const C<R> *>(bra), static_cast<const C<R> *>(ket), n, partials);
+    B200SV_CUDA(cudaGetLastError());
+    finalize(partials, nb, 2, out, 1, 1.0, st);
+}
+
+template <typename R>
+void reduce_pauli_group(const void *psi, uint32_t nq, const PauliWord *terms, int nterms, double *partials,
+                        double *out, cudaStream_t st) {
+    if (nterms <= 0) return;
+    if (nterms > 32) throw ArgError("at most 32 Pauli words per group");
+    PauliGroupP p{};
+    p.xmask = terms[0].xmask;
+    p.nterms = nterms;
+    for (int t = 0; t < nterms; ++t) {
+        if (terms[t].xmask != p.xmask) throw ArgError("Pauli group with mixed X masks");
+        p.zmask[t] = terms[t].zmask;
+        p.ny[t] = terms[t].ny;
+    }
+    const uint64_t n = uint64_t(1) << nq;
+    if (p.xmask) {
+        int hb = 63 - __builtin_clzll(p.xmask);
+        p.hb_low = (uint64_t(1) << hb) - 1;
+        p.npairs = n / 2;
+    } else {
+        p.hb_low = 0;
+        p.npairs = n;
+    }
+    const int nb = red_blocks(p.npairs);
+    const C<R> *a = static_cast<const C<R> *>(psi);
+    if (nterms == 1) k_pauli<R, 1><<<nb, kRT, 0, st>>>(a, p, partials);
+    else if (nterms <= 8) k_pauli<R, 8><<<nb, kRT, 0, st>>>(a, p, partials);
+    else k_pauli<R, 32><<<nb, kRT, 0, st>>>(a, p, partials);
+    B200SV_CUDA(cudaGetLastError());
+    finalize(partials, nb, nterms, out, 1, 1.0, st);
+}
+
+template <typename R>
+void reduce_dense_expval(const void *psi, uint32_t nq, const GateDesc &g, const void *dev_matrix, double *partials,
+                         double *out, cudaStream_t st) {
+    if (g.kind != Kind::Dense || g.k > 4 || !g.cbits.empty()) throw Unsupported("dense expval needs k <= 4");
+    DenseEvP<R> p{};
+    p.ins = insert_of(g.tbits);
+    p.k = g.k;
+    p.ngroups = uint64_t(1) << (nq - g.k);
+    for (int r = 0; r < (1 << g.k); ++r) {
+        uint64_t o = 0;
+        for (int j = 0; j < g.k; ++j)
+            if (r & (1 << (g.k - 1 - j))) o |= uint64_t(1) << g.tbits[j];
+        p.off[r] = o;
+    }
+    std::vector<C<R>> hm(g.m.size());
+    for (size_t i = 0; i < g.m.size(); ++i) hm[i] = cvt<R>(g.m[i]);
+    B200SV_CUDA(cudaMemcpyAsync(const_cast<void *>(dev_matrix), hm.data(), hm.size() * sizeof(C<R>),
+                                cudaMemcpyHostToDevice, st));
+    const int nb = red_blocks(p.ngroups);
+    k_dense_ev<R><<<nb, kRT, 0, st>>>(static_cast<const C<R> *>(psi), p, static_cast<const C<R> *>(dev_matrix),
+                                      partials);
+    B200SV_CUDA(cudaGetLastError());
+    finalize(partials, nb, 1, out, 1, 1.0, st);
+}
+
+template <typename R>
+void reduce_generator_inner(void *const *bras, int nbra, const void *ket, uint32_t nq, const GateDesc &g,
+                            double alpha, double *partials, double *out, int out_stride, cudaStream_t st) {
+    if (nbra <= 0) return;
+    if (nbra > 16) throw ArgError("at most 16 bras per generator product");
+    GenP<R> p{};
+    p.kind = (int)g.kind;
+    p.k = g.k;
+    if (!g.cbits.empty()) throw Unsupported("generator forms carry no control bits");
+    if (g.kind == Kind::Parity) {
+        p.ngroups = uint64_t(1) << nq;
+        p.pmask = g.pmask;
+        p.pph[0] = cvt<R>(g.pphase[0]);
+        p.pph[1] = cvt<R>(g.pphase[1]);
+    } else {
+        if (g.k > 4 || (g.kind == Kind::Dense && g.k > 2) || (g.kind == Kind::Diag && g.k > 2))
+            throw Unsupported("generator form too wide");
+        p.ins = insert_of(g.tbits);
+        p.ngroups = uint64_t(1) << (nq - g.k);
+        for (int r = 0; r < (1 << g.k); ++r) {
+            uint64_t o = 0;
+            for (int j = 0; j < g.k; ++j)
+                if (r & (1 << (g.k - 1 - j))) o |= uint64_t(1) << g.tbits[j];
+            p.off[r] = o;
+        }
+        for (size_t i = 0; i < g.m.size() && i < 16; ++i) p.m[i] = cvt<R>(g.m[i]);
+        for (int i = 0; i < 4; ++i) p.m2[i] = cvt<R>(g.m2[i]);
+        p.gamma = cvt<R>(g.gamma);
+        p.pa = (int)g.pa;
+        p.pb = (int)g.pb;
+    }
+    Bras<R> B{};
+    for (int o = 0; o < nbra; ++o) B.p[o] = static_cast<const C<R> *>(bras[o]);
+    const int nb = red_blocks(p.ngroups);
+    const C<R> *k = static_cast<const C<R> *>(ket);
+    if (nbra == 1) k_gen_inner<R, 1><<<nb, kRT, 0, st>>>(B, nbra, k, p, partials);
+    else if (nbra <= 4) k_gen_inner<R, 4><<<nb, kRT, 0, st>>>(B, nbra, k, p, partials);
+    else k_gen_inner<R, 16><<<nb, kRT, 0, st>>>(B, nbra, k, p, partials);
+    B200SV_CUDA(cudaGetLastError());
+    finalize(partials, nb, nbra, out, out_stride, alpha, st);
+}
+
+template <typename R>
+void reduce_probs(const void *psi, uint32_t nq, const std::vector<uint32_t> &bits, double *partials,
+                  size_t partials_cap, double *out, cudaStream_t st) {
+    const C<R> *a = static_cast<const C<R> *>(psi);
+    const int k = (int)bits.size();
+    const uint64_t n = uint64_t(1) << nq;
+    bool identity = (k == (int)nq);
+    for (int j = 0; identity && j < k; ++j) identity = (bits[j] == nq - 1 - (uint32_t)j);
+    if (identity) {
+        k_probs_all<R><<<ew_grid(n), kRT, 0, st>>>(a, n, out);
+        B200SV_CUDA(cudaGetLastError());
+        return;
+    }
+    ProbsP p{};
+    p.others = insert_of(bits);
+    p.k = k;
+    p.nothers = uint64_t(1) << (nq - k);
+    p.nbins = uint64_t(1) << k;
+    for (int j = 0; j < k; ++j) p.binmask[j] = uint64_t(1) << bits[j];
+    if (k <= 12) {
+        const uint64_t rows = (p.nbins + 7) / 8;
+        uint64_t nbx = std::max<uint64_t>(1, std::min<uint64_t>((p.nothers + kRT * 4 - 1) / (kRT * 4),
+                                                                 std::max<uint64_t>(1, kMaxRedBlocks / rows)));
+        while (nbx > 1 && nbx * p.nbins > partials_cap) nbx /= 2;
+        k_probs_hist<R><<<dim3((unsigned)nbx, (unsigned)rows), kRT, 0, st>>>(a, p, partials);
+        B200SV_CUDA(cudaGetLastError());
+        k_finalize<<<(unsigned)p.nbins, 128, 0, st>>>(partials, (int)nbx, out, 1, 1.0);
+        B200SV_CUDA(cudaGetLastError());
+    } else {
+        k_probs_perbin<R><<<ew_grid(p.nbins), kRT, 0, st>>>(a, p, out);
+        B200SV_CUDA(cudaGetLastError());
+    }
+}
+
+template <typename R> void set_basis(void *psi, uint32_t nq, uint64_t index, cudaStream_t st) {
+    B200SV_CUDA(cudaMemsetAsync(psi, 0, sizeof(C<R>) << nq, st));
+    k_set_one<R><<<1, 1, 0, st>>>(static_cast<C<R> *>(psi), index);
+    B200SV_CUDA(cudaGetLastError());
+}
+
+template <typename R>
+void axpy_pauli(void *acc, const void *psi, uint32_t nq, const PauliWord &w, double c, cudaStream_t st) {
+    const uint64_t n = uint64_t(1) << nq;
+    k_axpy_pauli<R><<<ew_grid(n), kRT, 0, st>>>(static_cast<C<R> *>(acc), static_cast<const C<R> *>(psi), n,
+                                                w.xmask, w.zmask, w.ny, c);
+    B200SV_CUDA(cudaGetLastError());
+}
+
+template <typename R> void axpy(void *acc, const void *x, uint32_t nq, double c, cudaStream_t st) {
+    const uint64_t n = uint64_t(1) << nq;
+    k_axpy<R><<<ew_grid(n), kRT, 0, st>>>(static_cast<C<R> *>(acc), static_cast<const C<R> *>(x), n, c);
+    B200SV_CUDA(cudaGetLastError());
+}
+
+#define B200SV_INST(R)                                                                                          \
+    template void reduce_norm2<R>(const void *, uint32_t, double *, double *, cudaStream_t);                    \
+    template void reduce_inner<R>(const void *, const void *, uint32_t, double *, double *, cudaStream_t);      \
+    template void reduce_pauli_group<R>(const void *, uint32_t, const PauliWord *, int, double *, double *,     \
+                                        cudaStream_t);                                                          \
+    template void reduce_dense_expval<R>(const void *, uint32_t, const GateDesc &, const void *, double *,      \
+                                         double *, cudaStream_t);                                               \
+    template void reduce_generator_inner<R>(void *const *, int, const void *, uint32_t, const GateDesc &,       \
+                                            double, double *, double *, int, cudaStream_t);                     \
+    template void reduce_probs<R>(const void *, uint32_t, const std::vector<uint32_t> &, double *, size_t,      \
+                                  double *, cudaStream_t);                                                      \
+    template void set_basis<R>(void *, uint32_t, uint64_t, cudaStream_t);                                       \
+    template void axpy_pauli<R>(void *, const void *, uint32_t, const PauliWord &, double, cudaStream_t);       \
+    template void axpy<R>(void *, const void *, uint32_t, double, cudaStream_t);
+B200SV_INST(float)
+B200SV_INST(double)
+
+}  // namespace b200sv

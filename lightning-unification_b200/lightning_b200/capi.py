@@ -1,0 +1,389 @@
+"""ctypes view of the C ABI in include/b200sv.h (libb200sv.so).
+
+This is the Python binding a maintainer would add on the reference side for the
+batched and autograd paths; the lightning.qubit class surface itself is the
+pybind11 module ``lightning_qubit_ops``.  Loading fails loudly when the shared
+library is missing: there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+_LIB_PATH = Path(__file__).resolve().parent / "libb200sv.so"
+
+B200SV_OK = 0
+B200SV_C64 = 0
+B200SV_C128 = 1
+OP_MATRIX = 1000
+OP_SKIP = 1001
+FACTOR_NAMED = 0
+FACTOR_MATRIX = 1
+
+# CS/gates/GateOperation.hpp:27-70 (the enum values of the reference)
+GATE_IDS = {
+    name: i for i, name in enumerate([
+        "Identity", "PauliX", "PauliY", "PauliZ", "Hadamard", "S", "T", "PhaseShift", "RX", "RY", "RZ",
+        "Rot", "CNOT", "CY", "CZ", "SWAP", "IsingXX", "IsingXY", "IsingYY", "IsingZZ",
+        "ControlledPhaseShift", "CRX", "CRY", "CRZ", "CRot", "SingleExcitation", "SingleExcitationMinus",
+        "SingleExcitationPlus", "Toffoli", "CSWAP", "DoubleExcitation", "DoubleExcitationMinus",
+        "DoubleExcitationPlus", "MultiRZ"])
+}
+GATE_NAMES = {v: k for k, v in GATE_IDS.items()}
+# CS/gates/GateOperation.hpp:75-98
+GENERATOR_IDS = {
+    name: i for i, name in enumerate([
+        "PhaseShift", "RX", "RY", "RZ", "IsingXX", "IsingXY", "IsingYY", "IsingZZ", "CRX", "CRY", "CRZ",
+        "ControlledPhaseShift", "SingleExcitation", "SingleExcitationMinus", "SingleExcitationPlus",
+        "DoubleExcitation", "DoubleExcitationMinus", "DoubleExcitationPlus", "MultiRZ"])
+}
+
+
+class B200Error(RuntimeError):
+    """Raised when a libb200sv call returns a non-zero status."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(message)
+        self.status = status
+
+
+class Op(C.Structure):
+    _fields_ = [("gate", C.c_uint32), ("nwires", C.c_uint32), ("wires", C.POINTER(C.c_uint32)),
+                ("inverse", C.c_int32), ("nparams", C.c_uint32), ("params", C.POINTER(C.c_double)),
+                ("matrix", C.c_void_p)]
+
+
+class Factor(C.Structure):
+    _fields_ = [("kind", C.c_uint32), ("gate", C.c_uint32), ("nwires", C.c_uint32),
+                ("wires", C.POINTER(C.c_uint32)), ("matrix", C.c_void_p)]
+
+
+class Term(C.Structure):
+    _fields_ = [("coeff", C.c_double), ("nfactors", C.c_uint32), ("factors", C.POINTER(Factor))]
+
+
+class Observable(C.Structure):
+    _fields_ = [("nterms", C.c_uint32), ("terms", C.POINTER(Term))]
+
+
+class BatchCircuit(C.Structure):
+    _fields_ = [("num_qubits", C.c_uint32), ("nops", C.c_uint32), ("ops", C.POINTER(Op)),
+                ("param_index", C.POINTER(C.c_int64)), ("nobs", C.c_uint32),
+                ("obs_nterms", C.POINTER(C.c_uint32)), ("obs_coeffs", C.POINTER(C.c_double)),
+                ("obs_offsets", C.POINTER(C.c_uint32)), ("obs_wires", C.POINTER(C.c_uint32)),
+                ("obs_paulis", C.c_char_p)]
+
+
+_SIGS = {
+    "b200sv_last_error": ([], C.c_char_p),
+    "b200sv_version": ([], C.c_int),
+    "b200sv_device_count": ([C.POINTER(C.c_int)], C.c_int),
+    "b200sv_create": ([C.c_uint32, C.c_int, C.POINTER(C.c_void_p)], C.c_int),
+    "b200sv_destroy": ([C.c_void_p], C.c_int),
+    "b200sv_num_qubits": ([C.c_void_p, C.POINTER(C.c_uint32)], C.c_int),
+    "b200sv_dtype": ([C.c_void_p, C.POINTER(C.c_int)], C.c_int),
+    "b200sv_set_stream": ([C.c_void_p, C.c_void_p], C.c_int),
+    "b200sv_synchronize": ([C.c_void_p], C.c_int),
+    "b200sv_device_ptr": ([C.c_void_p, C.POINTER(C.c_void_p)], C.c_int),
+    "b200sv_upload": ([C.c_void_p, C.c_void_p, C.c_uint64], C.c_int),
+    "b200sv_download": ([C.c_void_p, C.c_void_p, C.c_uint64], C.c_int),
+    "b200sv_copy": ([C.c_void_p, C.c_void_p], C.c_int),
+    "b200sv_set_basis_state": ([C.c_void_p, C.c_uint64], C.c_int),
+    "b200sv_apply_gate": ([C.c_void_p, C.c_uint32, C.POINTER(C.c_uint32), C.c_uint32, C.c_int,
+                           C.POINTER(C.c_double), C.c_uint32], C.c_int),
+    "b200sv_apply_matrix": ([C.c_void_p, C.c_void_p, C.POINTER(C.c_uint32), C.c_uint32, C.c_int], C.c_int),
+    "b200sv_apply_ops": ([C.c_void_p, C.POINTER(Op), C.c_uint32], C.c_int),
+    "b200sv_apply_generator": ([C.c_void_p, C.c_uint32, C.POINTER(C.c_uint32), C.c_uint32, C.c_int,
+                                C.POINTER(C.c_double)], C.c_int),
+    "b200sv_probs": ([C.c_void_p, C.POINTER(C.c_uint32), C.c_uint32, C.POINTER(C.c_double)], C.c_int),
+    "b200sv_probs_device": ([C.c_void_p, C.POINTER(C.c_uint32), C.c_uint32, C.c_void_p], C.c_int),
+    "b200sv_expval": ([C.c_void_p, C.POINTER(Observable), C.POINTER(C.c_double)], C.c_int),
+    "b200sv_var": ([C.c_void_p, C.POINTER(Observable), C.POINTER(C.c_double)], C.c_int),
+    "b200sv_expval_pauli": ([C.c_void_p, C.c_uint32, C.POINTER(C.c_double), C.POINTER(C.c_uint32),
+                             C.POINTER(C.c_uint32), C.c_char_p, C.POINTER(C.c_double),
+                             C.POINTER(C.c_double)], C.c_int),
+    "b200sv_inner_product": ([C.c_void_p, C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double)], C.c_int),
+    "b200sv_norm2": ([C.c_void_p, C.POINTER(C.c_double)], C.c_int),
+    "b200sv_sample": ([C.c_void_p, C.c_uint64, C.POINTER(C.c_double), C.c_uint64,
+                       C.POINTER(C.c_uint64)], C.c_int),
+    "b200sv_sample_bits": ([C.c_void_p, C.c_uint64, C.POINTER(C.c_double), C.c_uint64,
+                            C.POINTER(C.c_uint64)], C.c_int),
+    "b200sv_adjoint_jacobian": ([C.c_void_p, C.POINTER(Op), C.c_uint32, C.POINTER(Observable), C.c_uint32,
+                                 C.POINTER(C.c_uint64), C.c_uint32, C.c_int, C.POINTER(C.c_double)], C.c_int),
+    "b200sv_batch_create": ([C.c_int, C.POINTER(BatchCircuit), C.c_uint32, C.c_uint64,
+                             C.POINTER(C.c_void_p)], C.c_int),
+    "b200sv_batch_destroy": ([C.c_void_p], C.c_int),
+    "b200sv_batch_set_stream": ([C.c_void_p, C.c_void_p], C.c_int),
+    "b200sv_batch_forward": ([C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
+    "b200sv_batch_vjp": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
+    "b200sv_batch_jacobian": ([C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
+    "b200sv_batch_use_graphs": ([C.c_void_p, C.c_int], C.c_int),
+    "b200sv_batch_autotune": ([C.c_void_p, C.c_void_p, C.POINTER(C.c_int)], C.c_int),
+    "b200sv_batch_last_launches": ([C.c_void_p, C.POINTER(C.c_uint32)], C.c_int),
+}
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """Load libb200sv.so (once).  Raises if the library was not built."""
+    global _lib
+    if _lib is None:
+        if not _LIB_PATH.exists():
+            raise ImportError(f"libb200sv.so not found at {_LIB_PATH}; run __graft_entry__.build() "
+                              "(the CUDA extension is required, there is no CPU path)")
+        L = C.CDLL(str(_LIB_PATH))
+        for name, (args, res) in _SIGS.items():
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = res
+        _lib = L
+    return _lib
+
+
+def declared_symbols():
+    return list(_SIGS)
+
+
+def check(status: int) -> None:
+    if status != B200SV_OK:
+        msg = lib().b200sv_last_error().decode(errors="replace")
+        raise B200Error(status, msg)
+
+
+def device_count() -> int:
+    n = C.c_int(0)
+    check(lib().b200sv_device_count(C.byref(n)))
+    return n.value
+
+
+def _u32(seq):
+    a = np.ascontiguousarray(np.asarray(seq, dtype=np.uint32))
+    return a, a.ctypes.data_as(C.POINTER(C.c_uint32))
+
+
+def _f64(seq):
+    a = np.ascontiguousarray(np.asarray(seq, dtype=np.float64))
+    return a, a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+class OpList:
+    """Packs a list of (name_or_id, wires, inverse, params[, matrix]) into b200sv_op records.
+
+    Keeps every backing array alive for the lifetime of the object."""
+
+    def __init__(self, ops, complex_dtype=np.complex128):
+        self._keep = []
+        self.arr = (Op * max(1, len(ops)))()
+        self.n = len(ops)
+        for i, op in enumerate(ops):
+            name, wires, inverse, params = op[:4]
+            matrix = op[4] if len(op) > 4 else None
+            gid = name if isinstance(name, int) else (
+                OP_MATRIX if name in ("QubitUnitary", "Matrix") else
+                OP_SKIP if name in ("QubitStateVector", "BasisState", "StatePrep") else GATE_IDS[name])
+            w, wp = _u32(wires)
+            p, pp = _f64(params if params is not None else [])
+            self._keep += [w, p]
+            rec = self.arr[i]
+            rec.gate = gid
+            rec.nwires = len(w)
+            rec.wires = wp
+            rec.inverse = 1 if inverse else 0
+            rec.nparams = len(p)
+            rec.params = pp
+            if matrix is not None:
+                m = np.ascontiguousarray(np.asarray(matrix, dtype=complex_dtype))
+                self._keep.append(m)
+                rec.matrix = m.ctypes.data
+            else:
+                rec.matrix = None
+
+    @property
+    def ptr(self):
+        return self.arr
+
+
+class ObservableBuilder:
+    """Builds b200sv_observable records.
+
+    An observable is a list of terms ``(coeff, [factor, ...])``; a factor is
+    ``(name, wires)`` for a named operator or ``("Hermitian", wires, matrix)``."""
+
+    def __init__(self, terms, complex_dtype=np.complex128):
+        self._keep = []
+        self.terms = (Term * max(1, len(terms)))()
+        for t, (coeff, factors) in enumerate(terms):
+            fa = (Factor * max(1, len(factors)))()
+            self._keep.append(fa)
+            for j, f in enumerate(factors):
+                w, wp = _u32(f[1])
+                self._keep.append(w)
+                fa[j].nwires = len(w)
+                fa[j].wires = wp
+                if f[0] == "Hermitian":
+                    m = np.ascontiguousarray(np.asarray(f[2], dtype=complex_dtype))
+                    self._keep.append(m)
+                    fa[j].kind = FACTOR_MATRIX
+                    fa[j].gate = 0
+                    fa[j].matrix = m.ctypes.data
+                else:
+                    fa[j].kind = FACTOR_NAMED
+                    fa[j].gate = GATE_IDS[f[0]]
+                    fa[j].matrix = None
+            self.terms[t].coeff = float(coeff)
+            self.terms[t].nfactors = len(factors)
+            self.terms[t].factors = fa
+        self.obs = Observable(len(terms), self.terms)
+
+
+class StateVector:
+    """Device state vector handle (b200sv_create / b200sv_destroy)."""
+
+    def __init__(self, num_qubits: int, dtype=np.complex128):
+        self.num_qubits = int(num_qubits)
+        self.np_dtype = np.dtype(dtype)
+        self.code = B200SV_C64 if self.np_dtype == np.complex64 else B200SV_C128
+        h = C.c_void_p()
+        check(lib().b200sv_create(self.num_qubits, self.code, C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().b200sv_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # data movement
+    def upload(self, data):
+        a = np.ascontiguousarray(np.asarray(data, dtype=self.np_dtype))
+        check(lib().b200sv_upload(self.h, a.ctypes.data, a.size))
+
+    def download(self):
+        a = np.empty(1 << self.num_qubits, dtype=self.np_dtype)
+        check(lib().b200sv_download(self.h, a.ctypes.data, a.size))
+        return a
+
+    def set_basis_state(self, index: int):
+        check(lib().b200sv_set_basis_state(self.h, int(index)))
+
+    def device_ptr(self) -> int:
+        p = C.c_void_p()
+        check(lib().b200sv_device_ptr(self.h, C.byref(p)))
+        return p.value
+
+    def synchronize(self):
+        check(lib().b200sv_synchronize(self.h))
+
+    def set_stream(self, stream_handle: int | None):
+        check(lib().b200sv_set_stream(self.h, C.c_void_p(stream_handle or 0)))
+
+    # gates
+    def apply(self, name, wires, inverse=False, params=()):
+        gid = name if isinstance(name, int) else GATE_IDS[name]
+        w, wp = _u32(wires)
+        p, pp = _f64(params)
+        check(lib().b200sv_apply_gate(self.h, gid, wp, len(w), 1 if inverse else 0, pp, len(p)))
+
+    def apply_matrix(self, matrix, wires, inverse=False):
+        m = np.ascontiguousarray(np.asarray(matrix, dtype=self.np_dtype))
+        w, wp = _u32(wires)
+        check(lib().b200sv_apply_matrix(self.h, m.ctypes.data, wp, len(w), 1 if inverse else 0))
+
+    def apply_ops(self, ops):
+        ol = OpList(ops, self.np_dtype)
+        check(lib().b200sv_apply_ops(self.h, ol.ptr, ol.n))
+
+    def apply_generator(self, name, wires, adj=False) -> float:
+        gid = name if isinstance(name, int) else GENERATOR_IDS[name]
+        w, wp = _u32(wires)
+        s = C.c_double()
+        check(lib().b200sv_apply_generator(self.h, gid, wp, len(w), 1 if adj else 0, C.byref(s)))
+        return s.value
+
+    # measurements
+    def probs(self, wires=None):
+        wires = [] if wires is None else list(wires)
+        k = len(wires) if wires else self.num_qubits
+        out = np.empty(1 << k, dtype=np.float64)
+        w, wp = _u32(wires)
+        check(lib().b200sv_probs(self.h, wp, len(w), out.ctypes.data_as(C.POINTER(C.c_double))))
+        return out
+
+    def expval(self, terms) -> float:
+        ob = ObservableBuilder(terms, self.np_dtype)
+        r = C.c_double()
+        check(lib().b200sv_expval(self.h, C.byref(ob.obs), C.byref(r)))
+        return r.value
+
+    def var(self, terms) -> float:
+        ob = ObservableBuilder(terms, self.np_dtype)
+        r = C.c_double()
+        check(lib().b200sv_var(self.h, C.byref(ob.obs), C.byref(r)))
+        return r.value
+
+    def expval_pauli(self, words, coeffs=None):
+        """words: list of (pauli_string, wires); returns (per-term values, weighted sum)."""
+        coeffs = np.ones(len(words)) if coeffs is None else np.asarray(coeffs, dtype=np.float64)
+        offs = [0]
+        wires, letters = [], []
+        for s, w in words:
+            assert len(s) == len(w)
+            wires += list(w)
+            letters += list(s)
+            offs.append(len(wires))
+        o, op_ = _u32(offs)
+        w, wp = _u32(wires)
+        c, cp = _f64(coeffs)
+        pl = "".join(letters).encode() + b"\0"
+        out = np.empty(max(1, len(words)))
+        tot = C.c_double()
+        check(lib().b200sv_expval_pauli(self.h, len(words), cp, op_, wp, pl,
+                                        out.ctypes.data_as(C.POINTER(C.c_double)), C.byref(tot)))
+        return out[:len(words)], tot.value
+
+    def inner(self, ket: "StateVector") -> complex:
+        re, im = C.c_double(), C.c_double()
+        check(lib().b200sv_inner_product(self.h, ket.h, C.byref(re), C.byref(im)))
+        return complex(re.value, im.value)
+
+    def norm2(self) -> float:
+        r = C.c_double()
+        check(lib().b200sv_norm2(self.h, C.byref(r)))
+        return r.value
+
+    def sample(self, nshots: int, uniforms=None, seed: int = 0):
+        out = np.empty(max(1, nshots), dtype=np.uint64)
+        up = None
+        if uniforms is not None:
+            u, up = _f64(uniforms)
+            assert len(u) == nshots
+        check(lib().b200sv_sample(self.h, nshots, up, seed, out.ctypes.data_as(C.POINTER(C.c_uint64))))
+        return out[:nshots]
+
+    def sample_bits(self, nshots: int, uniforms=None, seed: int = 0):
+        out = np.empty(max(1, nshots * self.num_qubits), dtype=np.uint64)
+        up = None
+        if uniforms is not None:
+            u, up = _f64(uniforms)
+        check(lib().b200sv_sample_bits(self.h, nshots, up, seed, out.ctypes.data_as(C.POINTER(C.c_uint64))))
+        return out[:nshots * self.num_qubits].reshape(nshots, self.num_qubits)
+
+    def adjoint_jacobian(self, ops, observables, trainable, apply_operations=False):
+        ol = OpList(ops, self.np_dtype)
+        builders = [ObservableBuilder(t, self.np_dtype) for t in observables]
+        arr = (Observable * max(1, len(builders)))(*[b.obs for b in builders])
+        tp = np.ascontiguousarray(np.asarray(trainable, dtype=np.uint64))
+        jac = np.zeros(max(1, len(builders) * len(tp)), dtype=np.float64)
+        check(lib().b200sv_adjoint_jacobian(self.h, ol.ptr, ol.n, arr, len(builders),
+                                            tp.ctypes.data_as(C.POINTER(C.c_uint64)), len(tp),
+                                            1 if apply_operations else 0,
+                                            jac.ctypes.data_as(C.POINTER(C.c_double))))
+        return jac[:len(builders) * len(tp)].reshape(len(builders), len(tp))

@@ -1,0 +1,163 @@
+"""Batched engine on the B200 vs the FP64 oracle: forward expectation values,
+vector-Jacobian products through torch.autograd and full per-circuit Jacobians.
+
+Circuit widths straddle the on-chip threshold so both the shared-memory-resident
+path and the tiled HBM path run."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def small_hea(dtype, seed=3):
+    from lightning_b200.workloads import hea_batch
+    return hea_batch(ncirc=24, nmin=2, nmax=15 if dtype == np.complex64 else 14, dmin=1, dmax=3, seed=seed)
+
+
+def mixed_batch(seed=8):
+    """Circuits using every gate kind the batch supports, with shared and constant parameters."""
+    rng = np.random.default_rng(seed)
+    circuits, params = [], list(rng.uniform(0, 2 * np.pi, 6))
+    kinds1 = ["RX", "RY", "RZ", "PhaseShift"]
+    kinds2 = ["CRX", "CRY", "CRZ", "ControlledPhaseShift", "IsingXX", "IsingYY", "IsingZZ", "IsingXY",
+              "SingleExcitation", "SingleExcitationMinus", "SingleExcitationPlus"]
+    const = ["Hadamard", "PauliX", "PauliY", "PauliZ", "S", "T", "Identity"]
+    for c in range(10):
+        n = [3, 5, 9, 13, 14, 15][c % 6]
+        ops, pidx = [], []
+        for _ in range(30):
+            r = rng.random()
+            if r < 0.3:
+                ops.append((kinds1[rng.integers(4)], [int(rng.integers(n))], bool(rng.random() < 0.3), []))
+                pidx.append(len(params))
+                params.append(float(rng.uniform(0, 2 * np.pi)))
+            elif r < 0.55:
+                w = [int(x) for x in rng.choice(n, 2, replace=False)]
+                ops.append((kinds2[rng.integers(len(kinds2))], w, bool(rng.random() < 0.3), []))
+                pidx.append(len(params))
+                params.append(float(rng.uniform(0, 2 * np.pi)))
+            elif r < 0.65:  # shared parameter slot
+                ops.append(("RY", [int(rng.integers(n))], False, []))
+                pidx.append(int(rng.integers(6)))
+            elif r < 0.75:
+                ops.append(("RX", [int(rng.integers(n))], False, [float(rng.uniform(0, 6))]))  # constant angle
+                pidx.append(-1)
+            elif r < 0.85:
+                ops.append((const[rng.integers(len(const))], [int(rng.integers(n))], False, []))
+                pidx.append(-1)
+            else:
+                k = 3 if n >= 3 and rng.random() < 0.3 else 2
+                name = {2: ["CNOT", "CZ", "SWAP", "CY"][rng.integers(4)], 3: ["Toffoli", "CSWAP"][rng.integers(2)]}[k]
+                ops.append((name, [int(x) for x in rng.choice(n, k, replace=False)], False, []))
+                pidx.append(-1)
+        ops.append(("MultiRZ", [0, n - 1], False, []))
+        pidx.append(len(params))
+        params.append(0.77)
+        obs = [[(0.5, "Z", [0]), (-1.5, "XZ", [n - 1, 1 % n])], [(1.0, "Y", [n // 2])], [(0.3, "ZZ", [0, n - 1])]]
+        circuits.append({"num_qubits": n, "ops": ops, "param_index": pidx, "observables": obs})
+    return circuits, np.array(params)
+
+
+def oracle_outputs(circuits, params):
+    import lq_oracle as O
+    from lightning_b200.workloads import bind, obs_terms
+    out = []
+    for c in circuits:
+        st = O.run_circuit(c["num_qubits"], bind(c, params))
+        out += [O.expval(st, obs_terms(ob)) for ob in c["observables"]]
+    return np.array(out)
+
+
+def oracle_vjp(circuits, params, dy):
+    import lq_oracle as O
+    from lightning_b200.workloads import bind, obs_terms
+    grad = np.zeros(len(params))
+    k = 0
+    for c in circuits:
+        ops = bind(c, params)
+        n = c["num_qubits"]
+        obs = [obs_terms(ob) for ob in c["observables"]]
+        slots = [p for p in c["param_index"] if p >= 0]
+        tp = list(range(len(slots)))
+        psi = O.run_circuit(n, ops)
+        # only ops with a slot are trainable; constant-angle ops are parametric but not trainable
+        pops = [i for i, op in enumerate(ops) if len(op[3]) > 0]
+        trainable = [j for j, i in enumerate(pops) if c["param_index"][i] >= 0]
+        j = O.adjoint_jacobian(psi, ops, obs, trainable)
+        for oi in range(len(obs)):
+            for col, i in enumerate([pops[t] for t in trainable]):
+                grad[c["param_index"][i]] += dy[k + oi] * j[oi, col]
+        k += len(obs)
+        del tp
+    return grad
+
+
+@pytest.mark.parametrize("dtype", [np.complex128, np.complex64])
+@pytest.mark.parametrize("maker", ["hea", "mixed"])
+def test_batch_forward_and_vjp(dtype, maker):
+    import torch
+    from lightning_b200.batch import BatchedCircuits
+    from lightning_b200.autograd import batched_expval
+    circuits, params = small_hea(dtype) if maker == "hea" else mixed_batch()
+    eng = BatchedCircuits(circuits, len(params), dtype=dtype, use_graphs=False)
+    p = torch.tensor(params, dtype=torch.float64, device="cuda", requires_grad=True)
+    out = batched_expval(p, eng)
+    want = oracle_outputs(circuits, params)
+    tol = 1e-11 if dtype == np.complex128 else 2e-5
+    assert np.abs(out.detach().cpu().numpy() - want).max() < tol
+    rng = np.random.default_rng(1)
+    dy = rng.normal(size=out.numel())
+    (out * torch.tensor(dy, device="cuda")).sum().backward()
+    gwant = oracle_vjp(circuits, params, dy)
+    assert np.abs(p.grad.cpu().numpy() - gwant).max() < (1e-10 if dtype == np.complex128 else 1e-4)
+
+
+@pytest.mark.parametrize("dtype", [np.complex128, np.complex64])
+def test_batch_graphs_and_autotune_repeatable(dtype):
+    import torch
+    from lightning_b200.batch import BatchedCircuits
+    circuits, params = small_hea(dtype, seed=9)
+    eng = BatchedCircuits(circuits, len(params), dtype=dtype, use_graphs=True)
+    p = torch.tensor(params, dtype=torch.float64, device="cuda")
+    a = eng.forward(p)
+    b = eng.forward(p)  # graph replay
+    assert torch.equal(a, b)
+    dy = torch.ones_like(a)
+    g1 = eng.vjp(p, dy)
+    eng.autotune(p)
+    g2 = eng.vjp(p, dy)
+    c = eng.forward(p)
+    assert np.abs(a.cpu().numpy() - oracle_outputs(circuits, params)).max() < (1e-11 if dtype == np.complex128 else 2e-5)
+    assert torch.allclose(a, c, atol=1e-12 if dtype == np.complex128 else 1e-5)
+    assert torch.allclose(g1, g2, atol=1e-10 if dtype == np.complex128 else 1e-4)
+
+
+def test_batch_jacobian_rot_ring():
+    import torch
+    import lq_oracle as O
+    from lightning_b200.batch import BatchedCircuits
+    from lightning_b200.workloads import rot_ring_batch, bind, obs_terms
+    circuits, params = rot_ring_batch(ncirc=3, n=6, layers=2, seed=4)
+    eng = BatchedCircuits(circuits, len(params), dtype=np.complex128, use_graphs=False)
+    p = torch.tensor(params, dtype=torch.float64, device="cuda")
+    jac = eng.jacobian(p).cpu().numpy()
+    off = 0
+    for c in circuits:
+        ops = bind(c, params)
+        obs = [obs_terms(o) for o in c["observables"]]
+        npo = sum(1 for q in c["param_index"] if q >= 0)
+        want = O.adjoint_jacobian(O.run_circuit(6, ops), ops, obs, list(range(npo)))
+        got = jac[off:off + len(obs) * npo].reshape(len(obs), npo)
+        assert np.abs(got - want).max() < 1e-11
+        off += len(obs) * npo
+
+
+def test_batch_rejects_bad_input():
+    from lightning_b200 import capi
+    from lightning_b200.batch import BatchedCircuits
+    with pytest.raises(capi.B200Error, match="decomposed"):
+        BatchedCircuits([{"num_qubits": 2, "ops": [("Rot", [0], False, [])], "param_index": [0],
+                          "observables": [[(1.0, "Z", [0])]]}], 1)
+    with pytest.raises(capi.B200Error, match="out of range"):
+        BatchedCircuits([{"num_qubits": 2, "ops": [("RX", [0], False, [])], "param_index": [5],
+                          "observables": [[(1.0, "Z", [0])]]}], 1)

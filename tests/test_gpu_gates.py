@@ -1,0 +1,163 @@
+"""Gate application on the B200 vs the FP64 oracle (GateImplementationsLM semantics).
+
+Mirrors the reference's gate tests (LQ/gates/tests/Test_GateImplementations_*.cpp):
+every gate, both directions, random states, every wire placement on small
+registers, dense matrices of 1..7 wires, and generators.
+"""
+import itertools
+
+import numpy as np
+import pytest
+
+from conftest import TOL, random_state
+
+pytestmark = pytest.mark.gpu
+
+GATES = {"Identity": (1, 0), "PauliX": (1, 0), "PauliY": (1, 0), "PauliZ": (1, 0), "Hadamard": (1, 0),
+         "S": (1, 0), "T": (1, 0), "PhaseShift": (1, 1), "RX": (1, 1), "RY": (1, 1), "RZ": (1, 1),
+         "Rot": (1, 3), "CNOT": (2, 0), "CY": (2, 0), "CZ": (2, 0), "SWAP": (2, 0), "IsingXX": (2, 1),
+         "IsingXY": (2, 1), "IsingYY": (2, 1), "IsingZZ": (2, 1), "ControlledPhaseShift": (2, 1),
+         "CRX": (2, 1), "CRY": (2, 1), "CRZ": (2, 1), "CRot": (2, 3), "SingleExcitation": (2, 1),
+         "SingleExcitationMinus": (2, 1), "SingleExcitationPlus": (2, 1), "Toffoli": (3, 0),
+         "CSWAP": (3, 0), "DoubleExcitation": (4, 1), "DoubleExcitationMinus": (4, 1),
+         "DoubleExcitationPlus": (4, 1), "MultiRZ": (3, 1)}
+
+
+@pytest.fixture(scope="module")
+def capi():
+    from lightning_b200 import capi as c
+    if c.device_count() == 0:
+        pytest.fail("no CUDA device visible to libb200sv")
+    return c
+
+
+@pytest.mark.parametrize("dtype", [np.complex128, np.complex64])
+@pytest.mark.parametrize("inverse", [False, True])
+@pytest.mark.parametrize("name", list(GATES))
+def test_gate_random_state(capi, name, inverse, dtype):
+    import lq_oracle as O
+    rng = np.random.default_rng(abs(hash((name, inverse))) % 2**32)
+    n = 9
+    k, p = GATES[name]
+    for _ in range(3):
+        st = random_state(rng, n, dtype)
+        wires = [int(w) for w in rng.choice(n, k, replace=False)]
+        params = list(rng.uniform(0, 2 * np.pi, p))
+        sv = capi.StateVector(n, dtype)
+        sv.upload(st)
+        sv.apply(name, wires, inverse, params)
+        got = sv.download()
+        want = O.apply_op(st.astype(np.complex128), name, wires, inverse, params)
+        assert np.abs(got - want).max() < TOL[dtype] * 10, (name, wires)
+
+
+@pytest.mark.parametrize("name", ["CNOT", "CRY", "IsingXY", "SWAP", "CSWAP", "Toffoli", "DoubleExcitationPlus",
+                                  "ControlledPhaseShift", "CY", "SingleExcitationMinus"])
+def test_gate_every_wire_placement(capi, name):
+    import lq_oracle as O
+    rng = np.random.default_rng(5)
+    n = 5
+    k, p = GATES[name]
+    st = random_state(rng, n)
+    sv = capi.StateVector(n)
+    for wires in itertools.permutations(range(n), k):
+        params = list(rng.uniform(0, 2 * np.pi, p))
+        sv.upload(st)
+        sv.apply(name, list(wires), False, params)
+        want = O.apply_op(st, name, list(wires), False, params)
+        assert np.abs(sv.download() - want).max() < 1e-12, wires
+
+
+@pytest.mark.parametrize("n", [1, 2, 14, 21])
+def test_low_and_high_wires(capi, n):
+    import lq_oracle as O
+    rng = np.random.default_rng(n)
+    st = random_state(rng, n)
+    sv = capi.StateVector(n)
+    sv.upload(st)
+    ops = [("RX", [0], False, [0.3]), ("RY", [n - 1], False, [1.1]), ("Hadamard", [n // 2], False, []),
+           ("PauliY", [n - 1], True, []), ("RZ", [0], False, [2.0])]
+    if n >= 2:
+        ops += [("CNOT", [n - 1, 0], False, []), ("CRX", [0, n - 1], True, [0.7])]
+    for op in ops:
+        sv.apply(*op)
+        st = O.apply_op(st, *op)
+    assert np.abs(sv.download() - st).max() < 1e-12
+
+
+@pytest.mark.parametrize("dtype", [np.complex128, np.complex64])
+@pytest.mark.parametrize("k", [1, 2, 3, 4, 5, 6, 7])
+def test_apply_matrix(capi, k, dtype):
+    import lq_oracle as O
+    from lightning_b200.workloads import random_unitary
+    rng = np.random.default_rng(100 + k)
+    n = max(k + 2, 9)
+    st = random_state(rng, n, dtype)
+    for inverse in (False, True):
+        u = random_unitary(rng, k)
+        wires = [int(w) for w in rng.choice(n, k, replace=False)]
+        sv = capi.StateVector(n, dtype)
+        sv.upload(st)
+        sv.apply_matrix(u.astype(dtype), wires, inverse)
+        want = O.apply_matrix(st.astype(np.complex128), u.astype(dtype).astype(np.complex128), wires, inverse)
+        assert np.abs(sv.download() - want).max() < TOL[dtype] * 20 * (1 << k)
+
+
+GENS = ["PhaseShift", "RX", "RY", "RZ", "IsingXX", "IsingXY", "IsingYY", "IsingZZ", "CRX", "CRY", "CRZ",
+        "ControlledPhaseShift", "SingleExcitation", "SingleExcitationMinus", "SingleExcitationPlus",
+        "DoubleExcitation", "DoubleExcitationMinus", "DoubleExcitationPlus", "MultiRZ"]
+
+
+@pytest.mark.parametrize("name", GENS)
+def test_generators(capi, name):
+    import lq_oracle as O
+    rng = np.random.default_rng(7)
+    n = 7
+    k = {"PhaseShift": 1, "RX": 1, "RY": 1, "RZ": 1, "MultiRZ": 3}.get(name, 4 if "Double" in name else 2)
+    st = random_state(rng, n)
+    wires = [int(w) for w in rng.choice(n, k, replace=False)]
+    sv = capi.StateVector(n)
+    sv.upload(st)
+    scale = sv.apply_generator(name, wires)
+    want, wscale = O.apply_generator(st, name, wires)
+    assert scale == wscale
+    assert np.abs(sv.download() - want).max() < 1e-12
+
+
+def test_generator_definition(capi):
+    """i G |psi> = dU/dtheta |psi> at theta = 0 (Test_GateImplementations_Generator.cpp:30-40)."""
+    import lq_oracle as O
+    rng = np.random.default_rng(11)
+    n = 6
+    eps = 1e-6
+    for name in GENS:
+        k = {"PhaseShift": 1, "RX": 1, "RY": 1, "RZ": 1, "MultiRZ": 2}.get(name, 4 if "Double" in name else 2)
+        wires = list(range(k))
+        st = random_state(rng, n)
+        sv = capi.StateVector(n)
+        sv.upload(st)
+        scale = sv.apply_generator(name, wires)
+        g = sv.download()
+        plus = O.apply_op(st, name, wires, False, [eps])
+        minus = O.apply_op(st, name, wires, False, [-eps])
+        deriv = (plus - minus) / (2 * eps)
+        assert np.abs(1j * scale * g - deriv).max() < 1e-8, name
+
+
+def test_apply_ops_sequence_and_errors(capi):
+    import lq_oracle as O
+    from lightning_b200.workloads import gate_sweep
+    n = 10
+    ops = gate_sweep(n, 60, seed=3)
+    sv = capi.StateVector(n)
+    sv.apply_ops(ops)
+    want = O.run_circuit(n, ops)
+    assert np.abs(sv.download() - want).max() < 1e-12
+    with pytest.raises(capi.B200Error, match="wires must be distinct"):
+        sv.apply("CNOT", [1, 1])
+    with pytest.raises(capi.B200Error, match="out of range"):
+        sv.apply("RX", [n], False, [0.1])
+    with pytest.raises(capi.B200Error, match="expected 1 parameters"):
+        sv.apply("RX", [0], False, [])
+    with pytest.raises(capi.B200Error, match="expected 2 wires"):
+        sv.apply("CNOT", [0])

@@ -1,0 +1,138 @@
+"""Measurements on the B200 vs the oracle: probs, expval, var, sampling.
+
+Golden values follow LQ/measurements/tests/Test_MeasurementsLQubit.cpp:41-197 on
+the state of CS/utils/TestHelpers.hpp:380-414 (RX then RY with angles 0.7, 0.5, 0.3
+on three qubits).  Sample indices are checked bit-exactly against the oracle's
+restatement of the inverse-CDF rule fed the same uniforms.
+"""
+import numpy as np
+import pytest
+
+from conftest import TOL, random_state
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def capi():
+    from lightning_b200 import capi as c
+    return c
+
+
+def nontrivial_state_ops():
+    angles = [0.7, 0.5, 0.3]
+    ops = []
+    for q, a in enumerate(angles):
+        ops.append(("RX", [q], False, [a]))
+        ops.append(("RY", [q], False, [a]))
+    return ops
+
+
+@pytest.mark.parametrize("dtype", [np.complex128, np.complex64])
+def test_golden_expvals(capi, dtype):
+    sv = capi.StateVector(3, dtype)
+    sv.apply_ops(nontrivial_state_ops())
+    tol = 1e-6
+    # Test_MeasurementsLQubit.cpp:56-69 (PauliX) and :76-89 (PauliY), :96-109 (PauliZ)
+    x = [sv.expval([(1.0, [("PauliX", [w])])]) for w in range(3)]
+    y = [sv.expval([(1.0, [("PauliY", [w])])]) for w in range(3)]
+    z = [sv.expval([(1.0, [("PauliZ", [w])])]) for w in range(3)]
+    assert np.allclose(x, [0.49272486, 0.42073549, 0.28232124], atol=tol)
+    assert np.allclose(y, [-0.64421768, -0.47942553, -0.29552020], atol=tol)
+    assert np.allclose(z, [0.58498357, 0.77015115, 0.91266780], atol=tol)
+
+
+@pytest.mark.parametrize("dtype", [np.complex128, np.complex64])
+def test_probs(capi, dtype):
+    import lq_oracle as O
+    rng = np.random.default_rng(2)
+    n = 11
+    st = random_state(rng, n, dtype)
+    sv = capi.StateVector(n, dtype)
+    sv.upload(st)
+    tol = 1e-14 if dtype == np.complex128 else 1e-7
+    assert np.abs(sv.probs() - O.probs(st)).max() < tol
+    for wires in ([0], [n - 1], [3, 1], [1, 3], [2, 7, 5], list(range(n))[::-1], [0, 1, 2, 3, 4, 5, 6, 8, 9, 10],
+                  list(range(1, n))):
+        assert np.abs(sv.probs(wires) - O.probs(st, wires)).max() < tol * 10, wires
+
+
+@pytest.mark.parametrize("dtype", [np.complex128, np.complex64])
+def test_pauli_sums_and_hamiltonians(capi, dtype):
+    import lq_oracle as O
+    rng = np.random.default_rng(4)
+    n = 10
+    st = random_state(rng, n, dtype)
+    sv = capi.StateVector(n, dtype)
+    sv.upload(st)
+    st64 = st.astype(np.complex128)
+    words = [("Z", [0]), ("X", [3]), ("Y", [9]), ("ZZ", [1, 2]), ("XY", [0, 9]), ("YYZ", [4, 2, 6]),
+             ("XX", [5, 8]), ("IZ", [3, 4]), ("ZXZ", [0, 5, 9])]
+    coeffs = rng.normal(size=len(words))
+    per, tot = sv.expval_pauli(words, coeffs)
+    want = [O.pauli_expval(st64, wd, ws) for wd, ws in words]
+    tol = 1e-12 if dtype == np.complex128 else 1e-6
+    assert np.abs(per - want).max() < tol
+    assert abs(tot - float(np.dot(coeffs, want))) < tol * 10
+    ham = [(float(c), [({"X": "PauliX", "Y": "PauliY", "Z": "PauliZ", "I": "Identity"}[ch], [w])
+                       for ch, w in zip(wd, ws)]) for c, (wd, ws) in zip(coeffs, words)]
+    assert abs(sv.expval(ham) - O.expval(st64, ham)) < tol * 10
+    assert abs(sv.var(ham) - O.var(st64, ham)) < tol * 20
+    # non-Pauli named observables and Hermitian matrices
+    herm = rng.normal(size=(4, 4)) + 1j * rng.normal(size=(4, 4))
+    herm = herm + herm.conj().T
+    for terms in ([(1.0, [("Hadamard", [2])])], [(1.0, [("Hermitian", [1, 7], herm)])],
+                  [(1.0, [("PauliX", [0]), ("Hermitian", [1, 7], herm)])],
+                  [(0.5, [("Hadamard", [3])]), (-2.0, [("Hermitian", [1, 7], herm)])],
+                  [(1.0, [("PauliZ", [4])])]):
+        assert abs(sv.expval(terms) - O.expval(st64, terms)) < tol * 100
+        assert abs(sv.var(terms) - O.var(st64, terms)) < tol * 100
+
+
+def test_inner_product_norm(capi):
+    rng = np.random.default_rng(6)
+    n = 12
+    a, b = random_state(rng, n), random_state(rng, n)
+    sa, sb = capi.StateVector(n), capi.StateVector(n)
+    sa.upload(a)
+    sb.upload(b)
+    assert abs(sa.inner(sb) - np.vdot(a, b)) < 1e-13
+    assert abs(sa.norm2() - 1.0) < 1e-13
+
+
+@pytest.mark.parametrize("dtype", [np.complex128, np.complex64])
+@pytest.mark.parametrize("n", [1, 3, 5, 6, 10, 16])
+def test_sampling_bit_exact(capi, n, dtype):
+    import lq_oracle as O
+    rng = np.random.default_rng(30 + n)
+    st = random_state(rng, n, dtype)
+    # make some probabilities exactly zero (the rule's edge cases)
+    st[rng.choice(st.size, st.size // 4, replace=False)] = 0
+    st /= np.linalg.norm(st.astype(np.complex128))
+    st = st.astype(dtype)
+    sv = capi.StateVector(n, dtype)
+    sv.upload(st)
+    u = rng.uniform(size=20000)
+    u[:4] = [0.0, 1e-300, np.nextafter(1.0, 0), 0.5]
+    cdf = O.cdf_fixed_order(st)
+    want = O.sample_kokkos_rule(cdf, u)
+    got = sv.sample(len(u), uniforms=u)
+    assert np.array_equal(got, want)
+    bits = sv.sample_bits(len(u), uniforms=u)
+    assert np.array_equal(bits, O.indices_to_bits(want, n))
+    # device Philox draws == oracle Philox draws
+    got_p = sv.sample(5000, seed=1234567)
+    want_p = O.sample_kokkos_rule(cdf, O.philox_uniforms(5000, 1234567))
+    assert np.array_equal(got_p, want_p)
+
+
+def test_sampling_distribution(capi):
+    """Histogram of 10^5 shots vs probabilities, margin 0.05 (Test_MeasurementsBase.cpp:364-424)."""
+    sv = capi.StateVector(3)
+    sv.apply_ops(nontrivial_state_ops())
+    p = sv.probs()
+    idx = sv.sample(100000, seed=99)
+    hist = np.bincount(idx.astype(np.int64), minlength=8) / 1e5
+    assert np.allclose(hist, p, atol=0.05)
+    assert np.allclose(p, [0.67078706, 0.03062806, 0.0870997, 0.00397696, 0.17564072, 0.00801973,
+                           0.02280642, 0.00104134], atol=1e-6)
