@@ -117,8 +117,7 @@ def test_random_circuit_vs_oracle(capi, dtype, ref_module=None):
                 ("SingleExcitation", [2, 5], False, [0.6]), ("SingleExcitationMinus", [0, 1], False, [1.1]),
                 ("SingleExcitationPlus", [6, 7], True, [0.35]), ("MultiRZ", [0, 3, 6], False, [0.45]),
                 ("DoubleExcitation", [0, 2, 4, 6], False, [0.7]), ("DoubleExcitationMinus", [1, 3, 5, 7], False, [0.2]),
-                ("DoubleExcitationPlus", [7, 5, 3, 1], True, [1.7]), ("Hadamard", [2], False, []),
-                ("QubitUnitary", [1, 6], False, [], __import__("lightning_b200.workloads", fromlist=["x"]).random_unitary(rng, 2))]
+                ("DoubleExcitationPlus", [7, 5, 3, 1], True, [1.7]), ("Hadamard", [2], False, [])]
     obs = [Zs(0), [(1.0, [("PauliX", [3]), ("PauliY", [5])])],
            [(0.4, [("PauliZ", [2]), ("PauliZ", [3])]), (-1.1, [("PauliX", [7])]), (0.2, [("Hadamard", [4])])]]
     npar = sum(1 for o in ops if len(o[3]) > 0)
@@ -133,6 +132,13 @@ def test_random_circuit_vs_oracle(capi, dtype, ref_module=None):
         final = O.run_circuit(n, ops)
         rj = ref.adjoint_jacobian(m, final.copy(), ops, obs, tp)
         assert np.abs(got - rj).max() < 1e-12
+    # matrix operations are not differentiated but must be undone exactly in the reverse sweep
+    from lightning_b200.workloads import random_unitary
+    ops2 = ops + [("QubitUnitary", [1, 6], False, [], random_unitary(rng, 2)), ("RY", [6], False, [0.4])]
+    npar2 = npar + 1
+    want2 = O.adjoint_jacobian(O.zero_state(n), ops2, obs, list(range(npar2)), apply_operations=True)
+    got2 = jac(capi, n, ops2, obs, list(range(npar2)), dtype)
+    assert np.abs(got2 - want2).max() < tol
 
 
 def test_layered_rotations_vs_fd(capi):

@@ -11,7 +11,7 @@ pytestmark = pytest.mark.gpu
 
 def small_hea(dtype, seed=3):
     from lightning_b200.workloads import hea_batch
-    return hea_batch(ncirc=24, nmin=2, nmax=15 if dtype == np.complex64 else 14, dmin=1, dmax=3, seed=seed)
+    return hea_batch(ncirc=24, nmin=3, nmax=15 if dtype == np.complex64 else 14, dmin=1, dmax=3, seed=seed)
 
 
 def mixed_batch(seed=8):
