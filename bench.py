@@ -1,0 +1,363 @@
+#!/usr/bin/env python
+"""Benchmark: batched adjoint circuits/s vs the plain path, and 30-qubit gate HBM GB/s.
+
+Headline (``value``): the batched adjoint workload — 1024 circuits of 16 qubits,
+8 layers of Rot(phi, theta, omega) on every qubit (serialised RZ RY RZ) plus a
+CNOT ring of layer-dependent range, 16 PauliZ observables per circuit,
+complex64 with FP64 reductions — one step = batched forward expectation values
+plus the adjoint vector-Jacobian product through torch.autograd, inputs resident
+in HBM.  Reported beside it: the plain per-circuit complex128 path (one gate per
+launch, the drop-in C ABI), the max gradient error against FP64, the 30-qubit
+complex128 gate sweep with the dense-gate roofline, the end-to-end number
+through the public API with host buffers, and the reference CPU path timed on
+this host.
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+(N > 1 runs N independent replicas under torchrun, one per GPU; weak scaling.)
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path[:0] = [str(ROOT / "lightning-unification_b200"), str(ROOT / "oracle")]
+
+METRIC = "batched adjoint circuits/s vs plain on B200 @1e-5; 30q gate HBM GB/s %peak"
+WORKLOAD = dict(ncirc=1024, n=16, layers=8, seed=5)
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+# ----------------------------------------------------------------------------
+class Clocks:
+    """Samples SM clocks and throttle reasons with nvidia-smi during a timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                                       "--format=csv,noheader,nounits", "-lms", "100"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.p:
+            self.p.terminate()
+            self.p.wait()
+
+    def summary(self):
+        self.f.seek(0)
+        rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.strip()]
+        sm, mx, reasons = [], 0.0, set()
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx = max(mx, float(r[2]))
+                names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+                for nm, v in zip(names, r[5:9]):
+                    if v.strip().lower() == "active":
+                        reasons.add(nm)
+            except (ValueError, IndexError):
+                continue
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ----------------------------------------------------------------------------
+def reference_cpu(circuits, params, dy, nsample, dtype=np.complex64):
+    """The reference's own CPU path on a bounded sample: forward with its StateVector,
+    16 expectation values, and the adjoint VJP as one Hamiltonian observable
+    (lightning_qubit.py:747-772).  Falls back to the NumPy port when oracle/_ref is absent."""
+    import ref
+    from lightning_b200.workloads import bind
+    m = ref.load()
+    kind = "reference" if m is not None else "port"
+    threads = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    for ci in range(nsample):
+        c = circuits[ci]
+        ops = bind(c, params)
+        nobs = len(c["observables"])
+        w = dy[ci * nobs:(ci + 1) * nobs]
+        ham = [[(float(w[o]), [("PauliZ", [o])]) for o in range(nobs)]]
+        npo = sum(1 for p in c["param_index"] if p >= 0)
+        if m is not None:
+            st = ref.run_circuit(m, c["num_qubits"], ops, dtype)
+            sv = getattr(m, "StateVector" + ("C64" if dtype == np.complex64 else "C128"))(st)
+            M = getattr(m, "Measurements" + ("C64" if dtype == np.complex64 else "C128"))(sv)
+            _ = [M.expval("PauliZ", [o]) for o in range(nobs)]
+            ref.adjoint_jacobian(m, st, ops, ham, list(range(npo)))
+        else:
+            import lq_oracle as O
+            st = O.run_circuit(c["num_qubits"], ops, dtype)
+            _ = [O.expval(st, [(1.0, [("PauliZ", [o])])]) for o in range(nobs)]
+            O.adjoint_jacobian(st, ops, ham, list(range(npo)))
+    dt = time.perf_counter() - t0
+    return {"value": nsample / dt, "unit": "circuits/s", "cores": threads if kind == "reference" else 1,
+            "kind": kind, "sample": f"{nsample} of {len(circuits)} circuits, forward + 16 expvals + adjoint VJP, "
+            f"complex64, OMP_NUM_THREADS={os.environ.get('OMP_NUM_THREADS', 'unset')}", "seconds": dt}
+
+
+def run_reference_arm(args):
+    from lightning_b200.workloads import rot_ring_batch
+    circuits, params = rot_ring_batch(**WORKLOAD)
+    rng = np.random.default_rng(0)
+    dy = rng.normal(size=len(circuits) * WORKLOAD["n"])
+    nsample = 4
+    for _ in range(args.warmup):
+        reference_cpu(circuits, params, dy, 1)
+    t0 = time.perf_counter()
+    res = None
+    for _ in range(args.steps):
+        res = reference_cpu(circuits, params, dy, nsample)
+    dt = (time.perf_counter() - t0) / args.steps
+    v = nsample / dt
+    line = {"metric": METRIC, "impl": "reference", "value": v, "unit": "circuits/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "c64", "data": "synthetic (seeded)",
+            "config": {"workload": "batched adjoint, 1024 circuits x 16 qubits x 8 Rot layers + CNOT rings, "
+                       "16 PauliZ observables, complex64", "sample_per_step": nsample},
+            "cpu_baseline": {k: res[k] for k in ("kind", "cores", "sample")} | {"value": v, "unit": "circuits/s"},
+            "e2e": {"value": v, "unit": "circuits/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ----------------------------------------------------------------------------
+def timed(fn, steps, warmup, stream=None):
+    import torch
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps  # ms
+
+
+def gate_sweep_30q(nq: int, hbm_peak: float):
+    """Per-gate HBM throughput at nq qubits (complex128); roofline of the dense 1-qubit gate kernel."""
+    import torch
+    from lightning_b200 import capi
+    from lightning_b200.workloads import gate_sweep, random_unitary
+    sv = capi.StateVector(nq, np.complex128)
+    stream = torch.cuda.current_stream()
+    sv.set_stream(stream.cuda_stream)
+    N = 1 << nq
+    state_bytes = 16 * N
+    rng = np.random.default_rng(0)
+    u2, u3 = random_unitary(rng, 2), random_unitary(rng, 3)
+    kinds = {
+        "Hadamard": lambda: sv.apply("Hadamard", [nq // 2]),
+        "RX": lambda: sv.apply("RX", [3], False, [0.3]),
+        "RY(wire n-1)": lambda: sv.apply("RY", [nq - 1], False, [0.3]),
+        "RZ": lambda: sv.apply("RZ", [7], False, [0.3]),
+        "CNOT": lambda: sv.apply("CNOT", [2, nq - 3]),
+        "CZ": lambda: sv.apply("CZ", [5, 9]),
+        "SWAP": lambda: sv.apply("SWAP", [1, nq - 2]),
+        "Toffoli": lambda: sv.apply("Toffoli", [0, 4, nq - 1]),
+        "U2": lambda: sv.apply_matrix(u2, [6, nq - 5]),
+        "U3": lambda: sv.apply_matrix(u3, [2, 11, nq - 7]),
+    }
+    # amplitudes each gate can change (algorithmic bytes = 2 x 16 B x that count)
+    touched = {"Hadamard": N, "RX": N, "RY(wire n-1)": N, "RZ": N, "CNOT": N // 2, "CZ": N // 4, "SWAP": N // 2,
+               "Toffoli": N // 4, "U2": N, "U3": N}
+    per = {}
+    for k, f in kinds.items():
+        ms = timed(f, 5, 2, stream)
+        per[k] = {"ms": ms, "gbs_touched": 2 * 16 * touched[k] / (ms * 1e6), "gbs_state": 2 * state_bytes / (ms * 1e6)}
+    ops = gate_sweep(nq, 200, seed=7)
+    sv.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    sv.apply_ops(ops)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    sweep_ms = e0.elapsed_time(e1)
+    dense = per["RX"]
+    roof = {"bound": "hbm", "kernel": f"k_dense<double,1> (RX, {nq} qubits complex128)",
+            "achieved": dense["gbs_touched"], "peak": hbm_peak, "unit": "GB/s",
+            "frac": dense["gbs_touched"] / hbm_peak, "traffic": None,
+            "algorithmic_bytes_per_launch": 2 * state_bytes}
+    sv.close()
+    return per, sweep_ms, roof
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--sweep-qubits", type=int, default=30)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        if rank == 0:
+            run_reference_arm(args)
+        return
+
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    from lightning_b200 import capi
+    from lightning_b200.batch import BatchedCircuits
+    from lightning_b200.autograd import batched_expval
+    from lightning_b200.workloads import rot_ring_batch, bind
+
+    hbm_peak, peak_kind = peaks()
+    circuits, params_np = rot_ring_batch(**WORKLOAD)
+    ncirc, n = WORKLOAD["ncirc"], WORKLOAD["n"]
+    eng = BatchedCircuits(circuits, len(params_np), dtype=np.complex64, use_graphs=True)
+    params = torch.tensor(params_np, dtype=torch.float64, device="cuda", requires_grad=True)
+    rng = np.random.default_rng(0)
+    dy_np = rng.normal(size=eng.total_obs)
+    dy = torch.tensor(dy_np, dtype=torch.float64, device="cuda")
+    tuned = eng.autotune(params.detach())
+
+    def step():
+        out = batched_expval(params, eng)
+        (g,) = torch.autograd.grad(out, params, dy)
+        return out, g
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clk = Clocks(local)
+    with clk:
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            out, g = step()
+        e1.record()
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    value = world * ncirc / (ms / 1e3)
+
+    # end to end through the public API: params from pinned host memory, results back to the host
+    params_host = torch.tensor(params_np, dtype=torch.float64).pin_memory()
+    dy_host = torch.tensor(dy_np, dtype=torch.float64).pin_memory()
+    out_host = torch.empty(eng.total_obs, dtype=torch.float64).pin_memory()
+    grad_host = torch.empty(len(params_np), dtype=torch.float64).pin_memory()
+
+    def e2e_step():
+        p = params_host.to("cuda", non_blocking=True).requires_grad_(True)
+        d = dy_host.to("cuda", non_blocking=True)
+        o = batched_expval(p, eng)
+        (gg,) = torch.autograd.grad(o, p, d)
+        out_host.copy_(o.detach(), non_blocking=True)
+        grad_host.copy_(gg, non_blocking=True)
+    e2e_ms = timed(e2e_step, args.steps, args.warmup)
+    h2d = (params_host.numel() + dy_host.numel()) * 8
+    d2h = (out_host.numel() + grad_host.numel()) * 8
+
+    if rank != 0:
+        if dist:
+            dist.destroy_process_group()
+        return
+
+    # plain per-circuit complex128 GPU path: one gate per launch through the C ABI
+    nplain = 8
+    sv = capi.StateVector(n, np.complex128)
+    grads_plain = []
+    t0 = time.perf_counter()
+    for ci in range(nplain):
+        c = circuits[ci]
+        ops = bind(c, params_np)
+        sv.set_basis_state(0)
+        sv.apply_ops(ops)
+        sv.expval_pauli([("Z", [q]) for q in range(n)])
+        w = dy_np[ci * n:(ci + 1) * n]
+        ham = [[(float(w[q]), [("PauliZ", [q])]) for q in range(n)]]
+        npo = sum(1 for p in c["param_index"] if p >= 0)
+        grads_plain.append(sv.adjoint_jacobian(ops, ham, list(range(npo)))[0])
+    plain_s = time.perf_counter() - t0
+    plain_value = nplain / plain_s
+    # gradient accuracy of the batched complex64 path against FP64 (plain complex128, oracle-checked)
+    g_np = g.detach().cpu().numpy()
+    err = 0.0
+    for ci in range(nplain):
+        slots = [p for p in circuits[ci]["param_index"] if p >= 0]
+        err = max(err, float(np.abs(g_np[slots] - grads_plain[ci]).max()))
+    sv.close()
+
+    per, sweep_ms, roof = gate_sweep_30q(args.sweep_qubits, hbm_peak)
+    roof["peak_kind"] = peak_kind
+
+    cpu = None if args.no_cpu else reference_cpu(circuits, params_np, dy_np, 4)
+    line = {
+        "metric": METRIC, "value": value, "unit": "circuits/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "c64 (fp32-pair compensated gates, fp64 reductions)",
+        "data": "synthetic (seeded)",
+        "config": {"workload": "batched adjoint: 1024 circuits x 16 qubits x 8 layers Rot(RZ RY RZ) + CNOT ring "
+                               "(range (l mod 15)+1), 16 PauliZ observables, forward + VJP per step",
+                   "circuits_per_gpu": ncirc, "qubits": n, "params_per_circuit": 3 * n * WORKLOAD["layers"],
+                   "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (1 GiB of live states per step)",
+                   "autotuned_config": tuned},
+        "plain": {"value": plain_value, "unit": "circuits/s", "dtype": "c128", "sample_circuits": nplain,
+                  "path": "C ABI, one gate per launch: apply_ops + 16 Pauli expvals + adjoint VJP"},
+        "ratio_vs_plain": value / world / plain_value,
+        "max_grad_err_vs_fp64": err,
+        "gate_sweep": {"qubits": args.sweep_qubits, "dtype": "c128", "per_gate": per,
+                       "sweep_200_gates_ms": sweep_ms, "fused": None},
+        "roofline": roof,
+        "cpu_baseline": cpu,
+        "e2e": {"value": world * ncirc / (e2e_ms / 1e3), "unit": "circuits/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h},
+        "gpu_launches": 3 * args.steps,
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -137,8 +137,9 @@ int b200sv_create(uint32_t num_qubits, int dtype, b200sv_handle *out);
 int b200sv_destroy(b200sv_handle h);
 int b200sv_num_qubits(b200sv_handle h, uint32_t *out);
 int b200sv_dtype(b200sv_handle h, int *out);
-/* Run the handle's work on an external stream (e.g. torch's current stream);
- * pass NULL to return to the handle's own stream. */
+/* Run the handle's work on `cuda_stream` from now on (e.g. torch's current
+ * stream).  NULL selects the legacy default stream, which torch uses unless told
+ * otherwise.  Until the first call the handle runs on a private stream. */
 int b200sv_set_stream(b200sv_handle h, void *cuda_stream);
 int b200sv_synchronize(b200sv_handle h);
 /* Device address of the amplitudes (complex<T>[2^n]) for zero-copy interop. */
@@ -244,6 +245,7 @@ int b200sv_batch_create(int dtype, const b200sv_batch_circuit *circuits,
                         uint32_t ncircuits, uint64_t nparams,
                         b200sv_batch_handle *out);
 int b200sv_batch_destroy(b200sv_batch_handle b);
+/* Same stream rule as b200sv_set_stream (NULL = legacy default stream). */
 int b200sv_batch_set_stream(b200sv_batch_handle b, void *cuda_stream);
 /* Forward: params_device (nparams doubles on the device) -> out_device
  * (sum over circuits of nobs doubles, circuit-major). */

@@ -1,0 +1,91 @@
+// MeasurementsB200.hpp — Measurements<StateVectorT> of lightning.qubit
+// (LQ/measurements/MeasurementsLQubit.hpp:61-641, CS/measurements/MeasurementsBase.hpp:42-106)
+// on the C ABI.  Expectation values are fused read-only reductions on the
+// device instead of copy + apply + inner product.
+#pragma once
+
+#include <random>
+
+#include "ObservablesB200.hpp"
+
+namespace Pennylane::LightningB200 {
+
+template <class StateVectorT> class Measurements {
+    using PrecisionT = typename StateVectorT::PrecisionT;
+    using ComplexT = typename StateVectorT::ComplexT;
+    const StateVectorT &sv_;
+
+    PrecisionT run_expval(const std::vector<TermData<PrecisionT>> &t) const {
+        ObsRecord<PrecisionT> r(t);
+        double out = 0;
+        check(b200sv_expval(sv_.handle(), &r.rec, &out));
+        return (PrecisionT)out;
+    }
+    PrecisionT run_var(const std::vector<TermData<PrecisionT>> &t) const {
+        ObsRecord<PrecisionT> r(t);
+        double out = 0;
+        check(b200sv_var(sv_.handle(), &r.rec, &out));
+        return (PrecisionT)out;
+    }
+
+  public:
+    explicit Measurements(const StateVectorT &sv) : sv_(sv) {}
+
+    // :79-88
+    std::vector<PrecisionT> probs() const { return probs({}); }
+    // :98-136 (wires[0] is the most significant bit of the result index)
+    std::vector<PrecisionT> probs(const std::vector<size_t> &wires) const {
+        std::vector<uint32_t> w(wires.begin(), wires.end());
+        const size_t k = wires.empty() ? sv_.getNumQubits() : wires.size();
+        std::vector<double> out(size_t(1) << k);
+        check(b200sv_probs(sv_.handle(), w.data(), (uint32_t)w.size(), out.data()));
+        return {out.begin(), out.end()};
+    }
+    // :167-180
+    PrecisionT expval(const std::string &name, const std::vector<size_t> &wires) const {
+        return run_expval({TermData<PrecisionT>{1.0, {FactorData<PrecisionT>{true, name, wires, {}}}}});
+    }
+    // :145-158
+    PrecisionT expval(const std::vector<ComplexT> &matrix, const std::vector<size_t> &wires) const {
+        return run_expval({TermData<PrecisionT>{1.0, {FactorData<PrecisionT>{false, "Hermitian", wires, matrix}}}});
+    }
+    // :248-265
+    PrecisionT expval(const Observable<StateVectorT> &ob) const { return run_expval(ob.terms()); }
+    // :218-240
+    template <typename op_type>
+    std::vector<PrecisionT> expval(const std::vector<op_type> &ops, const std::vector<std::vector<size_t>> &wires) const {
+        if (ops.size() != wires.size())
+            throw LightningException("The lengths of the list of operations and wires do not match.");
+        std::vector<PrecisionT> r;
+        for (size_t i = 0; i < ops.size(); ++i) r.push_back(expval(ops[i], wires[i]));
+        return r;
+    }
+    // :273-372
+    PrecisionT var(const Observable<StateVectorT> &ob) const { return run_var(ob.terms()); }
+    PrecisionT var(const std::string &name, const std::vector<size_t> &wires) const {
+        return run_var({TermData<PrecisionT>{1.0, {FactorData<PrecisionT>{true, name, wires, {}}}}});
+    }
+    PrecisionT var(const std::vector<ComplexT> &matrix, const std::vector<size_t> &wires) const {
+        return run_var({TermData<PrecisionT>{1.0, {FactorData<PrecisionT>{false, "Hermitian", wires, matrix}}}});
+    }
+    // generate_samples (:482-558 signature and output layout; sampling rule of
+    // LK/measurements/MeasuresFunctors.hpp:70-103 with device Philox draws).
+    std::vector<size_t> generate_samples(size_t num_samples, uint64_t seed) const {
+        const size_t n = sv_.getNumQubits();
+        std::vector<uint64_t> bits(num_samples * n);
+        check(b200sv_sample_bits(sv_.handle(), num_samples, nullptr, seed, bits.data()));
+        return {bits.begin(), bits.end()};
+    }
+    std::vector<size_t> generate_samples(size_t num_samples) const {
+        return generate_samples(num_samples, std::random_device{}());
+    }
+    // seeded variant taking caller uniforms (bit-exact reproducibility)
+    std::vector<size_t> generate_samples_from_uniforms(const std::vector<double> &u) const {
+        const size_t n = sv_.getNumQubits();
+        std::vector<uint64_t> bits(u.size() * n);
+        check(b200sv_sample_bits(sv_.handle(), u.size(), u.data(), 0, bits.data()));
+        return {bits.begin(), bits.end()};
+    }
+};
+
+}  // namespace Pennylane::LightningB200

@@ -542,7 +542,8 @@ struct Batch {
     int dtype = B200SV_C128;
     int device = 0;
     cudaStream_t own = nullptr, ext = nullptr;
-    cudaStream_t stream() const { return ext ? ext : own; }
+    bool has_ext = false;  // set_stream called: ext (NULL = legacy default stream)
+    cudaStream_t stream() const { return has_ext ? ext : own; }
     uint64_t nparams = 0;
     uint32_t ncirc = 0;
     Config cfg;
@@ -1059,18 +1060,22 @@ template <class F> void run_maybe_graph(Batch &B, cudaGraphExec_t &exec, F &&enq
         return;
     }
     if (!exec) {
+        // Capture on the batch's private non-blocking stream (the legacy default
+        // stream cannot be captured); the instantiated graph then launches on
+        // the caller's stream, ordered with its other work.
         cudaGraph_t g = nullptr;
-        B200SV_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        B200SV_CUDA(cudaStreamBeginCapture(B.own, cudaStreamCaptureModeThreadLocal));
         try {
-            enqueue(st);
+            enqueue(B.own);
         } catch (...) {
-            cudaStreamEndCapture(st, &g);
+            cudaStreamEndCapture(B.own, &g);
             if (g) cudaGraphDestroy(g);
             throw;
         }
-        B200SV_CUDA(cudaStreamEndCapture(st, &g));
-        B200SV_CUDA(cudaGraphInstantiate(&exec, g, 0));
+        B200SV_CUDA(cudaStreamEndCapture(B.own, &g));
+        const cudaError_t e = cudaGraphInstantiate(&exec, g, 0);
         cudaGraphDestroy(g);
+        B200SV_CUDA(e);
     }
     B200SV_CUDA(cudaGraphLaunch(exec, st));
 }
@@ -1168,10 +1173,8 @@ int b200sv_batch_destroy(b200sv_batch_handle b) {
 int b200sv_batch_set_stream(b200sv_batch_handle b, void *s) {
     return run_guarded([&] {
         if (!b) throw ArgError("NULL batch");
-        if (b->b->ext != static_cast<cudaStream_t>(s)) {
-            b->b->ext = static_cast<cudaStream_t>(s);
-            // graphs are instantiated per stream use; keep them (launchable on any stream)
-        }
+        b->b->ext = static_cast<cudaStream_t>(s);
+        b->b->has_ext = true;  // instantiated graphs launch on any stream
     });
 }
 

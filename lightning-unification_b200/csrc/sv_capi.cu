@@ -21,6 +21,7 @@ struct b200sv_state {
     int device = 0;
     cudaStream_t own = nullptr;
     cudaStream_t ext = nullptr;
+    bool has_ext = false;          // set_stream called: ext (NULL = legacy default stream)
     void *d_state = nullptr;
     double *d_partials = nullptr;  // kPartialsCapacity doubles
     double *d_small = nullptr;     // small results (kSmall doubles)
@@ -28,7 +29,7 @@ struct b200sv_state {
     void *d_matrix = nullptr;      // dense matrix staging
     size_t matrix_bytes = 0;
     void *d_scratch[2] = {nullptr, nullptr};  // two state-sized work buffers (lazy)
-    cudaStream_t stream() const { return ext ? ext : own; }
+    cudaStream_t stream() const { return has_ext ? ext : own; }
     size_t amp_bytes() const { return dtype == B200SV_C64 ? 8 : 16; }
     size_t state_bytes() const { return amp_bytes() << nq; }
 };
@@ -460,6 +461,7 @@ int b200sv_set_stream(b200sv_handle h, void *s) {
     return guard([&] {
         check_handle(h);
         h->ext = static_cast<cudaStream_t>(s);
+        h->has_ext = true;
     });
 }
 int b200sv_synchronize(b200sv_handle h) {
