@@ -583,7 +583,14 @@ int b200sv_probs_device(b200sv_handle h, const uint32_t *wires, uint32_t nwires,
         } else {
             need(wires != nullptr, "NULL wires");
             check_wires(wires, nwires, h->nq, "probs");
-            for (uint32_t j = 0; j < nwires; ++j) bits.push_back(bitpos(wires[j], h->nq));
+            // Output bit r belongs to wire wires[s[s[r]]], s = argsort(wires): the
+            // reference sums over the sorted wires and then applies
+            // transpose_state_tensor(probs, s) (MeasurementsLQubit.hpp:98-136,
+            // CS/utils/Util.hpp:465-496), which is this order.
+            std::vector<uint32_t> s(nwires);
+            for (uint32_t j = 0; j < nwires; ++j) s[j] = j;
+            std::stable_sort(s.begin(), s.end(), [&](uint32_t a, uint32_t b) { return wires[a] < wires[b]; });
+            for (uint32_t r = 0; r < nwires; ++r) bits.push_back(bitpos(wires[s[s[r]]], h->nq));
         }
         if (h->dtype == B200SV_C64)
             reduce_probs<float>(h->d_state, h->nq, bits, h->d_partials, kPartialsCapacity, out_device, h->stream());
