@@ -212,6 +212,36 @@ def gate_sweep_30q(nq: int, hbm_peak: float):
     return per, sweep_ms, roof
 
 
+def run_case(args):
+    """Small single-kernel cases for profiling: `gate` applies RX to a complex128 state of
+    --qubits qubits; `batch` runs forward + VJP of --ncirc circuits of the batched workload."""
+    import torch
+    from lightning_b200 import capi
+    torch.cuda.set_device(0)
+    if args.case == "gate":
+        sv = capi.StateVector(args.qubits, np.complex128)
+        st = torch.cuda.current_stream()
+        sv.set_stream(st.cuda_stream)
+        ms = timed(lambda: sv.apply("RX", [3], False, [0.3]), args.steps, args.warmup, st)
+        gbs = 2 * 16 * (1 << args.qubits) / (ms * 1e6)
+        print(json.dumps({"case": "gate", "kernel": "k_dense<double,1>", "qubits": args.qubits, "ms": ms,
+                          "gbs": gbs}))
+        return
+    from lightning_b200.batch import BatchedCircuits
+    from lightning_b200.autograd import batched_expval
+    from lightning_b200.workloads import rot_ring_batch
+    circuits, params_np = rot_ring_batch(**(WORKLOAD | {"ncirc": args.ncirc}))
+    eng = BatchedCircuits(circuits, len(params_np), dtype=np.complex64, use_graphs=False)
+    params = torch.tensor(params_np, dtype=torch.float64, device="cuda", requires_grad=True)
+    dy = torch.ones(eng.total_obs, dtype=torch.float64, device="cuda")
+
+    def step():
+        out = batched_expval(params, eng)
+        torch.autograd.grad(out, params, dy)
+    ms = timed(step, args.steps, args.warmup)
+    print(json.dumps({"case": "batch", "ncirc": args.ncirc, "ms": ms, "circuits_per_s": args.ncirc / (ms / 1e3)}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -220,8 +250,15 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--sweep-qubits", type=int, default=30)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--case", default="full", choices=["full", "gate", "batch"],
+                    help="gate / batch: one kernel family on a small case (profiling)")
+    ap.add_argument("--qubits", type=int, default=28, help="--case gate: state width (complex128)")
+    ap.add_argument("--ncirc", type=int, default=148, help="--case batch: number of circuits")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.case != "full":
+        run_case(args)
+        return
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
