@@ -209,6 +209,26 @@ int b200sv_sample(b200sv_handle h, uint64_t nshots, const double *uniforms,
 int b200sv_sample_bits(b200sv_handle h, uint64_t nshots, const double *uniforms,
                        uint64_t seed, uint64_t *bits_out);
 
+/* Allocation-free Pauli-word expectation values.  No counterpart in the
+ * reference: this entry point exists for callers that cannot call cudaMalloc
+ * when they need the result (device memory owned by another allocator such as
+ * PyTorch's caching allocator, serving loops that must not hit cudaMalloc's
+ * implicit synchronisation, hosts that forbid allocation after start-up).
+ * state_device: 2^num_qubits amplitudes of `dtype` owned by the caller;
+ * out_device: nterms doubles owned by the caller, receiving <psi|P_t|psi>;
+ * words as in b200sv_expval_pauli.  At most B200SV_NOALLOC_MAX_TERMS words per
+ * call (more is rejected with an error).  Work is queued on cuda_stream (NULL =
+ * legacy default stream) and not synchronised.  Scratch is one static device
+ * array shared by all calls: calls that overlap on the GPU race, so serialise
+ * them; the first call on a device sets up the array's address and should come
+ * before any stream capture. */
+#define B200SV_NOALLOC_MAX_TERMS 32
+int b200sv_expval_pauli_noalloc(const void *state_device, uint32_t num_qubits,
+                                int dtype, uint32_t nterms,
+                                const uint32_t *offsets, const uint32_t *wires,
+                                const char *paulis, double *out_device,
+                                void *cuda_stream);
+
 /* ---- adjoint Jacobian: LQ/algorithms/AdjointJacobianLQubit.hpp:212-335 ---- */
 /* jac (nobs x ntp doubles, [obs][param]) for the state in `psi` (unchanged).
  * With apply_operations != 0 the ops are applied to a copy of psi first.

@@ -110,6 +110,8 @@ _SIGS = {
                        C.POINTER(C.c_uint64)], C.c_int),
     "b200sv_sample_bits": ([C.c_void_p, C.c_uint64, C.POINTER(C.c_double), C.c_uint64,
                             C.POINTER(C.c_uint64)], C.c_int),
+    "b200sv_expval_pauli_noalloc": ([C.c_void_p, C.c_uint32, C.c_int, C.c_uint32, C.POINTER(C.c_uint32),
+                                     C.POINTER(C.c_uint32), C.c_char_p, C.c_void_p, C.c_void_p], C.c_int),
     "b200sv_adjoint_jacobian": ([C.c_void_p, C.POINTER(Op), C.c_uint32, C.POINTER(Observable), C.c_uint32,
                                  C.POINTER(C.c_uint64), C.c_uint32, C.c_int, C.POINTER(C.c_double)], C.c_int),
     "b200sv_batch_create": ([C.c_int, C.POINTER(BatchCircuit), C.c_uint32, C.c_uint64,
