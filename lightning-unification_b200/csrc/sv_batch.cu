@@ -41,6 +41,10 @@ constexpr int kMaxObsPerCircuit = 16;
 struct DOp {
     uint8_t form, gate, nb, inv;
     uint8_t nt, gform, gnb, gk;
+    uint8_t maxbit;      // highest tile bit the gate (or its generator) touches
+    uint8_t run;         // >= 2: first of `run` single-wire gates on bit `rbit` fused into one pass
+    uint8_t rbit;
+    uint8_t gcode;       // run members' generator: 1 X, 2 Y, 3 Z, 4 |1><1| (0: none / general)
     uint16_t low[4];     // insertion masks of the gate bits (ascending)
     uint16_t glow[2];    // insertion masks of the generator bits
     uint32_t cmask;      // control bits (must be set)
@@ -56,8 +60,8 @@ struct DOp {
 
 struct DSeg {
     uint32_t op_begin, nops;
-    uint8_t lbits[kMaxKt];   // tile bit j -> state bit
-    uint8_t gbits[40];       // tile index bit j -> state bit
+    uint8_t lbits[kMaxKt];   // tile bit j -> state bit (ascending)
+    uint8_t gbits[40];       // tile index bit j -> state bit (ascending)
     uint8_t nl, ng;
 };
 
@@ -76,6 +80,8 @@ struct DTerm {
     uint64_t xmask, zmask;
 };
 
+constexpr int kMaxRun = 3;
+
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ uint32_t ins_local(uint32_t g, const uint16_t *low, int nb) {
 #pragma unroll
@@ -88,9 +94,20 @@ __device__ __forceinline__ uint32_t ins_local(uint32_t g, const uint16_t *low, i
     return g;
 }
 
+// Per-parameter trigonometry, computed once per launch: (cos t/2, sin t/2, cos t, sin t).
+__global__ void k_trig(const double *__restrict__ params, uint64_t n, double4 *__restrict__ cs) {
+    for (uint64_t p = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; p < n; p += (uint64_t)gridDim.x * blockDim.x) {
+        double s, c, s2, c2;
+        sincos(0.5 * params[p], &s, &c);
+        sincos(params[p], &s2, &c2);
+        cs[p] = make_double4(c, s, c2, s2);
+    }
+}
+
+// Coefficients of a gate (or of its adjoint): MAT1 -> 4, MAT2 -> 16, DIAG -> 2^nt, PARITY -> 2.
 template <typename R>
-__device__ void op_coeffs(const DOp &op, const double *__restrict__ params, const double2 *__restrict__ consts,
-                          bool adj, C<R> *m) {
+__device__ __forceinline__ void op_coeffs(const DOp &op, const double4 *__restrict__ cs,
+                                          const double2 *__restrict__ consts, bool adj, C<R> *m) {
     if (op.gate == kConstGate) {
         const double2 *c = consts + (size_t)op.cidx * 16;
         if (op.form == F_MAT1 || op.form == F_MAT2) {
@@ -105,12 +122,9 @@ __device__ void op_coeffs(const DOp &op, const double *__restrict__ params, cons
         }
         return;
     }
-    const double th = params[op.pslot];
+    const double4 q = cs[op.pslot];
     const double sg = ((op.inv != 0) != adj) ? -1.0 : 1.0;
-    double s, c;
-    sincos(0.5 * th, &s, &c);
-    s *= sg;
-    const R cr = (R)c, sr = (R)s, z = (R)0, one = (R)1;
+    const R cr = (R)q.x, sr = (R)(sg * q.y), z = (R)0, one = (R)1;
     switch (op.gate) {
     case B200SV_RX: case B200SV_CRX:
         m[0] = mk<R>(cr, z); m[1] = mk<R>(z, -sr); m[2] = mk<R>(z, -sr); m[3] = mk<R>(cr, z); break;
@@ -118,12 +132,8 @@ __device__ void op_coeffs(const DOp &op, const double *__restrict__ params, cons
         m[0] = mk<R>(cr, z); m[1] = mk<R>(-sr, z); m[2] = mk<R>(sr, z); m[3] = mk<R>(cr, z); break;
     case B200SV_RZ: case B200SV_CRZ: case B200SV_MultiRZ:
         m[0] = mk<R>(cr, -sr); m[1] = mk<R>(cr, sr); break;
-    case B200SV_PhaseShift: case B200SV_ControlledPhaseShift: {
-        double s2, c2;
-        sincos(th, &s2, &c2);
-        m[0] = mk<R>((R)c2, (R)(sg * s2));
-        break;
-    }
+    case B200SV_PhaseShift: case B200SV_ControlledPhaseShift:
+        m[0] = mk<R>((R)q.z, (R)(sg * q.w)); break;
     case B200SV_IsingZZ:
         m[0] = mk<R>(cr, -sr); m[1] = mk<R>(cr, sr); m[2] = mk<R>(cr, sr); m[3] = mk<R>(cr, -sr); break;
     default: {
@@ -152,13 +162,54 @@ __device__ void op_coeffs(const DOp &op, const double *__restrict__ params, cons
     }
 }
 
-// apply one gate (or its adjoint, coefficients already conjugated) to NS tiles in shared memory
+// 2x2 matrix of a run member (single-wire gate on the run bit), or of its adjoint.
+template <typename R>
+__device__ __forceinline__ void member_mat(const DOp &op, const double4 *__restrict__ cs,
+                                           const double2 *__restrict__ consts, bool adj, C<R> (&m)[4]) {
+    const C<R> zero = mk<R>(0, 0), one = mk<R>(1, 0);
+    if (op.form == F_SWAP) {
+        m[0] = zero; m[1] = one; m[2] = one; m[3] = zero;
+        return;
+    }
+    C<R> t[16];
+    op_coeffs<R>(op, cs, consts, adj, t);
+    if (op.form == F_MAT1) {
+        m[0] = t[0]; m[1] = t[1]; m[2] = t[2]; m[3] = t[3];
+    } else if (op.nt == 1) {  // diagonal on the bit
+        m[0] = t[0]; m[1] = zero; m[2] = zero; m[3] = t[1];
+    } else {                  // phase on |1> of the bit
+        m[0] = one; m[1] = zero; m[2] = zero; m[3] = t[0];
+    }
+}
+
+// Iteration range of a step's groups: warp-local steps (every touched bit below
+// wl) keep each warp inside its own 2^wl-amplitude block, so consecutive
+// warp-local steps only need __syncwarp; other steps spread over the block.
+struct Range {
+    uint32_t g0, g1, gs;
+};
+__device__ __forceinline__ Range groups(int kt, int wl, int nb, bool wloc) {
+    Range r;
+    if (wloc) {
+        const uint32_t per = 1u << (wl - nb);
+        r.g0 = (threadIdx.x >> 5) * per + (threadIdx.x & 31);
+        r.g1 = ((threadIdx.x >> 5) + 1) * per;
+        r.gs = 32;
+    } else {
+        r.g0 = threadIdx.x;
+        r.g1 = 1u << (kt - nb);
+        r.gs = blockDim.x;
+    }
+    return r;
+}
+
+// apply one gate (coefficients already adjointed when needed) to NS tiles
 template <typename R, int NS>
-__device__ __forceinline__ void apply_tile(C<R> *const (&s)[NS], int kt, const DOp &op, const C<R> *m) {
+__device__ __forceinline__ void apply_op(C<R> *const (&s)[NS], int kt, int wl, bool wloc, const DOp &op, const C<R> *m) {
     if (op.form == F_NOOP) return;
     if (op.form == F_PARITY) {
-        const uint32_t n = 1u << kt;
-        for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+        const Range rg = groups(kt, wl, 0, wloc);
+        for (uint32_t i = rg.g0; i < rg.g1; i += rg.gs) {
             const C<R> f = m[__popc(i & op.pmask) & 1];
 #pragma unroll
             for (int q = 0; q < NS; ++q) {
@@ -169,8 +220,8 @@ __device__ __forceinline__ void apply_tile(C<R> *const (&s)[NS], int kt, const D
         }
         return;
     }
-    const uint32_t ng = 1u << (kt - op.nb);
-    for (uint32_t g = threadIdx.x; g < ng; g += blockDim.x) {
+    const Range rg = groups(kt, wl, op.nb, wloc);
+    for (uint32_t g = rg.g0; g < rg.g1; g += rg.gs) {
         const uint32_t base = ins_local(g, op.low, op.nb) | op.cmask;
 #pragma unroll
         for (int q = 0; q < NS; ++q) {
@@ -200,10 +251,13 @@ __device__ __forceinline__ void apply_tile(C<R> *const (&s)[NS], int kt, const D
             }
             case F_DIAG: {
                 const int rows = 1 << op.nt;
-                for (int r = 0; r < rows; ++r) {
-                    CAcc<R> a;
-                    a.add(m[r], t[base + op.off[r]]);
-                    t[base + op.off[r]] = a.get();
+#pragma unroll
+                for (int r = 0; r < 4; ++r) {
+                    if (r < rows) {
+                        CAcc<R> a;
+                        a.add(m[r], t[base + op.off[r]]);
+                        t[base + op.off[r]] = a.get();
+                    }
                 }
                 break;
             }
@@ -221,12 +275,12 @@ __device__ __forceinline__ void apply_tile(C<R> *const (&s)[NS], int kt, const D
 
 // per-thread part of Im<bra|G|ket> on one tile, FP64
 template <typename R>
-__device__ __forceinline__ double gen_inner_tile(const C<R> *bra, const C<R> *ket, int kt, const DOp &op,
-                                                 const double2 *__restrict__ consts) {
+__device__ __forceinline__ double gen_inner(const C<R> *bra, const C<R> *ket, int kt, int wl, bool wloc, const DOp &op,
+                                            const double2 *__restrict__ consts) {
     double acc = 0.0;
     if (op.gform == G_PARITY) {
-        const uint32_t n = 1u << kt;
-        for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+        const Range rg = groups(kt, wl, 0, wloc);
+        for (uint32_t i = rg.g0; i < rg.g1; i += rg.gs) {
             const double2 k = widen<R>(ket[i]), b = widen<R>(bra[i]);
             const double sg = (__popc(i & op.pmask) & 1) ? -1.0 : 1.0;
             acc += sg * (b.x * k.y - b.y * k.x);
@@ -235,8 +289,8 @@ __device__ __forceinline__ double gen_inner_tile(const C<R> *bra, const C<R> *ke
     }
     const double2 *G = consts + (size_t)op.gcidx * 16;
     const int D = 1 << op.gk;
-    const uint32_t ng = 1u << (kt - op.gnb);
-    for (uint32_t g = threadIdx.x; g < ng; g += blockDim.x) {
+    const Range rg = groups(kt, wl, op.gnb, wloc);
+    for (uint32_t g = rg.g0; g < rg.g1; g += rg.gs) {
         const uint32_t base = ins_local(g, op.glow, op.gnb);
         double2 v[4];
         for (int r = 0; r < D; ++r) v[r] = widen<R>(ket[base + op.goff[r]]);
@@ -254,21 +308,118 @@ __device__ __forceinline__ double gen_inner_tile(const C<R> *bra, const C<R> *ke
     return acc;
 }
 
-__device__ __forceinline__ uint64_t deposit(uint32_t v, const uint8_t *bits, int nb) {
-    uint64_t r = 0;
-    for (int j = 0; j < nb; ++j)
-        if (v & (1u << j)) r |= uint64_t(1) << bits[j];
-    return r;
+__device__ __forceinline__ void add_grad(double *gradw, int32_t gslot, double p, bool first) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) p += __shfl_down_sync(0xffffffffu, p, off);
+    if ((threadIdx.x & 31) == 0) {
+        double *slot = gradw + (size_t)gslot * (blockDim.x >> 5) + (threadIdx.x >> 5);
+        *slot = first ? p : *slot + p;
+    }
 }
-__device__ __forceinline__ uint64_t deposit64(uint64_t v, const uint8_t *bits, int nb) {
-    uint64_t r = 0;
-    for (int j = 0; j < nb; ++j)
-        if (v & (uint64_t(1) << j)) r |= uint64_t(1) << bits[j];
-    return r;
+
+// Im(conj(b) . G a) over one amplitude pair for the run generators X, Y, Z, |1><1|.
+__device__ __forceinline__ double pair_gen_im(int code, double2 a0, double2 a1, double2 b0, double2 b1) {
+    // w = G a;  Im(conj(b) w) = b.x w.y - b.y w.x
+    switch (code) {
+    case 1: return b0.x * a1.y - b0.y * a1.x + b1.x * a0.y - b1.y * a0.x;        // w = (a1, a0)
+    case 2: return -(b0.x * a1.x + b0.y * a1.y) + (b1.x * a0.x + b1.y * a0.y);   // w = (-i a1, i a0)
+    case 3: return b0.x * a0.y - b0.y * a0.x - (b1.x * a1.y - b1.y * a1.x);      // w = (a0, -a1)
+    default: return b1.x * a1.y - b1.y * a1.x;                                    // w = (0, a1)
+    }
+}
+
+// A run of `len` single-wire gates on bit rb, applied per amplitude pair in registers.
+// Forward: the run's product is formed once in FP64 and applied as one 2x2 matrix.
+// Adjoint: the members are undone one by one with the generator products between them.
+template <typename R, int NS, bool REV>
+__device__ void exec_run(C<R> *const (&s)[NS], int kt, int wl, bool wloc, const DOp *__restrict__ ops, int len,
+                         const double4 *__restrict__ cs, const double2 *__restrict__ consts, double *gradw,
+                         bool first_tile) {
+    const int rb = ops[0].rbit;
+    const uint32_t low = (1u << rb) - 1;
+    const uint32_t bit = 1u << rb;
+    const Range rg = groups(kt, wl, 1, wloc);
+    if (!REV) {
+        // product M = m_{len-1} ... m_0 in FP64
+        double2 P[4] = {make_double2(1, 0), make_double2(0, 0), make_double2(0, 0), make_double2(1, 0)};
+        for (int k = 0; k < len; ++k) {
+            C<double> q[4];
+            member_mat<double>(ops[k], cs, consts, false, q);
+            double2 Q[4];
+            for (int r = 0; r < 2; ++r)
+                for (int c = 0; c < 2; ++c) {
+                    const double2 x0 = q[r * 2 + 0], x1 = q[r * 2 + 1], y0 = P[0 * 2 + c], y1 = P[1 * 2 + c];
+                    Q[r * 2 + c] = make_double2(x0.x * y0.x - x0.y * y0.y + x1.x * y1.x - x1.y * y1.y,
+                                                x0.x * y0.y + x0.y * y0.x + x1.x * y1.y + x1.y * y1.x);
+                }
+            P[0] = Q[0]; P[1] = Q[1]; P[2] = Q[2]; P[3] = Q[3];
+        }
+        C<R> m[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) m[i] = mk<R>((R)P[i].x, (R)P[i].y);
+        for (uint32_t g = rg.g0; g < rg.g1; g += rg.gs) {
+            const uint32_t i0 = ((g & ~low) << 1) | (g & low), i1 = i0 | bit;
+#pragma unroll
+            for (int q = 0; q < NS; ++q) {
+                const C<R> a0 = s[q][i0], a1 = s[q][i1];
+                CAcc<R> p, r;
+                p.add(m[0], a0); p.add(m[1], a1);
+                r.add(m[2], a0); r.add(m[3], a1);
+                s[q][i0] = p.get();
+                s[q][i1] = r.get();
+            }
+        }
+        return;
+    }
+    // adjoint sweep: register copies in reverse order
+    C<R> m[kMaxRun][4];
+    double ip[kMaxRun];
+    int gc[kMaxRun];
+#pragma unroll
+    for (int kk = 0; kk < kMaxRun; ++kk) {
+        ip[kk] = 0.0;
+        gc[kk] = 0;
+        if (kk < len) {
+            const DOp &op = ops[len - 1 - kk];
+            member_mat<R>(op, cs, consts, true, m[kk]);
+            if (op.gslot >= 0) gc[kk] = op.gcode;
+        }
+    }
+    for (uint32_t g = rg.g0; g < rg.g1; g += rg.gs) {
+        const uint32_t i0 = ((g & ~low) << 1) | (g & low), i1 = i0 | bit;
+        C<R> a0 = s[0][i0], a1 = s[0][i1], b0 = s[NS - 1][i0], b1 = s[NS - 1][i1];
+#pragma unroll
+        for (int kk = 0; kk < kMaxRun; ++kk) {
+            if (kk < len) {
+                if (gc[kk]) ip[kk] += pair_gen_im(gc[kk], widen<R>(a0), widen<R>(a1), widen<R>(b0), widen<R>(b1));
+                CAcc<R> p, q, u, v;
+                p.add(m[kk][0], a0); p.add(m[kk][1], a1);
+                q.add(m[kk][2], a0); q.add(m[kk][3], a1);
+                u.add(m[kk][0], b0); u.add(m[kk][1], b1);
+                v.add(m[kk][2], b0); v.add(m[kk][3], b1);
+                a0 = p.get(); a1 = q.get(); b0 = u.get(); b1 = v.get();
+            }
+        }
+        s[0][i0] = a0;
+        s[0][i1] = a1;
+        s[NS - 1][i0] = b0;
+        s[NS - 1][i1] = b1;
+    }
+#pragma unroll
+    for (int kk = 0; kk < kMaxRun; ++kk)
+        if (kk < len && gc[kk]) add_grad(gradw, ops[len - 1 - kk].gslot, ip[kk], first_tile);
+}
+
+__device__ __forceinline__ uint64_t insert_zeros64(uint64_t v, const uint8_t *bits, int nb) {
+    for (int j = 0; j < nb; ++j) {
+        const uint64_t lo = v & ((uint64_t(1) << bits[j]) - 1);
+        v = ((v ^ lo) << 1) | lo;
+    }
+    return v;
 }
 
 // sum_t coeff_t <psi|P_t|psi> per observable into acc[obs] (per-thread part)
-template <typename R, bool GLOBAL>
+template <typename R>
 __device__ void expval_terms(const C<R> *psi, uint64_t n_amp, const DTerm *__restrict__ terms, uint32_t nterms,
                              double (&acc)[kMaxObsPerCircuit]) {
     for (uint32_t t = 0; t < nterms; ++t) {
@@ -326,11 +477,12 @@ struct KArgs {
     const uint32_t *order;
     uint32_t ncirc;
     uint32_t *counter;
-    const double *params;
+    const double4 *cs;    // per-parameter trigonometry
     const double *dy;     // [sum nobs] (VJP)
     double *out;          // forward: [sum nobs]
     double *gradw;        // VJP: [ngslots * nwarps]
     void *pool_a, *pool_b;
+    const int *reuse;     // VJP: nonzero when pool A still holds this step's forward states
     int mode;             // 0 forward, 1 vjp
     int max_kt;
 };
@@ -341,39 +493,77 @@ template <typename R> __device__ __forceinline__ void zero_tile(C<R> *s, uint32_
 
 template <typename R>
 __device__ void load_tile(C<R> *dst, const C<R> *__restrict__ src, const DSeg &sg, uint64_t tbase, uint32_t nt) {
-    for (uint32_t l = threadIdx.x; l < nt; l += blockDim.x) dst[l] = src[tbase | deposit(l, sg.lbits, sg.nl)];
+    for (uint32_t l = threadIdx.x; l < nt; l += blockDim.x) dst[l] = src[tbase | insert_zeros64(l, sg.gbits, sg.ng)];
 }
 template <typename R>
 __device__ void store_tile(C<R> *__restrict__ dst, const C<R> *src, const DSeg &sg, uint64_t tbase, uint32_t nt) {
-    for (uint32_t l = threadIdx.x; l < nt; l += blockDim.x) dst[tbase | deposit(l, sg.lbits, sg.nl)] = src[l];
+    for (uint32_t l = threadIdx.x; l < nt; l += blockDim.x) dst[tbase | insert_zeros64(l, sg.gbits, sg.ng)] = src[l];
 }
 
-// one circuit, forward only: state ends in tile 0 (resident) or pool A (global)
+// Apply the gates of one segment to the tile(s): forward (NS = 1) or the adjoint
+// sweep over (lambda, bra) with gradient products (NS = 2, REV).
+template <typename R, int NS, bool REV>
+__device__ void exec_segment(const KArgs &A, C<R> *const (&tiles)[NS], int kt, const DSeg &sg, bool first_tile) {
+    const int wl = kt - (31 - __clz((int)(blockDim.x >> 5)));  // bits owned by one warp's block
+    C<R> m[16];
+    bool prev_wloc = false;
+    int o = REV ? (int)sg.nops - 1 : 0;
+    while (REV ? o >= 0 : o < (int)sg.nops) {
+        // find the step: a fused run (head op carries run >= 2) or a single gate
+        int head = o, len = 1;
+        if (REV) {
+            // walk back to the head of a run that ends at o
+            int h = o;
+            while (h > 0 && A.ops[sg.op_begin + h].run == 0) --h;
+            const DOp &hd = A.ops[sg.op_begin + h];
+            if (hd.run >= 2 && h + hd.run - 1 == o) {
+                head = h;
+                len = hd.run;
+            }
+        } else {
+            const DOp &hd = A.ops[sg.op_begin + o];
+            if (hd.run >= 2) len = hd.run;
+        }
+        const DOp *op0 = A.ops + sg.op_begin + head;
+        const bool wloc = wl >= 1 && op0->maxbit < wl && (len >= 2 || op0->nb <= wl);
+        if (prev_wloc && wloc) __syncwarp();
+        else __syncthreads();
+        if (len >= 2) {
+            exec_run<R, NS, REV>(tiles, kt, wl, wloc, op0, len, A.cs, A.consts, A.gradw, first_tile);
+        } else {
+            const DOp op = *op0;
+            if (REV && op.gslot >= 0) {
+                add_grad(A.gradw, op.gslot, gen_inner<R>(tiles[NS - 1], tiles[0], kt, wl, wloc, op, A.consts),
+                         first_tile);
+                if (wloc) __syncwarp();
+                else __syncthreads();
+            }
+            op_coeffs<R>(op, A.cs, A.consts, REV, m);
+            apply_op<R, NS>(tiles, kt, wl, wloc, op, m);
+        }
+        prev_wloc = wloc;
+        o = REV ? head - 1 : head + len;
+    }
+    __syncthreads();
+}
+
+// one circuit, forward: state ends in tile 0 (resident) or pool A (global)
 template <typename R>
 __device__ void run_forward(const KArgs &A, const DCirc &c, C<R> *sm, C<R> *pa) {
     const uint32_t tn = 1u << c.kt;
     C<R> *tiles[1] = {sm};
-    __shared__ C<R> coef[16];
     if (c.resident) {
         zero_tile<R>(sm, tn);
         __syncthreads();
         if (threadIdx.x == 0) sm[0] = mk<R>(1, 0);
-        __syncthreads();
-        const DSeg sg = A.segs[c.seg_begin];
-        for (uint32_t o = 0; o < sg.nops; ++o) {
-            const DOp op = A.ops[sg.op_begin + o];
-            if (threadIdx.x == 0) op_coeffs<R>(op, A.params, A.consts, false, coef);
-            __syncthreads();
-            apply_tile<R, 1>(tiles, c.kt, op, coef);
-            __syncthreads();
-        }
+        exec_segment<R, 1, false>(A, tiles, c.kt, A.segs[c.seg_begin], true);
         return;
     }
     const uint64_t ntiles = uint64_t(1) << (c.n - c.kt);
     for (uint32_t si = 0; si < c.nseg; ++si) {
         const DSeg sg = A.segs[c.seg_begin + si];
         for (uint64_t t = 0; t < ntiles; ++t) {
-            const uint64_t tbase = deposit64(t, sg.gbits, sg.ng);
+            const uint64_t tbase = insert_zeros64(t, sg.lbits, sg.nl);
             if (si == 0) {
                 zero_tile<R>(sm, tn);
                 __syncthreads();
@@ -381,14 +571,7 @@ __device__ void run_forward(const KArgs &A, const DCirc &c, C<R> *sm, C<R> *pa) 
             } else {
                 load_tile<R>(sm, pa, sg, tbase, tn);
             }
-            __syncthreads();
-            for (uint32_t o = 0; o < sg.nops; ++o) {
-                const DOp op = A.ops[sg.op_begin + o];
-                if (threadIdx.x == 0) op_coeffs<R>(op, A.params, A.consts, false, coef);
-                __syncthreads();
-                apply_tile<R, 1>(tiles, c.kt, op, coef);
-                __syncthreads();
-            }
+            exec_segment<R, 1, false>(A, tiles, c.kt, sg, true);
             store_tile<R>(pa, sm, sg, tbase, tn);
             __syncthreads();
         }
@@ -396,14 +579,12 @@ __device__ void run_forward(const KArgs &A, const DCirc &c, C<R> *sm, C<R> *pa) 
 }
 
 template <typename R>
-__global__ void k_batch(KArgs A) {
+__global__ void __launch_bounds__(512) k_batch(KArgs A) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ uint32_t s_next;
     __shared__ double s_red[kMaxObsPerCircuit * 32];
-    __shared__ C<R> coef[16];
     C<R> *sm0 = reinterpret_cast<C<R> *>(smem_raw);
     C<R> *sm1 = sm0 + (size_t(1) << A.max_kt);
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
     for (;;) {
         if (threadIdx.x == 0) s_next = atomicAdd(A.counter, 1u);
         __syncthreads();
@@ -414,13 +595,14 @@ __global__ void k_batch(KArgs A) {
         C<R> *pa = static_cast<C<R> *>(A.pool_a) + c.off_a;
         C<R> *pb = static_cast<C<R> *>(A.pool_b) + c.off_b;
         const uint64_t namp = uint64_t(1) << c.n;
-        run_forward<R>(A, c, sm0, pa);
+        const bool reuse = A.mode == 1 && !c.resident && A.reuse && *A.reuse != 0;
+        if (!reuse) run_forward<R>(A, c, sm0, pa);
         const C<R> *psi = c.resident ? sm0 : pa;
         if (A.mode == 0) {
             double acc[kMaxObsPerCircuit];
 #pragma unroll
             for (int o = 0; o < kMaxObsPerCircuit; ++o) acc[o] = 0.0;
-            expval_terms<R, false>(psi, namp, A.terms + c.term_begin, c.nterms, acc);
+            expval_terms<R>(psi, namp, A.terms + c.term_begin, c.nterms, acc);
             block_reduce<kMaxObsPerCircuit>(acc, s_red);
             if (threadIdx.x == 0)
                 for (uint32_t o = 0; o < c.nobs; ++o) A.out[c.out_begin + o] = acc[o];
@@ -431,56 +613,32 @@ __global__ void k_batch(KArgs A) {
         C<R> *bra = c.resident ? sm1 : pb;
         init_bra<R>(bra, psi, namp, A.terms + c.term_begin, c.nterms, A.dy + c.out_begin);
         __syncthreads();
+        C<R> *tiles[2] = {sm0, sm1};
         if (c.resident) {
-            C<R> *tiles[2] = {sm0, sm1};
-            const DSeg sg = A.segs[c.seg_begin];
-            for (int32_t o = (int32_t)sg.nops - 1; o >= 0; --o) {
-                const DOp op = A.ops[sg.op_begin + o];
-                if (op.gslot >= 0) {
-                    double p = gen_inner_tile<R>(sm1, sm0, c.kt, op, A.consts);
-#pragma unroll
-                    for (int off = 16; off > 0; off >>= 1) p += __shfl_down_sync(0xffffffffu, p, off);
-                    if (lane == 0) A.gradw[(size_t)op.gslot * nw + warp] = p;
-                }
-                if (threadIdx.x == 0) op_coeffs<R>(op, A.params, A.consts, true, coef);
-                __syncthreads();
-                apply_tile<R, 2>(tiles, c.kt, op, coef);
-                __syncthreads();
-            }
+            exec_segment<R, 2, true>(A, tiles, c.kt, A.segs[c.seg_begin], true);
             continue;
         }
         const uint64_t ntiles = uint64_t(1) << (c.n - c.kt);
         const uint32_t tn = 1u << c.kt;
-        C<R> *tiles[2] = {sm0, sm1};
         for (int32_t si = (int32_t)c.nseg - 1; si >= 0; --si) {
             const DSeg sg = A.segs[c.seg_begin + si];
             for (uint64_t t = 0; t < ntiles; ++t) {
-                const uint64_t tbase = deposit64(t, sg.gbits, sg.ng);
+                const uint64_t tbase = insert_zeros64(t, sg.lbits, sg.nl);
                 load_tile<R>(sm0, pa, sg, tbase, tn);
                 load_tile<R>(sm1, pb, sg, tbase, tn);
-                __syncthreads();
-                for (int32_t o = (int32_t)sg.nops - 1; o >= 0; --o) {
-                    const DOp op = A.ops[sg.op_begin + o];
-                    if (op.gslot >= 0) {
-                        double p = gen_inner_tile<R>(sm1, sm0, c.kt, op, A.consts);
-#pragma unroll
-                        for (int off = 16; off > 0; off >>= 1) p += __shfl_down_sync(0xffffffffu, p, off);
-                        if (lane == 0) {
-                            double *slot = A.gradw + (size_t)op.gslot * nw + warp;
-                            *slot = (t == 0) ? p : *slot + p;
-                        }
-                    }
-                    if (threadIdx.x == 0) op_coeffs<R>(op, A.params, A.consts, true, coef);
-                    __syncthreads();
-                    apply_tile<R, 2>(tiles, c.kt, op, coef);
-                    __syncthreads();
-                }
+                exec_segment<R, 2, true>(A, tiles, c.kt, sg, t == 0);
                 store_tile<R>(pa, sm0, sg, tbase, tn);
                 store_tile<R>(pb, sm1, sg, tbase, tn);
                 __syncthreads();
             }
         }
     }
+}
+
+// flag <- valid && all(a == b)   (the caller copies `valid` into `flag` first)
+__global__ void k_params_equal(const double *__restrict__ a, const double *__restrict__ b, uint64_t n, int *flag) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        if (a[i] != b[i]) *flag = 0;
 }
 
 // grad[p] = sum over ops referencing p (CSR order) of gscale * sum_w gradw[op, w]
@@ -574,6 +732,10 @@ struct Batch {
     uint64_t *d_jac_base = nullptr;
     double *d_dy_tmp = nullptr;
     double *d_params_in = nullptr, *d_dy_in = nullptr, *d_out = nullptr, *d_grad = nullptr;
+    double *d_params_fwd = nullptr;   // parameters of the last forward
+    double4 *d_cs = nullptr;          // per-parameter trigonometry
+    int *d_fwd_valid = nullptr;       // pool A holds the last forward's states
+    int *d_reuse = nullptr;           // per-VJP decision
     uint32_t ngslots = 0;
     size_t smem_bytes = 0;
     int grid = 0;
@@ -751,6 +913,10 @@ DOp lower(Planned &P, const HostOp &h, const std::vector<int> &loc /* state bit 
     d.gslot = -1;
     std::vector<uint32_t> lb(h.bits.size());
     for (size_t i = 0; i < h.bits.size(); ++i) lb[i] = (uint32_t)loc[h.bits[i]];
+    uint32_t mb = 0;
+    for (auto x : lb) mb = std::max(mb, x);
+    d.maxbit = (uint8_t)mb;  // every form, swaps included: decides warp-local scheduling
+    d.run = 1;
     // targets are the last nt bits of the reference wire order; the rest are controls
     const size_t nc = h.form == F_PARITY || h.form == F_NOOP ? 0 : lb.size() - h.nt;
     std::vector<uint32_t> tgt(lb.begin() + nc, lb.end()), ctl(lb.begin(), lb.begin() + nc);
@@ -803,6 +969,14 @@ DOp lower(Planned &P, const HostOp &h, const std::vector<int> &loc /* state bit 
         for (size_t i = 0; i < lb.size(); ++i) vw[i] = vq - 1 - lb[i];
         GateDesc G = compile_generator((uint32_t)h.gen, vw.data(), (uint32_t)vw.size(), vq, &sc);
         d.gscale = -2.0 * sc * (h.inv ? -1.0 : 1.0);
+        // single-wire generators get a code for the fused-run path
+        switch (h.gen) {
+        case 0: d.gcode = 4; break;  // PhaseShift: |1><1|
+        case 1: d.gcode = 1; break;  // RX: X
+        case 2: d.gcode = 2; break;  // RY: Y
+        case 3: d.gcode = 3; break;  // RZ: Z
+        default: d.gcode = 0; break;
+        }
         if (G.kind == Kind::Parity) {
             d.gform = G_PARITY;
             d.pmask = (uint32_t)G.pmask;
@@ -838,6 +1012,34 @@ DOp lower(Planned &P, const HostOp &h, const std::vector<int> &loc /* state bit 
         }
     }
     return d;
+}
+
+// Single-wire gate whose generator (if any) acts on the same wire: it can join
+// a run that is applied per amplitude pair in registers.
+int run_bit(const DOp &d) {
+    int bit = -1;
+    if (d.form == F_MAT1 && d.nb == 1 && d.cmask == 0) bit = d.maxbit;
+    else if (d.form == F_DIAG && d.nb == 1 && (d.nt == 1 ? d.cmask == 0 : d.nt == 0)) bit = d.maxbit;
+    else if (d.form == F_SWAP && d.nt == 1 && d.nb == 1 && d.cmask == 0) bit = d.maxbit;
+    if (bit < 0) return -1;
+    if (d.gslot >= 0 && d.gcode == 0) return -1;
+    return bit;
+}
+
+void mark_runs(DOp *ops, uint32_t n) {
+    uint32_t i = 0;
+    while (i < n) {
+        const int b = run_bit(ops[i]);
+        uint32_t j = i + 1;
+        if (b >= 0)
+            while (j < n && j - i < (uint32_t)kMaxRun && run_bit(ops[j]) == b) ++j;
+        if (j - i >= 2) {
+            ops[i].run = (uint8_t)(j - i);
+            for (uint32_t q = i; q < j; ++q) ops[q].rbit = (uint8_t)b;
+            for (uint32_t q = i + 1; q < j; ++q) ops[q].run = 0;
+        }
+        i = j;
+    }
 }
 
 Planned plan(const Batch &B, const Config &cfg, bool vjp) {
@@ -906,6 +1108,7 @@ Planned plan(const Batch &B, const Config &cfg, bool vjp) {
                 }
                 P.ops.push_back(d);
             }
+            mark_runs(P.ops.data() + s.op_begin, s.nops);
             P.segs.push_back(s);
             if (ops.empty()) break;
             i = j;
@@ -991,6 +1194,11 @@ void build_program(Batch &B, const Config &cfg) {
     upload(B, B.d_jac_base, B.jac_base);
     B.d_dy_tmp = B.dalloc<double>(B.total_obs);
     B.d_params_in = B.dalloc<double>(B.nparams);
+    B.d_params_fwd = B.dalloc<double>(B.nparams);
+    B.d_cs = B.dalloc<double4>(B.nparams);
+    B.d_fwd_valid = B.dalloc<int>(1);
+    B.d_reuse = B.dalloc<int>(1);
+    B200SV_CUDA(cudaMemset(B.d_fwd_valid, 0, sizeof(int)));
     B.d_dy_in = B.dalloc<double>(B.total_obs);
     B.d_out = B.dalloc<double>(B.total_obs);
     B.d_grad = B.dalloc<double>(B.nparams);
@@ -1015,7 +1223,15 @@ void build_program(Batch &B, const Config &cfg) {
     B200SV_CUDA(cudaDeviceSynchronize());
 }
 
-void launch_main(Batch &B, int mode, const double *params, const double *dy, double *out, cudaStream_t st) {
+// Per-parameter trigonometry for this launch (one k_trig pass over the batch parameters).
+void launch_trig(Batch &B, const double *params, cudaStream_t st) {
+    if (!B.nparams) return;
+    const uint64_t nb = std::min<uint64_t>((B.nparams + 255) / 256, 4096);
+    k_trig<<<(unsigned)nb, 256, 0, st>>>(params, B.nparams, B.d_cs);
+    B200SV_CUDA(cudaGetLastError());
+}
+
+void launch_main(Batch &B, int mode, const double *dy, double *out, const int *reuse, cudaStream_t st) {
     KArgs A{};
     A.circs = B.d_circs;
     A.segs = B.d_segs;
@@ -1025,12 +1241,13 @@ void launch_main(Batch &B, int mode, const double *params, const double *dy, dou
     A.order = B.d_order;
     A.ncirc = B.ncirc;
     A.counter = B.d_counter;
-    A.params = params;
+    A.cs = B.d_cs;
     A.dy = dy;
     A.out = out;
     A.gradw = B.d_gradw;
     A.pool_a = B.d_pool_a;
     A.pool_b = B.d_pool_b;
+    A.reuse = reuse;
     A.mode = mode;
     int mk = 1;
     for (auto &c : B.h_circs) mk = std::max<int>(mk, (int)c.kt);
@@ -1041,11 +1258,30 @@ void launch_main(Batch &B, int mode, const double *params, const double *dy, dou
     B200SV_CUDA(cudaGetLastError());
 }
 
+// Forward: expectation values; the final states of circuits wider than a tile stay
+// in pool A, and a copy of the parameters marks them valid for the next VJP.
 void enqueue_forward(Batch &B, cudaStream_t st) {
-    launch_main(B, 0, B.d_params_in, nullptr, B.d_out, st);
+    launch_trig(B, B.d_params_in, st);
+    launch_main(B, 0, nullptr, B.d_out, nullptr, st);
+    if (B.nparams)
+        B200SV_CUDA(cudaMemcpyAsync(B.d_params_fwd, B.d_params_in, B.nparams * sizeof(double),
+                                    cudaMemcpyDeviceToDevice, st));
+    B200SV_CUDA(cudaMemsetAsync(B.d_fwd_valid, 1, sizeof(int), st));
 }
+
+// VJP: reuses pool A when it still holds the forward states of the same
+// parameters (decided on the device, so the recorded graph stays valid), then
+// invalidates it — the reverse sweep consumes those states.
 void enqueue_vjp(Batch &B, cudaStream_t st) {
-    launch_main(B, 1, B.d_params_in, B.d_dy_in, nullptr, st);
+    launch_trig(B, B.d_params_in, st);
+    B200SV_CUDA(cudaMemcpyAsync(B.d_reuse, B.d_fwd_valid, sizeof(int), cudaMemcpyDeviceToDevice, st));
+    if (B.nparams) {
+        const uint64_t nb = std::min<uint64_t>((B.nparams + 255) / 256, 4096);
+        k_params_equal<<<(unsigned)nb, 256, 0, st>>>(B.d_params_in, B.d_params_fwd, B.nparams, B.d_reuse);
+        B200SV_CUDA(cudaGetLastError());
+    }
+    launch_main(B, 1, B.d_dy_in, nullptr, B.d_reuse, st);
+    B200SV_CUDA(cudaMemsetAsync(B.d_fwd_valid, 0, sizeof(int), st));
     const int nw = B.cfg.threads / 32;
     const uint64_t np = std::max<uint64_t>(B.nparams, 1);
     k_grad_params<<<(unsigned)std::min<uint64_t>((np + 255) / 256, 4096), 256, 0, st>>>(
@@ -1196,7 +1432,7 @@ int b200sv_batch_forward(b200sv_batch_handle bh, const double *params, double *o
             B200SV_CUDA(cudaMemcpyAsync(B.d_params_in, params, B.nparams * sizeof(double), cudaMemcpyDeviceToDevice, st));
         run_maybe_graph(B, B.g_forward, [&](cudaStream_t s) { enqueue_forward(B, s); });
         B200SV_CUDA(cudaMemcpyAsync(out, B.d_out, B.total_obs * sizeof(double), cudaMemcpyDeviceToDevice, st));
-        B.last_launches = 1;
+        B.last_launches = 2;  // k_trig, k_batch
     });
 }
 
@@ -1212,7 +1448,7 @@ int b200sv_batch_vjp(b200sv_batch_handle bh, const double *params, const double 
         run_maybe_graph(B, B.g_vjp, [&](cudaStream_t s) { enqueue_vjp(B, s); });
         if (B.nparams)
             B200SV_CUDA(cudaMemcpyAsync(grad, B.d_grad, B.nparams * sizeof(double), cudaMemcpyDeviceToDevice, st));
-        B.last_launches = 2;
+        B.last_launches = 4;  // k_trig, k_params_equal, k_batch, k_grad_params
     });
 }
 
@@ -1227,10 +1463,12 @@ int b200sv_batch_jacobian(b200sv_batch_handle bh, const double *params, double *
         uint32_t maxobs = 0;
         for (auto n : B.nobs) maxobs = std::max(maxobs, n);
         const int nw = B.cfg.threads / 32;
-        uint32_t launches = 0;
+        uint32_t launches = 1;
+        B200SV_CUDA(cudaMemsetAsync(B.d_fwd_valid, 0, sizeof(int), st));
+        launch_trig(B, B.d_params_in, st);
         for (uint32_t o = 0; o < maxobs; ++o) {
             k_onehot_dy<<<std::max(1u, (B.ncirc + 255) / 256), 256, 0, st>>>(B.d_dy_in, B.d_circs, B.ncirc, o);
-            launch_main(B, 1, B.d_params_in, B.d_dy_in, nullptr, st);
+            launch_main(B, 1, B.d_dy_in, nullptr, nullptr, st);
             if (B.ngslots)
                 k_grad_scatter<<<std::max(1u, (B.ngslots + 255) / 256), 256, 0, st>>>(
                     B.d_gscale, B.d_gradw, nw, B.ngslots, o, B.d_gslot_circ, B.d_circs, B.d_jac_base,
@@ -1252,7 +1490,7 @@ int b200sv_batch_autotune(b200sv_batch_handle bh, const double *params, int *cho
         std::vector<Config> cands;
         const int kts_c64[] = {11, 12, 13};
         const int kts_c128[] = {10, 11, 12};
-        for (int th : {256, 512, 1024})
+        for (int th : {256, 512})
             for (int i = 0; i < 3; ++i) cands.push_back(Config{th, B.dtype == B200SV_C64 ? kts_c64[i] : kts_c128[i]});
         float best = 1e30f;
         int best_i = -1;

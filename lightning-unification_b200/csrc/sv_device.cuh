@@ -46,42 +46,37 @@ struct Insert {
 
 // ---- accumulation policies ---------------------------------------------
 // complex128: plain FMA chains.
-// complex64: compensated dot products in FP32 pairs — every product is split
-// exactly with an FMA (TwoProduct) and every addition with Knuth's TwoSum; the
-// error terms are summed separately and added once at the end.  This is the
-// Dot2 algorithm of Ogita, Rump and Oishi, "Accurate sum and dot product",
-// SIAM J. Sci. Comput. 26(6), 2005; the result is as accurate as if computed in
-// twice the working precision and then rounded once.
-template <typename R> struct Acc;
-template <> struct Acc<double> {
-    double s = 0.0;
-    __device__ __forceinline__ void add_prod(double a, double b) { s = fma(a, b, s); }
-    __device__ __forceinline__ double get() const { return s; }
-};
-template <> struct Acc<float> {
-    float s = 0.0f, c = 0.0f;
-    __device__ __forceinline__ void add_prod(float a, float b) {
-        const float p = a * b;
-        const float ep = fmaf(a, b, -p);  // exact: a*b = p + ep
-        const float t = s + p;            // TwoSum(s, p) = t + et
-        const float z = t - s;
-        const float et = (s - (t - z)) + (p - z);
-        s = t;
-        c += ep + et;
+// complex64: each output is a compensated sum in FP32 pairs (value, error).
+// Every complex product term is formed with one FMA per component
+// (re = fma(a.x, b.x, -a.y*b.y), im = fma(a.x, b.y, a.y*b.x)), and the terms are
+// added with Knuth's TwoSum (D. E. Knuth, TAOCP vol. 2, 4.2.2), whose rounding
+// errors are carried in a second FP32 word and added once at the end — the
+// summation half of the Dot2 scheme of Ogita, Rump and Oishi, "Accurate sum and
+// dot product", SIAM J. Sci. Comput. 26(6), 2005.
+template <typename R> struct CAcc;
+template <> struct CAcc<double> {
+    double re = 0.0, im = 0.0;
+    __device__ __forceinline__ void add(double2 m, double2 v) {
+        re = fma(m.x, v.x, re);
+        re = fma(-m.y, v.y, re);
+        im = fma(m.x, v.y, im);
+        im = fma(m.y, v.x, im);
     }
-    __device__ __forceinline__ float get() const { return s + c; }
+    __device__ __forceinline__ double2 get() const { return make_double2(re, im); }
 };
-
-// out = sum_j m_j * v_j for complex m, v with the precision policy of R.
-template <typename R> struct CAcc {
-    Acc<R> re, im;
-    __device__ __forceinline__ void add(C<R> m, C<R> v) {
-        re.add_prod(m.x, v.x);
-        re.add_prod(-m.y, v.y);
-        im.add_prod(m.x, v.y);
-        im.add_prod(m.y, v.x);
+__device__ __forceinline__ void two_sum_acc(float &s, float &c, float t) {
+    const float u = s + t;
+    const float z = u - s;
+    c += (s - (u - z)) + (t - z);
+    s = u;
+}
+template <> struct CAcc<float> {
+    float sr = 0.0f, si = 0.0f, cr = 0.0f, ci = 0.0f;
+    __device__ __forceinline__ void add(float2 m, float2 v) {
+        two_sum_acc(sr, cr, fmaf(m.x, v.x, -(m.y * v.y)));
+        two_sum_acc(si, ci, fmaf(m.x, v.y, m.y * v.x));
     }
-    __device__ __forceinline__ C<R> get() const { return mk<R>(re.get(), im.get()); }
+    __device__ __forceinline__ float2 get() const { return make_float2(sr + cr, si + ci); }
 };
 
 // ---- deterministic FP64 block reduction -----------------------------------

@@ -161,3 +161,37 @@ def test_batch_rejects_bad_input():
     with pytest.raises(capi.B200Error, match="out of range"):
         BatchedCircuits([{"num_qubits": 2, "ops": [("RX", [0], False, [])], "param_index": [5],
                           "observables": [[(1.0, "Z", [0])]]}], 1)
+
+
+@pytest.mark.parametrize("dtype", [np.complex128, np.complex64])
+def test_batch_vjp_tiled_rot_ring(dtype):
+    """The benchmark's circuit family at 16 qubits: wider than a tile, so every circuit runs the
+    segmented HBM path with CNOT rings crossing tile bits; forward, VJP (which reuses the forward's
+    states) and a second VJP (which must recompute them) against the FP64 oracle."""
+    import torch
+    import lq_oracle as O
+    from lightning_b200.batch import BatchedCircuits
+    from lightning_b200.autograd import batched_expval
+    from lightning_b200.workloads import rot_ring_batch, bind, obs_terms
+    circuits, params = rot_ring_batch(ncirc=3, n=16, layers=3, seed=12)
+    eng = BatchedCircuits(circuits, len(params), dtype=dtype, use_graphs=True)
+    p = torch.tensor(params, dtype=torch.float64, device="cuda", requires_grad=True)
+    out = batched_expval(p, eng)
+    dy = np.random.default_rng(2).normal(size=out.numel())
+    (g,) = torch.autograd.grad(out, p, torch.tensor(dy, device="cuda"))
+    g2 = eng.vjp(p.detach(), torch.tensor(dy, device="cuda"))
+    want_out, want_g = [], np.zeros(len(params))
+    for ci, c in enumerate(circuits):
+        ops = bind(c, params)
+        obs = [obs_terms(o) for o in c["observables"]]
+        psi = O.run_circuit(16, ops)
+        want_out += [O.expval(psi, o) for o in obs]
+        npo = sum(1 for q in c["param_index"] if q >= 0)
+        ham = [[(float(dy[ci * 16 + q]), [("PauliZ", [q])]) for q in range(16)]]
+        jac = O.adjoint_jacobian(psi, ops, ham, list(range(npo)))[0]
+        slots = [q for q in c["param_index"] if q >= 0]
+        want_g[slots] = jac
+    tol_out, tol_g = (1e-11, 1e-10) if dtype == np.complex128 else (2e-5, 1e-4)
+    assert np.abs(out.detach().cpu().numpy() - want_out).max() < tol_out
+    assert np.abs(g.cpu().numpy() - want_g).max() < tol_g
+    assert np.abs(g2.cpu().numpy() - want_g).max() < tol_g
