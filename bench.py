@@ -196,20 +196,33 @@ def gate_sweep_30q(nq: int, hbm_peak: float):
         ms = timed(f, 5, 2, stream)
         per[k] = {"ms": ms, "gbs_touched": 2 * 16 * touched[k] / (ms * 1e6), "gbs_state": 2 * state_bytes / (ms * 1e6)}
     ops = gate_sweep(nq, 200, seed=7)
-    sv.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    sv.apply_ops(ops)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    sweep_ms = e0.elapsed_time(e1)
+    sweep = {}
+    for label, fn in (("unfused", sv.apply_ops), ("fused", sv.apply_ops_fused)):
+        fn(ops[:10])  # warm
+        sv.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn(ops)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        sweep[label] = e0.elapsed_time(e1)
+    sweep_ms = sweep
     dense = per["RX"]
     roof = {"bound": "hbm", "kernel": f"k_dense<double,1> (RX, {nq} qubits complex128)",
             "achieved": dense["gbs_touched"], "peak": hbm_peak, "unit": "GB/s",
-            "frac": dense["gbs_touched"] / hbm_peak, "traffic": None,
+            "frac": dense["gbs_touched"] / hbm_peak,
+            "traffic": RX_DRAM_BYTES_26Q * float(1 << (nq - 26)),
+            "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one 26-qubit launch "
+                              "(profiles/k_dense_rx_c128_26q.md), scaled by the state size",
             "algorithmic_bytes_per_launch": 2 * state_bytes}
     sv.close()
     return per, sweep_ms, roof
+
+
+# DRAM bytes (read + write) of one k_dense<double,1> launch (RX) on a 26-qubit complex128
+# state, from an ncu capture; the kernel streams each amplitude once, so the traffic
+# grows in proportion to the state.
+RX_DRAM_BYTES_26Q = 1.0737e9 + 1.0137e9
 
 
 def run_case(args):
@@ -227,6 +240,19 @@ def run_case(args):
         print(json.dumps({"case": "gate", "kernel": "k_dense<double,1>", "qubits": args.qubits, "ms": ms,
                           "gbs": gbs}))
         return
+    if args.case == "fused":
+        from lightning_b200.workloads import gate_sweep, random_state
+        ops = gate_sweep(args.qubits, 200, seed=7)
+        sv = capi.StateVector(args.qubits, np.complex128)
+        sv.upload(random_state(args.qubits, seed=3))
+        st = torch.cuda.current_stream()
+        sv.set_stream(st.cuda_stream)
+        ol = capi.OpList(ops)
+        res = {"case": "fused", "qubits": args.qubits, "gates": len(ops)}
+        for name, fn in (("fused", sv.apply_ops_fused), ("unfused", sv.apply_ops)):
+            res[name + "_ms"] = timed(lambda: fn(ol), args.steps, args.warmup, st)
+        print(json.dumps(res))
+        return
     from lightning_b200.batch import BatchedCircuits
     from lightning_b200.autograd import batched_expval
     from lightning_b200.workloads import rot_ring_batch
@@ -242,6 +268,72 @@ def run_case(args):
     print(json.dumps({"case": "batch", "ncirc": args.ncirc, "ms": ms, "circuits_per_s": args.ncirc / (ms / 1e3)}))
 
 
+def hea_forward(steps: int, warmup: int, ncirc: int = 4096):
+    """Batched hardware-efficient-ansatz forward (n ~ U[10, 20], depth ~ U[4, 16], 3n-term
+    Hamiltonian), complex64, one persistent launch replayed as a CUDA graph, vs a per-circuit loop
+    through the plain C ABI on a sample."""
+    import torch
+    from lightning_b200 import capi
+    from lightning_b200.batch import BatchedCircuits
+    from lightning_b200.workloads import hea_batch, bind
+    circuits, params_np = hea_batch(ncirc=ncirc, seed=11)
+    eng = BatchedCircuits(circuits, len(params_np), dtype=np.complex64, use_graphs=True)
+    params = torch.tensor(params_np, dtype=torch.float64, device="cuda")
+    ms = timed(lambda: eng.forward(params), steps, warmup)
+    out = eng.forward(params).cpu().numpy()
+    nsample = 16
+    t0 = time.perf_counter()
+    plain, handles = [], {}
+    for c in circuits[:nsample]:
+        n = c["num_qubits"]
+        if n not in handles:
+            handles[n] = capi.StateVector(n, np.complex64)
+        sv = handles[n]
+        sv.set_basis_state(0)
+        sv.apply_ops(bind(c, params_np))
+        words = [(w, ws) for _, w, ws in c["observables"][0]]
+        coeffs = [cf for cf, _, _ in c["observables"][0]]
+        plain.append(sv.expval_pauli(words, coeffs)[1])
+    plain_s = time.perf_counter() - t0
+    for sv in handles.values():
+        sv.close()
+    err = float(np.abs(np.array(plain) - out[:nsample]).max())
+    return {"circuits": ncirc, "dtype": "c64", "value": ncirc / (ms / 1e3), "unit": "circuits/s",
+            "ms_per_step": ms, "per_circuit_loop": nsample / plain_s, "ratio": (ncirc / (ms / 1e3)) / (nsample / plain_s),
+            "max_abs_diff_vs_loop": err}
+
+
+def sampling_case(nq: int, shots: int = 10_000_000):
+    """RY layer + QFT-style ladder applied with the fused path, then `shots` samples by the
+    fixed-order inverse CDF (device Philox draws); chi-squared of the sampled top-10-wire marginal."""
+    import torch
+    from lightning_b200 import capi
+    from lightning_b200.workloads import qft_circuit
+    sv = capi.StateVector(nq, np.complex128)
+    st = torch.cuda.current_stream()
+    sv.set_stream(st.cuda_stream)
+    ops = qft_circuit(nq, seed=9)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    sv.apply_ops_fused(ops)
+    sv.synchronize()
+    t_gates = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    idx = sv.sample(shots, seed=2024)
+    t_sample = time.perf_counter() - t0
+    k = min(10, nq)
+    marg = sv.probs(list(range(k)))
+    hist = np.bincount((idx >> np.uint64(nq - k)).astype(np.int64), minlength=1 << k)
+    expct = marg * shots
+    mask = expct > 5
+    chi2 = float(((hist[mask] - expct[mask]) ** 2 / expct[mask]).sum())
+    dof = int(mask.sum()) - 1
+    sv.close()
+    return {"qubits": nq, "dtype": "c128", "gates": len(ops), "gates_fused_s": t_gates, "shots": shots,
+            "sample_s": t_sample, "shots_per_s": shots / t_sample, "chi2": chi2, "chi2_dof": dof,
+            "chi2_per_dof": chi2 / max(dof, 1)}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -250,7 +342,7 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--sweep-qubits", type=int, default=30)
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--case", default="full", choices=["full", "gate", "batch"],
+    ap.add_argument("--case", default="full", choices=["full", "gate", "batch", "fused"],
                     help="gate / batch: one kernel family on a small case (profiling)")
     ap.add_argument("--qubits", type=int, default=28, help="--case gate: state width (complex128)")
     ap.add_argument("--ncirc", type=int, default=148, help="--case batch: number of circuits")
@@ -343,8 +435,8 @@ def main():
     nplain = 8
     sv = capi.StateVector(n, np.complex128)
     grads_plain = []
-    t0 = time.perf_counter()
-    for ci in range(nplain):
+
+    def plain_circuit(ci):
         c = circuits[ci]
         ops = bind(c, params_np)
         sv.set_basis_state(0)
@@ -353,7 +445,11 @@ def main():
         w = dy_np[ci * n:(ci + 1) * n]
         ham = [[(float(w[q]), [("PauliZ", [q])]) for q in range(n)]]
         npo = sum(1 for p in c["param_index"] if p >= 0)
-        grads_plain.append(sv.adjoint_jacobian(ops, ham, list(range(npo)))[0])
+        return sv.adjoint_jacobian(ops, ham, list(range(npo)))[0]
+    plain_circuit(nplain)  # warm-up: loads every kernel the plain path uses
+    t0 = time.perf_counter()
+    for ci in range(nplain):
+        grads_plain.append(plain_circuit(ci))
     plain_s = time.perf_counter() - t0
     plain_value = nplain / plain_s
     # gradient accuracy of the batched complex64 path against FP64 (plain complex128, oracle-checked)
@@ -368,6 +464,10 @@ def main():
     roof["peak_kind"] = peak_kind
 
     cpu = None if args.no_cpu else reference_cpu(circuits, params_np, dy_np, 4)
+    del eng
+    torch.cuda.empty_cache()
+    hea = hea_forward(3, 3)
+    samp = sampling_case(28)
     line = {
         "metric": METRIC, "value": value, "unit": "circuits/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
@@ -383,7 +483,10 @@ def main():
         "ratio_vs_plain": value / world / plain_value,
         "max_grad_err_vs_fp64": err,
         "gate_sweep": {"qubits": args.sweep_qubits, "dtype": "c128", "per_gate": per,
-                       "sweep_200_gates_ms": sweep_ms, "fused": None},
+                       "sweep_200_gates_ms": sweep_ms,
+                       "fused_speedup": sweep_ms["unfused"] / sweep_ms["fused"]},
+        "hea_batch_forward": hea,
+        "sampling": samp,
         "roofline": roof,
         "cpu_baseline": cpu,
         "e2e": {"value": world * ncirc / (e2e_ms / 1e3), "unit": "circuits/s", "h2d_bytes_per_step": h2d,

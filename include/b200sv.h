@@ -164,6 +164,15 @@ int b200sv_apply_matrix(b200sv_handle h, const void *matrix,
                         const uint32_t *wires, uint32_t nwires, int inverse);
 /* applyOperations: a list applied in order on the handle's stream. */
 int b200sv_apply_ops(b200sv_handle h, const b200sv_op *ops, uint32_t nops);
+/* applyOperations with gate fusion: the list is cut into segments whose wires
+ * fit in a shared-memory tile (2^12 complex128 / 2^13 complex64 amplitudes, the
+ * lowest wires filling the rest so loads coalesce), and each segment is one
+ * pass over HBM instead of one pass per gate.  Same results as
+ * b200sv_apply_ops to rounding (complex128: 1e-12).  Gates outside the tile
+ * forms (more than three wires, dense matrices on three wires) run as their own
+ * pass in order.  States narrower than the tile plus 8 wires use the per-gate
+ * path. */
+int b200sv_apply_ops_fused(b200sv_handle h, const b200sv_op *ops, uint32_t nops);
 /* applyGenerator (LQ/StateVectorLQubit.hpp:250-275): G applied in place (it is
  * not unitary for projector-type generators); *scale receives the factor of
  * GateImplementationsLM.hpp:1355-1639 / PauliGenerator.hpp:34-56. */
@@ -195,11 +204,27 @@ int b200sv_inner_product(b200sv_handle bra, b200sv_handle ket, double *re,
                          double *im);
 /* ||psi||^2 in FP64. */
 int b200sv_norm2(b200sv_handle h, double *out);
+/* Sparse Hamiltonian H in CSR form (host arrays): row i holds the non-zeros
+ * [row_map[i] - row_map[0], row_map[i+1] - row_map[0]) of entries (column
+ * indices) and values (complex in the handle's dtype).  row_map_size must be
+ * 2^n + 1 ("Statevector and Hamiltonian have incompatible sizes." otherwise).
+ * expval = Re<psi|H psi>  (expval(row_map, ..., numNNZ),
+ * LQ/measurements/MeasurementsLQubit.hpp:197-214; binding
+ * LQ/bindings/LQubitBindings.hpp:127-138);
+ * var = <H psi|H psi> - Re<H psi|psi>^2  (var(row_map, ...), :451-472;
+ * binding LQubitBindings.hpp:150-161).  Accumulated in FP64. */
+int b200sv_expval_sparse(b200sv_handle h, const uint64_t *row_map,
+                         uint64_t row_map_size, const uint64_t *entries,
+                         const void *values, uint64_t nnz, double *out);
+int b200sv_var_sparse(b200sv_handle h, const uint64_t *row_map,
+                      uint64_t row_map_size, const uint64_t *entries,
+                      const void *values, uint64_t nnz, double *out);
 
 /* Sampling by inverse CDF (the lightning.kokkos rule,
  * LK/measurements/MeasuresFunctors.hpp:70-103 over an exclusive scan,
  * LK/measurements/MeasurementsKokkos.hpp:713-722).  p_i = re*re + im*im in FP64
- * without contraction; the scan order is fixed (see DESIGN), so the indices
+ * without contraction; the scan order is fixed (runs of 32 summed in sequence,
+ * recursively, offsets added top-down), so the indices
  * are a deterministic function of the state and the uniforms.
  * uniforms: nshots doubles in [0,1) on the host, or NULL to draw them on the
  * device from Philox4x32-10 with `seed`.  idx_out: nshots basis indices. */
@@ -238,6 +263,15 @@ int b200sv_adjoint_jacobian(b200sv_handle psi, const b200sv_op *ops,
                             uint32_t nobs, const uint64_t *trainable,
                             uint32_t ntrainable, int apply_operations,
                             double *jac);
+
+/* State-return vector-Jacobian product (LQ/algorithms/VectorJacobianProduct.hpp:60-156):
+ * vjp[j] = i * scale_p * <G_p mu | lambda> for trainable parameter p = trainable[j],
+ * where lambda starts from psi (after the ops when apply_operations != 0) and mu
+ * from the cotangent state dy (2^n complex<T> on the host); both are swept
+ * backwards through the ops.  out: ntrainable complex<double> as (re, im) pairs. */
+int b200sv_vjp_state(b200sv_handle psi, const b200sv_op *ops, uint32_t nops,
+                     const void *dy, uint64_t dy_length, const uint64_t *trainable,
+                     uint32_t ntrainable, int apply_operations, double *out);
 
 /* ---- batched engine ------------------------------------------------------ */
 /* A batch is a packed pool of independent circuits of uneven width, run by one

@@ -167,6 +167,9 @@ template <class T> void register_precision(py::module_ &m, py::module_ &obsm, py
 
     // ---- MeasurementsC* -------------------------------------------------------
     using M = Measurements<SV>;
+    // LQ/bindings/LQubitBindings.hpp:112-118: size_t indices, values in the state's precision
+    using SparseIdx = py::array_t<size_t, py::array::c_style | py::array::forcecast>;
+    using ArrC = py::array_t<std::complex<T>, py::array::c_style | py::array::forcecast>;
     auto sv_of = [](W &w) -> const SV & { return w.sv; };
     (void)sv_of;
     py::class_<M>(m, ("MeasurementsC" + bits).c_str(), py::module_local())
@@ -177,12 +180,22 @@ template <class T> void register_precision(py::module_ &m, py::module_ &obsm, py
              "Expected value of an observable object.")
         .def("expval", [](M &ms, const std::string &name, const std::vector<size_t> &w) { return ms.expval(name, w); },
              "Expected value of an operation by name.")
-        .def("expval",
-             [](M &, const py::array &, const py::array &, const py::array &) -> T {
-                 throw std::runtime_error("Sparse Hamiltonian observables are not supported by lightning_b200");
-             })
+        .def(
+            "expval",
+            [](M &ms, const SparseIdx &row_map, const SparseIdx &entries, const ArrC &values) {
+                return ms.expval(row_map.data(), (size_t)row_map.size(), entries.data(), values.data(),
+                                 (size_t)values.size());
+            },
+            "Expected value of a sparse Hamiltonian.")
         .def("var", [](M &ms, const std::shared_ptr<Obs> &o) { return ms.var(*o); })
         .def("var", [](M &ms, const std::string &name, const std::vector<size_t> &w) { return ms.var(name, w); })
+        .def(
+            "var",
+            [](M &ms, const SparseIdx &row_map, const SparseIdx &entries, const ArrC &values) {
+                return ms.var(row_map.data(), (size_t)row_map.size(), entries.data(), values.data(),
+                              (size_t)values.size());
+            },
+            "Variance of a sparse Hamiltonian.")
         .def("generate_samples",
              [](M &ms, size_t num_wires, size_t num_shots) {
                  auto r = ms.generate_samples(num_shots);
@@ -245,6 +258,17 @@ template <class T> void register_precision(py::module_ &m, py::module_ &obsm, py
             JacobianData<SV> jd(ops.getTotalNumParams(), w.sv.getLength(), nullptr, obs, ops, tp);
             adj.adjointJacobian(std::span<T>(jac), jd, false, &w.sv);
             return py::array_t<T>(py::cast(jac));
+        });
+    py::class_<VectorJacobianProduct<SV>>(algm, ("VectorJacobianProductC" + bits).c_str(), py::module_local())
+        .def(py::init<>())
+        .def("__call__", [](VectorJacobianProduct<SV> &vjp, W &w, const Ops &ops, const py::array_t<ComplexT> &dy,
+                            const std::vector<size_t> &tp) {
+            auto b = dy.request();
+            std::vector<ComplexT> jac(tp.size(), ComplexT{0, 0});
+            JacobianData<SV> jd(ops.getTotalNumParams(), w.sv.getLength(), nullptr, {}, ops, tp);
+            vjp(std::span<ComplexT>(jac), jd,
+                std::span<const ComplexT>(static_cast<const ComplexT *>(b.ptr), (size_t)b.size), false, &w.sv);
+            return py::array_t<ComplexT>(py::cast(jac));
         });
 }
 

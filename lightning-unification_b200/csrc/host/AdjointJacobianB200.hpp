@@ -125,4 +125,44 @@ template <class StateVectorT> class AdjointJacobian {
     }
 };
 
+// VectorJacobianProduct (LQ/algorithms/VectorJacobianProduct.hpp:60-156): jac[j] = i * scale *
+// <G mu | lambda> with mu the cotangent state dy, both swept backwards.
+template <class StateVectorT> class VectorJacobianProduct {
+    using PrecisionT = typename StateVectorT::PrecisionT;
+    using ComplexT = typename StateVectorT::ComplexT;
+
+  public:
+    void operator()(std::span<ComplexT> jac, const JacobianData<StateVectorT> &jd, std::span<const ComplexT> dy,
+                    bool apply_operations = false, const StateVectorT *device_psi = nullptr) {
+        if (dy.size() != jd.getSizeStateVec()) throw LightningException("Assertion failed: dy.size() == jd.getSizeStateVec()");
+        const auto &tp = jd.getTrainableParams();
+        if (!jd.hasTrainableParams()) return;
+        if (jac.size() != tp.size())
+            throw LightningException("The size of preallocated jacobian must be same as the number of trainable parameters.");
+        std::unique_ptr<StateVectorT> owned;
+        const StateVectorT *sv = device_psi;
+        if (!sv) {
+            owned = std::make_unique<StateVectorT>(jd.getPtrStateVec(), jd.getSizeStateVec());
+            sv = owned.get();
+        }
+        const auto &ops = jd.getOperations();
+        std::vector<b200sv_op> cops(ops.getSize());
+        std::vector<std::vector<uint32_t>> w(ops.getSize());
+        std::vector<std::vector<double>> p(ops.getSize());
+        for (size_t i = 0; i < ops.getSize(); ++i) {
+            w[i].assign(ops.getOpsWires()[i].begin(), ops.getOpsWires()[i].end());
+            p[i].assign(ops.getOpsParams()[i].begin(), ops.getOpsParams()[i].end());
+            const bool has_mat = !ops.getOpsMatrices()[i].empty();
+            cops[i] = b200sv_op{has_mat ? (uint32_t)B200SV_OP_MATRIX : op_id(ops.getOpsName()[i]), (uint32_t)w[i].size(),
+                                w[i].data(), ops.getOpsInverses()[i] ? 1 : 0, (uint32_t)p[i].size(), p[i].data(),
+                                has_mat ? ops.getOpsMatrices()[i].data() : nullptr};
+        }
+        std::vector<uint64_t> tpu(tp.begin(), tp.end());
+        std::vector<double> out(2 * tp.size());
+        check(b200sv_vjp_state(sv->handle(), cops.data(), (uint32_t)cops.size(), dy.data(), dy.size(), tpu.data(),
+                               (uint32_t)tpu.size(), apply_operations ? 1 : 0, out.data()));
+        for (size_t j = 0; j < tp.size(); ++j) jac[j] = ComplexT((PrecisionT)out[2 * j], (PrecisionT)out[2 * j + 1]);
+    }
+};
+
 }  // namespace Pennylane::LightningB200

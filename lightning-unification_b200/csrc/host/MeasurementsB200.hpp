@@ -28,6 +28,16 @@ template <class StateVectorT> class Measurements {
         return (PrecisionT)out;
     }
 
+    template <class index_type>
+    double run_sparse(const index_type *rows, index_type nrows, const index_type *cols, const ComplexT *vals,
+                      index_type nnz, bool variance) const {
+        std::vector<uint64_t> r(rows, rows + nrows), c(cols, cols + std::min<index_type>(nnz, nrows ? rows[nrows - 1] - rows[0] : 0));
+        double out = 0;
+        check((variance ? b200sv_var_sparse : b200sv_expval_sparse)(sv_.handle(), r.data(), (uint64_t)nrows, c.data(),
+                                                                     vals, (uint64_t)nnz, &out));
+        return out;
+    }
+
   public:
     explicit Measurements(const StateVectorT &sv) : sv_(sv) {}
 
@@ -67,6 +77,18 @@ template <class StateVectorT> class Measurements {
     }
     PrecisionT var(const std::vector<ComplexT> &matrix, const std::vector<size_t> &wires) const {
         return run_var({TermData<PrecisionT>{1.0, {FactorData<PrecisionT>{false, "Hermitian", wires, matrix}}}});
+    }
+    // :197-214 (CSR sparse Hamiltonian; values in the state's precision)
+    template <class index_type>
+    PrecisionT expval(const index_type *row_map_ptr, const index_type row_map_size, const index_type *entries_ptr,
+                      const ComplexT *values_ptr, const index_type numNNZ) const {
+        return (PrecisionT)run_sparse(row_map_ptr, row_map_size, entries_ptr, values_ptr, numNNZ, false);
+    }
+    // :451-472
+    template <class index_type>
+    PrecisionT var(const index_type *row_map_ptr, const index_type row_map_size, const index_type *entries_ptr,
+                   const ComplexT *values_ptr, const index_type numNNZ) const {
+        return (PrecisionT)run_sparse(row_map_ptr, row_map_size, entries_ptr, values_ptr, numNNZ, true);
     }
     // generate_samples (:482-558 signature and output layout; sampling rule of
     // LK/measurements/MeasuresFunctors.hpp:70-103 with device Philox draws).

@@ -45,6 +45,7 @@ struct DOp {
     uint8_t run;         // >= 2: first of `run` single-wire gates on bit `rbit` fused into one pass
     uint8_t rbit;
     uint8_t gcode;       // run members' generator: 1 X, 2 Y, 3 Z, 4 |1><1| (0: none / general)
+    uint8_t mkind;       // run members' matrix structure (MK_* below)
     uint16_t low[4];     // insertion masks of the gate bits (ascending)
     uint16_t glow[2];    // insertion masks of the generator bits
     uint32_t cmask;      // control bits (must be set)
@@ -81,6 +82,58 @@ struct DTerm {
 };
 
 constexpr int kMaxRun = 3;
+// structure of a single-wire matrix, used to spend fewer instructions per amplitude pair
+enum MKind : uint8_t { MK_GENERAL = 0, MK_DIAG = 1, MK_PHASE1 = 2, MK_REAL = 3, MK_SWAP = 4, MK_RX = 5 };
+
+// single complex product m * v (FMA-formed components)
+template <typename R> __device__ __forceinline__ C<R> cmul1(C<R> m, C<R> v) {
+    return mk<R>(fma(m.x, v.x, -(m.y * v.y)), fma(m.x, v.y, m.y * v.x));
+}
+// a*x + b*y for real coefficients, accurate to about one rounding: the product b*y is
+// split exactly with an FMA (TwoProduct) and its error added back after the second FMA.
+template <typename R> __device__ __forceinline__ R dot2r(R a, R x, R b, R y) {
+    const R w = b * y;
+    const R e = fma(b, y, -w);
+    return fma(a, x, w) + e;
+}
+
+// Apply a single-wire matrix m (given its structure) to the pair (v0, v1) in place.
+template <typename R> __device__ __forceinline__ void apply_pair(int kind, const C<R> (&m)[4], C<R> &v0, C<R> &v1) {
+    switch (kind) {
+    case MK_DIAG:
+        v0 = cmul1<R>(m[0], v0);
+        v1 = cmul1<R>(m[3], v1);
+        break;
+    case MK_PHASE1:
+        v1 = cmul1<R>(m[3], v1);
+        break;
+    case MK_SWAP: {
+        const C<R> t = v0;
+        v0 = v1;
+        v1 = t;
+        break;
+    }
+    case MK_REAL: {  // m real
+        const C<R> a = v0, b = v1;
+        v0 = mk<R>(dot2r<R>(m[0].x, a.x, m[1].x, b.x), dot2r<R>(m[0].x, a.y, m[1].x, b.y));
+        v1 = mk<R>(dot2r<R>(m[2].x, a.x, m[3].x, b.x), dot2r<R>(m[2].x, a.y, m[3].x, b.y));
+        break;
+    }
+    case MK_RX: {  // real diagonal, imaginary off-diagonal
+        const C<R> a = v0, b = v1;
+        v0 = mk<R>(dot2r<R>(m[0].x, a.x, -m[1].y, b.y), dot2r<R>(m[0].x, a.y, m[1].y, b.x));
+        v1 = mk<R>(dot2r<R>(-m[2].y, a.y, m[3].x, b.x), dot2r<R>(m[2].y, a.x, m[3].x, b.y));
+        break;
+    }
+    default: {
+        CAcc<R> p, q;
+        p.add(m[0], v0); p.add(m[1], v1);
+        q.add(m[2], v0); q.add(m[3], v1);
+        v0 = p.get();
+        v1 = q.get();
+    }
+    }
+}
 
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ uint32_t ins_local(uint32_t g, const uint16_t *low, int nb) {
@@ -318,14 +371,20 @@ __device__ __forceinline__ void add_grad(double *gradw, int32_t gslot, double p,
 }
 
 // Im(conj(b) . G a) over one amplitude pair for the run generators X, Y, Z, |1><1|.
-__device__ __forceinline__ double pair_gen_im(int code, double2 a0, double2 a1, double2 b0, double2 b1) {
+// complex128: in FP64.  complex64: the pair's value is formed in FP32 with FMAs
+// (two roundings at most) and returned as a double; the sums over pairs, warps,
+// tiles and the state are FP64.
+template <typename R>
+__device__ __forceinline__ double pair_gen_im(int code, C<R> a0, C<R> a1, C<R> b0, C<R> b1) {
     // w = G a;  Im(conj(b) w) = b.x w.y - b.y w.x
+    R r;
     switch (code) {
-    case 1: return b0.x * a1.y - b0.y * a1.x + b1.x * a0.y - b1.y * a0.x;        // w = (a1, a0)
-    case 2: return -(b0.x * a1.x + b0.y * a1.y) + (b1.x * a0.x + b1.y * a0.y);   // w = (-i a1, i a0)
-    case 3: return b0.x * a0.y - b0.y * a0.x - (b1.x * a1.y - b1.y * a1.x);      // w = (a0, -a1)
-    default: return b1.x * a1.y - b1.y * a1.x;                                    // w = (0, a1)
+    case 1: r = fma(b0.x, a1.y, -(b0.y * a1.x)) + fma(b1.x, a0.y, -(b1.y * a0.x)); break;   // w = (a1, a0)
+    case 2: r = fma(b1.x, a0.x, b1.y * a0.y) - fma(b0.x, a1.x, b0.y * a1.y); break;         // w = (-i a1, i a0)
+    case 3: r = fma(b0.x, a0.y, -(b0.y * a0.x)) - fma(b1.x, a1.y, -(b1.y * a1.x)); break;   // w = (a0, -a1)
+    default: r = fma(b1.x, a1.y, -(b1.y * a1.x)); break;                                   // w = (0, a1)
     }
+    return (double)r;
 }
 
 // A run of `len` single-wire gates on bit rb, applied per amplitude pair in registers.
@@ -374,14 +433,16 @@ __device__ void exec_run(C<R> *const (&s)[NS], int kt, int wl, bool wloc, const 
     // adjoint sweep: register copies in reverse order
     C<R> m[kMaxRun][4];
     double ip[kMaxRun];
-    int gc[kMaxRun];
+    int gc[kMaxRun], mk_[kMaxRun];
 #pragma unroll
     for (int kk = 0; kk < kMaxRun; ++kk) {
         ip[kk] = 0.0;
         gc[kk] = 0;
+        mk_[kk] = MK_GENERAL;
         if (kk < len) {
             const DOp &op = ops[len - 1 - kk];
             member_mat<R>(op, cs, consts, true, m[kk]);
+            mk_[kk] = op.mkind;
             if (op.gslot >= 0) gc[kk] = op.gcode;
         }
     }
@@ -391,13 +452,9 @@ __device__ void exec_run(C<R> *const (&s)[NS], int kt, int wl, bool wloc, const 
 #pragma unroll
         for (int kk = 0; kk < kMaxRun; ++kk) {
             if (kk < len) {
-                if (gc[kk]) ip[kk] += pair_gen_im(gc[kk], widen<R>(a0), widen<R>(a1), widen<R>(b0), widen<R>(b1));
-                CAcc<R> p, q, u, v;
-                p.add(m[kk][0], a0); p.add(m[kk][1], a1);
-                q.add(m[kk][2], a0); q.add(m[kk][3], a1);
-                u.add(m[kk][0], b0); u.add(m[kk][1], b1);
-                v.add(m[kk][2], b0); v.add(m[kk][3], b1);
-                a0 = p.get(); a1 = q.get(); b0 = u.get(); b1 = v.get();
+                if (gc[kk]) ip[kk] += pair_gen_im<R>(gc[kk], a0, a1, b0, b1);
+                apply_pair<R>(mk_[kk], m[kk], a0, a1);
+                apply_pair<R>(mk_[kk], m[kk], b0, b1);
             }
         }
         s[0][i0] = a0;
@@ -491,13 +548,40 @@ template <typename R> __device__ __forceinline__ void zero_tile(C<R> *s, uint32_
     for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) s[i] = mk<R>(0, 0);
 }
 
+// Tile element l lives at tbase | deposit(l over lbits).  Threads take l = tid + k*blockDim
+// (blockDim a power of two), so the deposit of the low bits is fixed per thread and
+// only the few high bits change with k.
+__device__ __forceinline__ uint64_t deposit_bits(uint32_t v, const uint8_t *bits, int from, int to) {
+    uint64_t r = 0;
+    for (int j = from; j < to; ++j)
+        if (v & (1u << (j - from))) r |= uint64_t(1) << bits[j];
+    return r;
+}
+template <typename R, bool LOAD>
+__device__ __forceinline__ void move_tile(C<R> *sm, C<R> *gm, const DSeg &sg, uint64_t tbase, uint32_t nt) {
+    const int bl = 31 - __clz((int)blockDim.x);
+    if (nt <= blockDim.x) {
+        if (threadIdx.x < nt) {
+            const uint64_t a = tbase | deposit_bits(threadIdx.x, sg.lbits, 0, sg.nl);
+            if (LOAD) sm[threadIdx.x] = gm[a];
+            else gm[a] = sm[threadIdx.x];
+        }
+        return;
+    }
+    const uint64_t lo = tbase | deposit_bits(threadIdx.x, sg.lbits, 0, bl);
+    for (uint32_t k = 0, l = threadIdx.x; l < nt; ++k, l += blockDim.x) {
+        const uint64_t a = lo | deposit_bits(k, sg.lbits, bl, sg.nl);
+        if (LOAD) sm[l] = gm[a];
+        else gm[a] = sm[l];
+    }
+}
 template <typename R>
 __device__ void load_tile(C<R> *dst, const C<R> *__restrict__ src, const DSeg &sg, uint64_t tbase, uint32_t nt) {
-    for (uint32_t l = threadIdx.x; l < nt; l += blockDim.x) dst[l] = src[tbase | insert_zeros64(l, sg.gbits, sg.ng)];
+    move_tile<R, true>(dst, const_cast<C<R> *>(src), sg, tbase, nt);
 }
 template <typename R>
 __device__ void store_tile(C<R> *__restrict__ dst, const C<R> *src, const DSeg &sg, uint64_t tbase, uint32_t nt) {
-    for (uint32_t l = threadIdx.x; l < nt; l += blockDim.x) dst[tbase | insert_zeros64(l, sg.gbits, sg.ng)] = src[l];
+    move_tile<R, false>(const_cast<C<R> *>(src), dst, sg, tbase, nt);
 }
 
 // Apply the gates of one segment to the tile(s): forward (NS = 1) or the adjoint
@@ -632,6 +716,25 @@ __global__ void __launch_bounds__(512) k_batch(KArgs A) {
                 __syncthreads();
             }
         }
+    }
+}
+
+// One fused segment over a single large state: every CTA takes tiles of the
+// segment's local bits, applies the segment's gates in shared memory and writes
+// the tile back — one HBM pass for the whole run of gates.
+template <typename R>
+__global__ void __launch_bounds__(512) k_segment(KArgs A, DSeg sg, void *state, uint64_t ntiles, int kt) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C<R> *tile = reinterpret_cast<C<R> *>(smem_raw);
+    C<R> *sv = static_cast<C<R> *>(state);
+    C<R> *tiles[1] = {tile};
+    const uint32_t tn = 1u << kt;
+    for (uint64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const uint64_t tbase = insert_zeros64(t, sg.lbits, sg.nl);
+        load_tile<R>(tile, sv, sg, tbase, tn);
+        exec_segment<R, 1, false>(A, tiles, kt, sg, true);
+        store_tile<R>(sv, tile, sg, tbase, tn);
+        __syncthreads();
     }
 }
 
@@ -1026,7 +1129,26 @@ int run_bit(const DOp &d) {
     return bit;
 }
 
-void mark_runs(DOp *ops, uint32_t n) {
+// Structure of a run member's matrix (the adjoint has the same structure).
+uint8_t member_kind(const DOp &d, const double2 *consts) {
+    if (d.form == F_SWAP) return MK_SWAP;
+    if (d.form == F_DIAG) return d.nt == 1 ? MK_DIAG : MK_PHASE1;
+    if (d.gate == B200SV_RY) return MK_REAL;
+    if (d.gate == B200SV_RX) return MK_RX;
+    if (d.gate == kConstGate) {  // classify a constant 2x2 by its entries
+        const double2 *c = consts + (size_t)d.cidx * 16;
+        auto zero = [](double2 z) { return z.x == 0.0 && z.y == 0.0; };
+        if (zero(c[1]) && zero(c[2])) return MK_DIAG;
+        bool real = true, rx = true;
+        for (int i = 0; i < 4; ++i) real = real && c[i].y == 0.0;
+        rx = c[0].y == 0.0 && c[3].y == 0.0 && c[1].x == 0.0 && c[2].x == 0.0;
+        if (real) return MK_REAL;
+        if (rx) return MK_RX;
+    }
+    return MK_GENERAL;
+}
+
+void mark_runs(DOp *ops, uint32_t n, const double2 *consts) {
     uint32_t i = 0;
     while (i < n) {
         const int b = run_bit(ops[i]);
@@ -1035,11 +1157,20 @@ void mark_runs(DOp *ops, uint32_t n) {
             while (j < n && j - i < (uint32_t)kMaxRun && run_bit(ops[j]) == b) ++j;
         if (j - i >= 2) {
             ops[i].run = (uint8_t)(j - i);
-            for (uint32_t q = i; q < j; ++q) ops[q].rbit = (uint8_t)b;
+            for (uint32_t q = i; q < j; ++q) {
+                ops[q].rbit = (uint8_t)b;
+                ops[q].mkind = member_kind(ops[q], consts);
+            }
             for (uint32_t q = i + 1; q < j; ++q) ops[q].run = 0;
         }
         i = j;
     }
+}
+
+// Lowest state bits every tile keeps: 2^r contiguous amplitudes = 128 bytes.
+uint64_t low_reserve_mask(int dtype, uint32_t kt) {
+    const uint32_t r = std::min<uint32_t>(dtype == B200SV_C64 ? 4 : 3, kt > 4 ? kt - 4 : 0);
+    return (uint64_t(1) << r) - 1;
 }
 
 Planned plan(const Batch &B, const Config &cfg, bool vjp) {
@@ -1067,13 +1198,16 @@ Planned plan(const Batch &B, const Config &cfg, bool vjp) {
         // segmentation
         const auto &ops = B.hops[c];
         size_t i = 0;
+        // tiles of a multi-tile circuit always hold the lowest state bits, so every
+        // tile is made of contiguous runs of at least 128 bytes
+        const uint64_t low = dc.resident ? 0 : low_reserve_mask(B.dtype, dc.kt);
         while (i < ops.size() || (i == 0 && ops.empty())) {
             uint64_t used = 0;
             size_t j = i;
             while (j < ops.size()) {
                 uint64_t b = 0;
                 for (auto x : ops[j].bits) b |= uint64_t(1) << x;
-                if (popcount64(used | b) > (int)dc.kt) break;
+                if (popcount64(used | b) > (int)dc.kt || (popcount64(used | b | low) > (int)dc.kt && j > i)) break;
                 used |= b;
                 ++j;
             }
@@ -1108,7 +1242,7 @@ Planned plan(const Batch &B, const Config &cfg, bool vjp) {
                 }
                 P.ops.push_back(d);
             }
-            mark_runs(P.ops.data() + s.op_begin, s.nops);
+            mark_runs(P.ops.data() + s.op_begin, s.nops, P.consts.data());
             P.segs.push_back(s);
             if (ops.empty()) break;
             i = j;
@@ -1316,6 +1450,149 @@ template <class F> void run_maybe_graph(Batch &B, cudaGraphExec_t &exec, F &&enq
     B200SV_CUDA(cudaGraphLaunch(exec, st));
 }
 
+// ---- fused application of one op list to one state ---------------------------
+int fused_tile_bits(int dtype, uint32_t n) {
+    const int kt = dtype == B200SV_C64 ? 13 : 12;
+    return (int)std::min<uint32_t>(kt, n > 8 ? n - 8 : 1);
+}
+
+void apply_ops_fused(const StateView &v, const b200sv_op *ops, uint32_t nops) {
+    const uint32_t n = v.nq;
+    const int kt = fused_tile_bits(v.dtype, n);
+    const cudaStream_t st = v.stream;
+    const size_t amp = v.dtype == B200SV_C64 ? 8 : 16;
+    // which ops the tile forms cover
+    std::vector<HostOp> hops(nops);
+    std::vector<char> tiled(nops, 0);
+    for (uint32_t i = 0; i < nops; ++i) {
+        if (ops[i].gate == B200SV_OP_SKIP) continue;
+        try {
+            hops[i] = make_hostop(ops[i], -1, n, v.dtype);
+            tiled[i] = (int)hops[i].bits.size() <= kt ? 1 : 0;
+        } catch (const Unsupported &) {
+            tiled[i] = 0;
+        }
+    }
+    Planned P;
+    push_const(P, {});
+    struct Piece {
+        bool seg;
+        DSeg s;
+        uint32_t op;  // untiled op index
+    };
+    std::vector<Piece> pieces;
+    uint32_t i = 0;
+    while (i < nops) {
+        if (ops[i].gate == B200SV_OP_SKIP) { ++i; continue; }
+        if (!tiled[i]) {
+            pieces.push_back(Piece{false, DSeg{}, i});
+            ++i;
+            continue;
+        }
+        uint64_t used = 0;
+        const uint64_t low = low_reserve_mask(v.dtype, (uint32_t)kt);
+        uint32_t j = i;
+        while (j < nops && (tiled[j] || ops[j].gate == B200SV_OP_SKIP)) {
+            if (ops[j].gate == B200SV_OP_SKIP) { ++j; continue; }
+            uint64_t b = 0;
+            for (auto x : hops[j].bits) b |= uint64_t(1) << x;
+            if (popcount64(used | b) > kt || (popcount64(used | b | low) > kt && j > i)) break;
+            used |= b;
+            ++j;
+        }
+        std::vector<uint32_t> L;
+        for (uint32_t x = 0; x < n; ++x)
+            if (used & (uint64_t(1) << x)) L.push_back(x);
+        for (uint32_t x = 0; x < n && (int)L.size() < kt; ++x)
+            if (!(used & (uint64_t(1) << x))) L.push_back(x);
+        std::sort(L.begin(), L.end());
+        DSeg sg{};
+        sg.nl = (uint8_t)L.size();
+        std::vector<int> loc(n, -1);
+        for (size_t q = 0; q < L.size(); ++q) {
+            sg.lbits[q] = (uint8_t)L[q];
+            loc[L[q]] = (int)q;
+        }
+        uint8_t ng = 0;
+        for (uint32_t x = 0; x < n; ++x)
+            if (loc[x] < 0) sg.gbits[ng++] = (uint8_t)x;
+        sg.ng = ng;
+        sg.op_begin = (uint32_t)P.ops.size();
+        for (uint32_t q = i; q < j; ++q)
+            if (ops[q].gate != B200SV_OP_SKIP) P.ops.push_back(lower(P, hops[q], loc));
+        sg.nops = (uint32_t)(P.ops.size() - sg.op_begin);
+        mark_runs(P.ops.data() + sg.op_begin, sg.nops, P.consts.data());
+        pieces.push_back(Piece{true, sg, 0});
+        i = j;
+    }
+    DOp *d_ops = nullptr;
+    double2 *d_consts = nullptr;
+    void *d_mat = nullptr;
+    B200SV_CUDA(cudaMallocAsync((void **)&d_ops, std::max<size_t>(1, P.ops.size()) * sizeof(DOp), st));
+    B200SV_CUDA(cudaMallocAsync((void **)&d_consts, std::max<size_t>(1, P.consts.size()) * sizeof(double2), st));
+    struct Free {
+        DOp *&o;
+        double2 *&c;
+        void *&m;
+        cudaStream_t s;
+        ~Free() {
+            cudaFreeAsync(o, s);
+            cudaFreeAsync(c, s);
+            if (m) cudaFreeAsync(m, s);
+        }
+    } guard{d_ops, d_consts, d_mat, st};
+    if (!P.ops.empty())
+        B200SV_CUDA(cudaMemcpyAsync(d_ops, P.ops.data(), P.ops.size() * sizeof(DOp), cudaMemcpyHostToDevice, st));
+    B200SV_CUDA(cudaMemcpyAsync(d_consts, P.consts.data(), P.consts.size() * sizeof(double2), cudaMemcpyHostToDevice, st));
+    KArgs A{};
+    A.ops = d_ops;
+    A.consts = d_consts;
+    const int threads = 512;
+    const size_t smem = amp << kt;
+    int per_sm = 1;
+    if (v.dtype == B200SV_C64) {
+        B200SV_CUDA(cudaFuncSetAttribute(k_segment<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        B200SV_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_segment<float>, threads, smem));
+    } else {
+        B200SV_CUDA(cudaFuncSetAttribute(k_segment<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        B200SV_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_segment<double>, threads, smem));
+    }
+    const uint64_t ntiles = uint64_t(1) << (n - kt);
+    const unsigned grid = (unsigned)std::min<uint64_t>(ntiles, (uint64_t)sm_count() * std::max(1, per_sm));
+    for (const Piece &pc : pieces) {
+        if (pc.seg) {
+            if (v.dtype == B200SV_C64) k_segment<float><<<grid, threads, smem, st>>>(A, pc.s, v.state, ntiles, kt);
+            else k_segment<double><<<grid, threads, smem, st>>>(A, pc.s, v.state, ntiles, kt);
+            B200SV_CUDA(cudaGetLastError());
+            continue;
+        }
+        // a gate outside the tile forms: its own pass with the per-gate kernels
+        const b200sv_op &o = ops[pc.op];
+        GateDesc g;
+        if (o.gate == B200SV_OP_MATRIX) {
+            const size_t d = size_t(1) << o.nwires;
+            std::vector<cd> m(d * d);
+            for (size_t q = 0; q < d * d; ++q) {
+                if (v.dtype == B200SV_C64) {
+                    const float *f = static_cast<const float *>(o.matrix);
+                    m[q] = cd(f[2 * q], f[2 * q + 1]);
+                } else {
+                    const double *f = static_cast<const double *>(o.matrix);
+                    m[q] = cd(f[2 * q], f[2 * q + 1]);
+                }
+            }
+            g = compile_matrix(m.data(), o.wires, o.nwires, o.inverse != 0, n);
+        } else {
+            g = compile_gate(o.gate, o.wires, o.nwires, o.inverse != 0, o.params, o.nparams, n);
+        }
+        if (g.kind == Kind::Dense && g.k >= 4 && !d_mat)
+            B200SV_CUDA(cudaMallocAsync(&d_mat, amp << (2 * 11), st));
+        void *states[1] = {v.state};
+        if (v.dtype == B200SV_C64) launch_gate<float>(states, 1, n, g, d_mat, st);
+        else launch_gate<double>(states, 1, n, g, d_mat, st);
+    }
+}
+
 }  // namespace batch
 }  // namespace b200sv
 
@@ -1395,6 +1672,24 @@ int b200sv_batch_create(int dtype, const b200sv_batch_circuit *circuits, uint32_
         auto *h = new b200sv_batch;
         h->b = std::move(B);
         *out = h;
+    });
+}
+
+int b200sv_apply_ops_fused(b200sv_handle h, const b200sv_op *ops, uint32_t nops) {
+    return run_guarded([&] {
+        const StateView v = state_view(h);
+        if (nops && !ops) throw ArgError("operations pointer is NULL");
+        int cur = -1;
+        cudaGetDevice(&cur);
+        if (cur != v.device) B200SV_CUDA(cudaSetDevice(v.device));
+        if (v.nq < (uint32_t)fused_tile_bits(v.dtype, v.nq) + 8) {
+            // too narrow for enough tiles to fill the GPU: the per-gate path
+            const int rc = b200sv_apply_ops(h, ops, nops);
+            if (rc != B200SV_OK) throw ArgError(b200sv_last_error());
+        } else {
+            apply_ops_fused(v, ops, nops);
+        }
+        if (cur != v.device && cur >= 0) cudaSetDevice(cur);
     });
 }
 

@@ -374,6 +374,11 @@ void check_handle(b200sv_state *h) { need(h != nullptr, "NULL state handle"); }
 
 int b200sv::run_guarded(const std::function<void()> &f) { return guard(f); }
 
+b200sv::StateView b200sv::state_view(b200sv_handle h) {
+    need(h != nullptr, "NULL state handle");
+    return StateView{h->d_state, h->nq, h->dtype, h->stream(), h->device};
+}
+
 // =============================================================================
 extern "C" {
 
@@ -694,6 +699,74 @@ int b200sv_norm2(b200sv_handle h, double *out) {
     });
 }
 
+// ---- sparse Hamiltonian: LQ/measurements/MeasurementsLQubit.hpp:197-214, :451-472 ----
+// out[0] = Re<psi|H psi>, out[1] = <H psi|H psi>.  The CSR arrays are checked on the host
+// (the reference reads them unchecked) so no launch reads outside them or the state.
+static void sparse_impl(b200sv_state *h, const uint64_t *row_map, uint64_t row_map_size, const uint64_t *entries,
+                        const void *values, uint64_t nnz, double out[2]) {
+    const uint64_t N = uint64_t(1) << h->nq;
+    need(row_map != nullptr || row_map_size == 0, "NULL row_map");
+    need(row_map_size >= 1 && row_map_size - 1 == N, "Statevector and Hamiltonian have incompatible sizes.");
+    const uint64_t base = row_map[0];
+    for (uint64_t i = 0; i < N; ++i) need(row_map[i] <= row_map[i + 1], "row_map must be non-decreasing");
+    const uint64_t used = row_map[N] - base;
+    need(used <= nnz, "row_map addresses more non-zeros than the value array holds");
+    need(used == 0 || (entries != nullptr && values != nullptr), "NULL entries or values");
+    for (uint64_t k = 0; k < used; ++k) need(entries[k] < N, "sparse column index out of range");
+    const cudaStream_t st = h->stream();
+    const size_t S = h->dtype == B200SV_C64 ? 8 : 16;
+    uint64_t *d_rows = nullptr, *d_cols = nullptr;
+    void *d_vals = nullptr;
+    B200SV_CUDA(cudaMallocAsync((void **)&d_rows, (N + 1) * sizeof(uint64_t), st));
+    B200SV_CUDA(cudaMallocAsync((void **)&d_cols, std::max<uint64_t>(1, used) * sizeof(uint64_t), st));
+    B200SV_CUDA(cudaMallocAsync(&d_vals, std::max<uint64_t>(1, used) * S, st));
+    struct Free {
+        void *a, *b, *c;
+        cudaStream_t s;
+        ~Free() {
+            cudaFreeAsync(a, s);
+            cudaFreeAsync(b, s);
+            cudaFreeAsync(c, s);
+        }
+    } fr{d_rows, d_cols, d_vals, st};
+    B200SV_CUDA(cudaMemcpyAsync(d_rows, row_map, (N + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice, st));
+    if (used) {
+        B200SV_CUDA(cudaMemcpyAsync(d_cols, entries, used * sizeof(uint64_t), cudaMemcpyHostToDevice, st));
+        B200SV_CUDA(cudaMemcpyAsync(d_vals, values, used * S, cudaMemcpyHostToDevice, st));
+    }
+    if (h->dtype == B200SV_C64)
+        reduce_sparse<float>(h->d_state, h->nq, d_rows, d_cols, d_vals, used, h->d_partials, h->d_small, st);
+    else
+        reduce_sparse<double>(h->d_state, h->nq, d_rows, d_cols, d_vals, used, h->d_partials, h->d_small, st);
+    read_small(h, 1);
+    out[0] = h->h_small[0];
+    out[1] = h->h_small[1];
+}
+
+int b200sv_expval_sparse(b200sv_handle h, const uint64_t *row_map, uint64_t row_map_size, const uint64_t *entries,
+                         const void *values, uint64_t nnz, double *out) {
+    return guard([&] {
+        check_handle(h);
+        need(out != nullptr, "NULL output");
+        DeviceGuard dg(h->device);
+        double r[2];
+        sparse_impl(h, row_map, row_map_size, entries, values, nnz, r);
+        *out = r[0];
+    });
+}
+
+int b200sv_var_sparse(b200sv_handle h, const uint64_t *row_map, uint64_t row_map_size, const uint64_t *entries,
+                      const void *values, uint64_t nnz, double *out) {
+    return guard([&] {
+        check_handle(h);
+        need(out != nullptr, "NULL output");
+        DeviceGuard dg(h->device);
+        double r[2];
+        sparse_impl(h, row_map, row_map_size, entries, values, nnz, r);
+        *out = r[1] - r[0] * r[0];
+    });
+}
+
 static void sample_impl(b200sv_state *h, uint64_t nshots, const double *uniforms, uint64_t seed, uint64_t *idx_host) {
     const cudaStream_t st = h->stream();
     const uint64_t N = uint64_t(1) << h->nq;
@@ -842,6 +915,87 @@ int b200sv_adjoint_jacobian(b200sv_handle psi, const b200sv_op *ops, uint32_t no
         // [tp][obs] -> [obs][tp]  (AdjointJacobianLQubit.hpp:331-334)
         for (uint32_t p = 0; p < ntp; ++p)
             for (uint32_t o = 0; o < nobs; ++o) jac[(size_t)o * ntp + p] = jt[(size_t)p * nobs + o];
+    });
+}
+
+// ---- state-return VJP: LQ/algorithms/VectorJacobianProduct.hpp:60-156 --------
+int b200sv_vjp_state(b200sv_handle psi, const b200sv_op *ops, uint32_t nops, const void *dy, uint64_t dy_length,
+                     const uint64_t *trainable, uint32_t ntp, int apply_operations, double *out) {
+    return guard([&] {
+        check_handle(psi);
+        need(dy != nullptr, "NULL cotangent state");
+        need(dy_length == (uint64_t(1) << psi->nq), "dy must have 2^num_qubits entries");
+        need(ntp == 0 || (trainable && out), "NULL trainable list or output");
+        if (ntp == 0) return;
+        for (uint32_t i = 1; i < ntp; ++i) need(trainable[i - 1] < trainable[i], "trainable parameters must be sorted");
+        DeviceGuard dg(psi->device);
+        b200sv_state *h = psi;
+        const cudaStream_t st = h->stream();
+        auto rec = read_ops(ops, nops, h->dtype);
+        size_t num_param_ops = 0;
+        for (auto &o : rec)
+            if (!o.params.empty()) ++num_param_ops;
+        void *lambda = nullptr, *mu = nullptr;
+        double *d_z = nullptr;
+        B200SV_CUDA(cudaMallocAsync(&lambda, h->state_bytes(), st));
+        B200SV_CUDA(cudaMallocAsync(&mu, h->state_bytes(), st));
+        B200SV_CUDA(cudaMallocAsync((void **)&d_z, sizeof(double) * 2 * ntp, st));
+        struct Cleanup {
+            void *a, *b;
+            double *z;
+            cudaStream_t s;
+            ~Cleanup() {
+                cudaFreeAsync(a, s);
+                cudaFreeAsync(b, s);
+                cudaFreeAsync(z, s);
+                cudaStreamSynchronize(s);
+            }
+        } cleanup{lambda, mu, d_z, st};
+        B200SV_CUDA(cudaMemsetAsync(d_z, 0, sizeof(double) * 2 * ntp, st));
+        B200SV_CUDA(cudaMemcpyAsync(lambda, h->d_state, h->state_bytes(), cudaMemcpyDeviceToDevice, st));
+        B200SV_CUDA(cudaMemcpyAsync(mu, dy, h->state_bytes(), cudaMemcpyHostToDevice, st));
+        if (apply_operations) {
+            for (auto &o : rec) {
+                void *s1[1] = {lambda};
+                apply_desc(h, s1, 1, compile_op(o, o.inverse, h->nq));
+            }
+        }
+        std::vector<double> scale(ntp, 0.0);
+        int64_t tp_pos = (int64_t)ntp - 1;
+        int64_t current = (int64_t)num_param_ops - 1;
+        for (int64_t op_idx = (int64_t)rec.size() - 1; op_idx >= 0; --op_idx) {
+            const OpRec &op = rec[op_idx];
+            if (op.params.size() > 1)
+                throw ArgError("The operation is not supported using the adjoint differentiation method");
+            if (op.gate == B200SV_OP_SKIP) continue;
+            if (tp_pos < 0) break;
+            if (!op.params.empty()) {
+                if ((uint64_t)current == trainable[tp_pos]) {
+                    const int gen = generator_of_gate(op.gate);
+                    if (gen < 0)
+                        throw ArgError("The operation is not supported using the adjoint differentiation method");
+                    double sc = 0.0;
+                    GateDesc G = compile_generator((uint32_t)gen, op.wires.data(), (uint32_t)op.wires.size(), h->nq, &sc);
+                    scale[tp_pos] = sc * (op.inverse ? -1.0 : 1.0);
+                    if (h->dtype == B200SV_C64)
+                        reduce_generator_inner_complex<float>(mu, lambda, h->nq, G, h->d_partials, d_z + 2 * tp_pos, st);
+                    else
+                        reduce_generator_inner_complex<double>(mu, lambda, h->nq, G, h->d_partials, d_z + 2 * tp_pos, st);
+                    --tp_pos;
+                }
+                --current;
+            }
+            GateDesc adj = compile_op(op, !op.inverse, h->nq);
+            void *two[2] = {lambda, mu};
+            apply_desc(h, two, 2, adj);
+        }
+        std::vector<double> z(2 * ntp);
+        B200SV_CUDA(cudaMemcpyAsync(z.data(), d_z, z.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+        B200SV_CUDA(cudaStreamSynchronize(st));
+        for (uint32_t j = 0; j < ntp; ++j) {  // i * scale * z
+            out[2 * j] = -scale[j] * z[2 * j + 1];
+            out[2 * j + 1] = scale[j] * z[2 * j];
+        }
     });
 }
 

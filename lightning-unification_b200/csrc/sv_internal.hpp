@@ -9,9 +9,20 @@
 #include <string>
 #include <vector>
 
+#include "../../include/b200sv.h"
 #include "gate_compiler.hpp"
 
 namespace b200sv {
+
+// What the fused and batched paths need to see of a state handle (sv_capi.cu).
+struct StateView {
+    void *state;
+    uint32_t nq;
+    int dtype;
+    cudaStream_t stream;
+    int device;
+};
+StateView state_view(b200sv_handle h);
 
 struct CudaError : std::runtime_error {
     using std::runtime_error::runtime_error;
@@ -71,6 +82,16 @@ template <typename R>
 void reduce_generator_inner(void *const *bras, int nbra, const void *ket, uint32_t nq,
                             const GateDesc &g, double alpha, double *partials, double *out_dev,
                             int out_stride, cudaStream_t st);
+// out2_dev[0..1] = (Re, Im) <bra| G |ket>.
+template <typename R>
+void reduce_generator_inner_complex(const void *bra, const void *ket, uint32_t nq, const GateDesc &g,
+                                    double *partials, double *out2_dev, cudaStream_t st);
+// out_dev[0] = Re<psi|H psi>, out_dev[1] = |H psi|^2 for H in CSR form (device arrays,
+// row i owning [row_map[i] - row_map[0], row_map[i+1] - row_map[0])); sv_sparse.cu.
+template <typename R>
+void reduce_sparse(const void *psi, uint32_t nq, const uint64_t *row_map_dev, const uint64_t *cols_dev,
+                   const void *vals_dev, uint64_t nnz, double *partials, double *out_dev, cudaStream_t st);
+int sparse_lanes(uint64_t nrows, uint64_t nnz);
 // Marginal probabilities over `bits` (bits[0] = MSB of the output index).
 template <typename R>
 void reduce_probs(const void *psi, uint32_t nq, const std::vector<uint32_t> &bits, double *partials,

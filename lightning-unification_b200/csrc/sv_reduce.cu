@@ -184,6 +184,31 @@ __device__ __forceinline__ int gen_apply(const GenP<R> &p, uint64_t g, const C<R
     return D;
 }
 
+// Both components of <bra|G|ket> for one bra: partials[0..nb) = Re, [nb..2nb) = Im.
+template <typename R>
+__global__ void __launch_bounds__(kRT) k_gen_inner_c(const C<R> *__restrict__ bra, const C<R> *__restrict__ ket,
+                                                     GenP<R> p, double *partials) {
+    __shared__ double sm[2 * 32];
+    double acc[2] = {0.0, 0.0};
+    for (uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < p.ngroups;
+         g += (uint64_t)gridDim.x * blockDim.x) {
+        uint64_t base;
+        double2 w[16];
+        const int D = gen_apply<R>(p, g, ket, base, w);
+        for (int r = 0; r < D; ++r) {
+            const uint64_t idx = (p.kind == (int)Kind::Parity) ? base : base + p.off[r];
+            const double2 b = widen<R>(bra[idx]);
+            acc[0] += b.x * w[r].x + b.y * w[r].y;  // Re conj(b) w
+            acc[1] += b.x * w[r].y - b.y * w[r].x;  // Im conj(b) w
+        }
+    }
+    block_reduce<2>(acc, sm);
+    if (threadIdx.x == 0) {
+        partials[blockIdx.x] = acc[0];
+        partials[gridDim.x + blockIdx.x] = acc[1];
+    }
+}
+
 template <typename R, int NB>
 __global__ void __launch_bounds__(kRT) k_gen_inner(Bras<R> bras, int nbra, const C<R> *__restrict__ ket,
                                                    GenP<R> p, double *partials) {
@@ -432,11 +457,19 @@ void reduce_dense_expval(const void *psi, uint32_t nq, const GateDesc &g, const 
     finalize(partials, nb, 1, out, 1, 1.0, st);
 }
 
+template <typename R> GenP<R> make_genp(uint32_t nq, const GateDesc &g);
+
 template <typename R>
-void reduce_generator_inner(void *const *bras, int nbra, const void *ket, uint32_t nq, const GateDesc &g,
-                            double alpha, double *partials, double *out, int out_stride, cudaStream_t st) {
-    if (nbra <= 0) return;
-    if (nbra > 16) throw ArgError("at most 16 bras per generator product");
+void reduce_generator_inner_complex(const void *bra, const void *ket, uint32_t nq, const GateDesc &g,
+                                    double *partials, double *out2, cudaStream_t st) {
+    GenP<R> p = make_genp<R>(nq, g);
+    const int nb = red_blocks(p.ngroups);
+    k_gen_inner_c<R><<<nb, kRT, 0, st>>>(static_cast<const C<R> *>(bra), static_cast<const C<R> *>(ket), p, partials);
+    B200SV_CUDA(cudaGetLastError());
+    finalize(partials, nb, 2, out2, 1, 1.0, st);
+}
+
+template <typename R> GenP<R> make_genp(uint32_t nq, const GateDesc &g) {
     GenP<R> p{};
     p.kind = (int)g.kind;
     p.k = g.k;
@@ -463,6 +496,15 @@ void reduce_generator_inner(void *const *bras, int nbra, const void *ket, uint32
         p.pa = (int)g.pa;
         p.pb = (int)g.pb;
     }
+    return p;
+}
+
+template <typename R>
+void reduce_generator_inner(void *const *bras, int nbra, const void *ket, uint32_t nq, const GateDesc &g,
+                            double alpha, double *partials, double *out, int out_stride, cudaStream_t st) {
+    if (nbra <= 0) return;
+    if (nbra > 16) throw ArgError("at most 16 bras per generator product");
+    GenP<R> p = make_genp<R>(nq, g);
     Bras<R> B{};
     for (int o = 0; o < nbra; ++o) B.p[o] = static_cast<const C<R> *>(bras[o]);
     const int nb = red_blocks(p.ngroups);
@@ -537,6 +579,8 @@ template <typename R> void axpy(void *acc, const void *x, uint32_t nq, double c,
                                          double *, cudaStream_t);                                               \
     template void reduce_generator_inner<R>(void *const *, int, const void *, uint32_t, const GateDesc &,       \
                                             double, double *, double *, int, cudaStream_t);                     \
+    template void reduce_generator_inner_complex<R>(const void *, const void *, uint32_t, const GateDesc &,     \
+                                                    double *, double *, cudaStream_t);                          \
     template void reduce_probs<R>(const void *, uint32_t, const std::vector<uint32_t> &, double *, size_t,      \
                                   double *, cudaStream_t);                                                      \
     template void set_basis<R>(void *, uint32_t, uint64_t, cudaStream_t);                                       \

@@ -68,6 +68,13 @@ class Observable(C.Structure):
     _fields_ = [("nterms", C.c_uint32), ("terms", C.POINTER(Term))]
 
 
+# numpy view of b200sv_op (same layout as the ctypes structure above)
+_OP_DTYPE = np.dtype({"names": ["gate", "nwires", "wires", "inverse", "nparams", "params", "matrix"],
+                      "formats": ["<u4", "<u4", "<u8", "<i4", "<u4", "<u8", "<u8"],
+                      "offsets": [0, 4, 8, 16, 20, 24, 32], "itemsize": 40})
+assert C.sizeof(Op) == 40 and Op.wires.offset == 8 and Op.params.offset == 24 and Op.matrix.offset == 32
+
+
 class BatchCircuit(C.Structure):
     _fields_ = [("num_qubits", C.c_uint32), ("nops", C.c_uint32), ("ops", C.POINTER(Op)),
                 ("param_index", C.POINTER(C.c_int64)), ("nobs", C.c_uint32),
@@ -95,6 +102,7 @@ _SIGS = {
                            C.POINTER(C.c_double), C.c_uint32], C.c_int),
     "b200sv_apply_matrix": ([C.c_void_p, C.c_void_p, C.POINTER(C.c_uint32), C.c_uint32, C.c_int], C.c_int),
     "b200sv_apply_ops": ([C.c_void_p, C.POINTER(Op), C.c_uint32], C.c_int),
+    "b200sv_apply_ops_fused": ([C.c_void_p, C.POINTER(Op), C.c_uint32], C.c_int),
     "b200sv_apply_generator": ([C.c_void_p, C.c_uint32, C.POINTER(C.c_uint32), C.c_uint32, C.c_int,
                                 C.POINTER(C.c_double)], C.c_int),
     "b200sv_probs": ([C.c_void_p, C.POINTER(C.c_uint32), C.c_uint32, C.POINTER(C.c_double)], C.c_int),
@@ -106,6 +114,10 @@ _SIGS = {
                              C.POINTER(C.c_double)], C.c_int),
     "b200sv_inner_product": ([C.c_void_p, C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double)], C.c_int),
     "b200sv_norm2": ([C.c_void_p, C.POINTER(C.c_double)], C.c_int),
+    "b200sv_expval_sparse": ([C.c_void_p, C.POINTER(C.c_uint64), C.c_uint64, C.POINTER(C.c_uint64), C.c_void_p,
+                              C.c_uint64, C.POINTER(C.c_double)], C.c_int),
+    "b200sv_var_sparse": ([C.c_void_p, C.POINTER(C.c_uint64), C.c_uint64, C.POINTER(C.c_uint64), C.c_void_p,
+                           C.c_uint64, C.POINTER(C.c_double)], C.c_int),
     "b200sv_sample": ([C.c_void_p, C.c_uint64, C.POINTER(C.c_double), C.c_uint64,
                        C.POINTER(C.c_uint64)], C.c_int),
     "b200sv_sample_bits": ([C.c_void_p, C.c_uint64, C.POINTER(C.c_double), C.c_uint64,
@@ -114,6 +126,8 @@ _SIGS = {
                                      C.POINTER(C.c_uint32), C.c_char_p, C.c_void_p, C.c_void_p], C.c_int),
     "b200sv_adjoint_jacobian": ([C.c_void_p, C.POINTER(Op), C.c_uint32, C.POINTER(Observable), C.c_uint32,
                                  C.POINTER(C.c_uint64), C.c_uint32, C.c_int, C.POINTER(C.c_double)], C.c_int),
+    "b200sv_vjp_state": ([C.c_void_p, C.POINTER(Op), C.c_uint32, C.c_void_p, C.c_uint64, C.POINTER(C.c_uint64),
+                          C.c_uint32, C.c_int, C.POINTER(C.c_double)], C.c_int),
     "b200sv_batch_create": ([C.c_int, C.POINTER(BatchCircuit), C.c_uint32, C.c_uint64,
                              C.POINTER(C.c_void_p)], C.c_int),
     "b200sv_batch_destroy": ([C.c_void_p], C.c_int),
@@ -174,34 +188,55 @@ def _f64(seq):
 class OpList:
     """Packs a list of (name_or_id, wires, inverse, params[, matrix]) into b200sv_op records.
 
-    Keeps every backing array alive for the lifetime of the object."""
+    All wires and parameters go into two contiguous arrays, and each record points into
+    them, so packing costs a few hundred nanoseconds per op.  The object keeps every
+    backing array alive for its lifetime."""
 
     def __init__(self, ops, complex_dtype=np.complex128):
+        n = len(ops)
+        self.n = n
         self._keep = []
-        self.arr = (Op * max(1, len(ops)))()
-        self.n = len(ops)
+        gids = np.empty(n, dtype=np.uint32)
+        nw = np.empty(n, dtype=np.uint32)
+        npar = np.empty(n, dtype=np.uint32)
+        inv = np.empty(n, dtype=np.int32)
+        wires, params = [], []
+        mats = {}
         for i, op in enumerate(ops):
-            name, wires, inverse, params = op[:4]
-            matrix = op[4] if len(op) > 4 else None
-            gid = name if isinstance(name, int) else (
-                OP_MATRIX if name in ("QubitUnitary", "Matrix") else
-                OP_SKIP if name in ("QubitStateVector", "BasisState", "StatePrep") else GATE_IDS[name])
-            w, wp = _u32(wires)
-            p, pp = _f64(params if params is not None else [])
-            self._keep += [w, p]
-            rec = self.arr[i]
-            rec.gate = gid
-            rec.nwires = len(w)
-            rec.wires = wp
-            rec.inverse = 1 if inverse else 0
-            rec.nparams = len(p)
-            rec.params = pp
-            if matrix is not None:
-                m = np.ascontiguousarray(np.asarray(matrix, dtype=complex_dtype))
-                self._keep.append(m)
-                rec.matrix = m.ctypes.data
+            name, w, inverse, p = op[:4]
+            if isinstance(name, (int, np.integer)):
+                gid = int(name)
+            elif name in ("QubitUnitary", "Matrix"):
+                gid = OP_MATRIX
+            elif name in ("QubitStateVector", "BasisState", "StatePrep"):
+                gid = OP_SKIP
             else:
-                rec.matrix = None
+                gid = GATE_IDS[name]
+            gids[i] = gid
+            nw[i] = len(w)
+            wires.extend(w)
+            p = () if p is None else p
+            npar[i] = len(p)
+            params.extend(p)
+            inv[i] = 1 if inverse else 0
+            if len(op) > 4 and op[4] is not None:
+                mats[i] = np.ascontiguousarray(np.asarray(op[4], dtype=complex_dtype))
+        W = np.ascontiguousarray(np.asarray(wires if wires else [0], dtype=np.uint32))
+        P = np.ascontiguousarray(np.asarray(params if params else [0.0], dtype=np.float64))
+        woff = np.concatenate([[0], np.cumsum(nw, dtype=np.uint64)[:-1]]).astype(np.uint64)
+        poff = np.concatenate([[0], np.cumsum(npar, dtype=np.uint64)[:-1]]).astype(np.uint64)
+        rec = np.zeros(max(1, n), dtype=_OP_DTYPE)
+        if n:
+            rec["gate"][:n] = gids
+            rec["nwires"][:n] = nw
+            rec["wires"][:n] = np.uint64(W.ctypes.data) + np.uint64(4) * woff[:n]
+            rec["inverse"][:n] = inv
+            rec["nparams"][:n] = npar
+            rec["params"][:n] = np.uint64(P.ctypes.data) + np.uint64(8) * poff[:n]
+            for i, m in mats.items():
+                rec["matrix"][i] = m.ctypes.data
+        self._keep += [W, P, list(mats.values()), rec]
+        self.arr = C.cast(rec.ctypes.data, C.POINTER(Op))
 
     @property
     def ptr(self):
@@ -273,6 +308,10 @@ class StateVector:
         check(lib().b200sv_download(self.h, a.ctypes.data, a.size))
         return a
 
+    def copy_from(self, src: "StateVector"):
+        """Device-to-device copy of another handle's amplitudes (same width and dtype)."""
+        check(lib().b200sv_copy(self.h, src.h))
+
     def set_basis_state(self, index: int):
         check(lib().b200sv_set_basis_state(self.h, int(index)))
 
@@ -299,9 +338,16 @@ class StateVector:
         w, wp = _u32(wires)
         check(lib().b200sv_apply_matrix(self.h, m.ctypes.data, wp, len(w), 1 if inverse else 0))
 
+    def _oplist(self, ops):
+        return ops if isinstance(ops, OpList) else OpList(ops, self.np_dtype)
+
     def apply_ops(self, ops):
-        ol = OpList(ops, self.np_dtype)
+        ol = self._oplist(ops)
         check(lib().b200sv_apply_ops(self.h, ol.ptr, ol.n))
+
+    def apply_ops_fused(self, ops):
+        ol = self._oplist(ops)
+        check(lib().b200sv_apply_ops_fused(self.h, ol.ptr, ol.n))
 
     def apply_generator(self, name, wires, adj=False) -> float:
         gid = name if isinstance(name, int) else GENERATOR_IDS[name]
@@ -330,6 +376,23 @@ class StateVector:
         r = C.c_double()
         check(lib().b200sv_var(self.h, C.byref(ob.obs), C.byref(r)))
         return r.value
+
+    def _sparse(self, fn, indptr, indices, data) -> float:
+        rows = np.ascontiguousarray(indptr, dtype=np.uint64)
+        cols = np.ascontiguousarray(indices, dtype=np.uint64)
+        vals = np.ascontiguousarray(data, dtype=self.np_dtype)
+        r = C.c_double()
+        check(fn(self.h, rows.ctypes.data_as(C.POINTER(C.c_uint64)), rows.size,
+                 cols.ctypes.data_as(C.POINTER(C.c_uint64)), vals.ctypes.data_as(C.c_void_p), vals.size,
+                 C.byref(r)))
+        return r.value
+
+    def expval_sparse(self, indptr, indices, data) -> float:
+        """Re<psi|H psi> for H in CSR form (scipy's indptr, indices, data)."""
+        return self._sparse(lib().b200sv_expval_sparse, indptr, indices, data)
+
+    def var_sparse(self, indptr, indices, data) -> float:
+        return self._sparse(lib().b200sv_var_sparse, indptr, indices, data)
 
     def expval_pauli(self, words, coeffs=None):
         """words: list of (pauli_string, wires); returns (per-term values, weighted sum)."""
@@ -377,6 +440,16 @@ class StateVector:
             u, up = _f64(uniforms)
         check(lib().b200sv_sample_bits(self.h, nshots, up, seed, out.ctypes.data_as(C.POINTER(C.c_uint64))))
         return out[:nshots * self.num_qubits].reshape(nshots, self.num_qubits)
+
+    def vjp_state(self, ops, dy, trainable, apply_operations=False):
+        ol = OpList(ops, self.np_dtype)
+        d = np.ascontiguousarray(np.asarray(dy, dtype=self.np_dtype))
+        tp = np.ascontiguousarray(np.asarray(trainable, dtype=np.uint64))
+        out = np.zeros(2 * max(1, len(tp)), dtype=np.float64)
+        check(lib().b200sv_vjp_state(self.h, ol.ptr, ol.n, d.ctypes.data, d.size,
+                                     tp.ctypes.data_as(C.POINTER(C.c_uint64)), len(tp), 1 if apply_operations else 0,
+                                     out.ctypes.data_as(C.POINTER(C.c_double))))
+        return out[0:2 * len(tp):2] + 1j * out[1:2 * len(tp):2]
 
     def adjoint_jacobian(self, ops, observables, trainable, apply_operations=False):
         ol = OpList(ops, self.np_dtype)

@@ -107,3 +107,35 @@ def adjoint_jacobian(m, state, ops, observables, trainable):
     adj = getattr(m.algorithms, "AdjointJacobian" + s)()
     jac = np.asarray(adj(sv, obs, opsd, list(trainable)))
     return jac.reshape(len(observables), len(trainable))
+
+
+def vjp_state(m, state, ops, dy, trainable):
+    """VectorJacobianProductC*()(sv, ops, dy, tp) of the reference (LQ/bindings/LQubitBindings.hpp:186-246)."""
+    dtype = state.dtype
+    s = _suffix(dtype)
+    sv = getattr(m, "StateVector" + s)(state)
+    names = [op[0] for op in ops]
+    params = [list(op[3]) for op in ops]
+    wires = [list(op[1]) for op in ops]
+    invs = [bool(op[2]) for op in ops]
+    mats = [np.zeros(0, dtype=dtype) for _ in ops]
+    opsd = getattr(m.algorithms, "create_ops_list" + s)(names, params, wires, invs, mats)
+    vjp = getattr(m.algorithms, "VectorJacobianProduct" + s)()
+    return np.asarray(vjp(sv, opsd, np.ascontiguousarray(np.asarray(dy, dtype=dtype)), list(trainable)))
+
+
+def _sparse(m, state, indptr, indices, data, what):
+    """MeasurementsC*.expval/var(row_map, entries, values) (LQ/bindings/LQubitBindings.hpp:127-161)."""
+    dtype = state.dtype
+    sv = getattr(m, "StateVector" + _suffix(dtype))(state)
+    M = getattr(m, "Measurements" + _suffix(dtype))(sv)
+    return float(getattr(M, what)(np.asarray(indptr, dtype=np.uint64), np.asarray(indices, dtype=np.uint64),
+                                  np.asarray(data, dtype=dtype)))
+
+
+def sparse_expval(m, state, indptr, indices, data):
+    return _sparse(m, state, indptr, indices, data, "expval")
+
+
+def sparse_var(m, state, indptr, indices, data):
+    return _sparse(m, state, indptr, indices, data, "var")

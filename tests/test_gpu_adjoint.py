@@ -156,3 +156,38 @@ def test_adjoint_errors(capi):
         jac(capi, 1, [("Rot", [0], False, [0.1, 0.2, 0.3])], [Zs(0)], [0])
     with pytest.raises(capi.B200Error, match="sorted"):
         jac(capi, 1, [("RX", [0], False, [0.1]), ("RY", [0], False, [0.1])], [Zs(0)], [1, 0])
+
+
+@pytest.mark.parametrize("dtype", [np.complex128, np.complex64])
+def test_vjp_state(capi, dtype):
+    """State-return VJP (VectorJacobianProduct.hpp:60-156) vs the oracle and the reference module."""
+    import lq_oracle as O
+    import ref
+    from lightning_b200.workloads import layered_rotations
+    rng = np.random.default_rng(9)
+    n = 7
+    ops, _, _ = layered_rotations(n=n, layers=2, seed=4)
+    ops = ops + [("CRX", [6, 1], False, [0.3]), ("SingleExcitation", [2, 5], True, [0.8]),
+                 ("MultiRZ", [0, 3, 6], False, [0.2]), ("DoubleExcitationMinus", [0, 2, 4, 6], False, [0.5])]
+    psi = O.run_circuit(n, ops)
+    dy = (rng.normal(size=1 << n) + 1j * rng.normal(size=1 << n)) / 8
+    npar = sum(1 for op in ops if op[3])
+    tp = list(range(1, npar, 2))
+    sv = capi.StateVector(n, dtype)
+    sv.upload(psi.astype(dtype))
+    got = sv.vjp_state(ops, dy.astype(dtype), tp)
+    want = O.vjp_state(psi.astype(dtype).astype(np.complex128), ops, dy.astype(dtype).astype(np.complex128), tp)
+    tol = 1e-12 if dtype == np.complex128 else 2e-5
+    assert np.abs(got - want).max() < tol
+    m = ref.load()
+    if m is not None and dtype == np.complex128:
+        assert np.abs(got - ref.vjp_state(m, psi.copy(), ops, dy, tp)).max() < 1e-12
+    import lightning_b200.lightning_qubit_ops as ours
+    st = psi.astype(dtype).copy()
+    svo = getattr(ours, "StateVectorC" + ("64" if dtype == np.complex64 else "128"))(st)
+    sfx = "C64" if dtype == np.complex64 else "C128"
+    opsd = getattr(ours.algorithms, "create_ops_list" + sfx)(
+        [o[0] for o in ops], [list(o[3]) for o in ops], [list(o[1]) for o in ops], [bool(o[2]) for o in ops],
+        [np.zeros(0, dtype=dtype) for _ in ops])
+    res = getattr(ours.algorithms, "VectorJacobianProduct" + sfx)()(svo, opsd, dy.astype(dtype), tp)
+    assert np.abs(np.asarray(res) - want).max() < tol * 10

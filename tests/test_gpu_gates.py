@@ -161,3 +161,29 @@ def test_apply_ops_sequence_and_errors(capi):
         sv.apply("RX", [0], False, [])
     with pytest.raises(capi.B200Error, match="expected 2 wires"):
         sv.apply("CNOT", [0])
+
+
+@pytest.mark.parametrize("dtype", [np.complex128, np.complex64])
+@pytest.mark.parametrize("n", [20, 22])
+def test_fused_apply_matches_oracle(capi, n, dtype):
+    """b200sv_apply_ops_fused (segments of gates applied per shared-memory tile) on the gate-sweep
+    family plus gates the tile forms do not cover (three-wire matrices, four-wire excitations,
+    Rot, wide MultiRZ), which run as their own passes in order."""
+    import lq_oracle as O
+    from lightning_b200.workloads import gate_sweep, random_unitary, random_state as rs
+    rng = np.random.default_rng(n)
+    ops = gate_sweep(n, 120, seed=n)
+    extra = [("Rot", [3], False, [0.1, 0.7, -0.4]), ("DoubleExcitation", [0, 5, 9, n - 1], False, [0.3]),
+             ("MultiRZ", list(range(0, n, 2)), False, [0.9]), ("QubitUnitary", [1, 7, n - 2], False, [],
+                                                                  random_unitary(rng, 3)),
+             ("CRot", [n - 1, 2], True, [0.2, 0.3, 0.4]), ("IsingXY", [4, n - 3], False, [1.1]),
+             ("PhaseShift", [n - 1], False, [0.5]), ("S", [0], True, []), ("CSWAP", [2, 9, 14], False, [])]
+    for k, op in enumerate(extra):
+        ops.insert(10 * k + 5, op)
+    st = rs(n, seed=n, dtype=dtype)
+    sv = capi.StateVector(n, dtype)
+    sv.upload(st)
+    sv.apply_ops_fused(ops)
+    want = O.run_circuit(n, ops, state=st.astype(np.complex128))
+    tol = 1e-12 if dtype == np.complex128 else 2e-5
+    assert np.abs(sv.download() - want).max() < tol

@@ -136,3 +136,58 @@ def test_sampling_distribution(capi):
     assert np.allclose(hist, p, atol=0.05)
     assert np.allclose(p, [0.67078706, 0.03062806, 0.0870997, 0.00397696, 0.17564072, 0.00801973,
                            0.02280642, 0.00104134], atol=1e-6)
+
+
+@pytest.mark.parametrize("dtype", [np.complex128, np.complex64])
+def test_sparse_golden(capi, dtype):
+    """LQ/measurements/tests/Test_MeasurementsLQubitSparse.cpp:41-78."""
+    import lq_oracle as O
+    sv = capi.StateVector(3, dtype)
+    sv.apply_ops(nontrivial_state_ops())
+    csr = O.tridiagonal_periodic_csr(8)
+    assert abs(sv.expval_sparse(*csr) - 0.5930885) < 1e-6
+    assert abs(sv.var_sparse(*csr) - 2.4624654) < 1e-6
+    with pytest.raises(capi.B200Error, match="Statevector and Hamiltonian have incompatible sizes."):
+        sv.expval_sparse(*O.tridiagonal_periodic_csr(16))
+
+
+@pytest.mark.parametrize("n,density", [(1, 1.0), (5, 0.3), (8, 0.03), (10, 0.04), (12, 0.0005), (14, 0.00002)])
+@pytest.mark.parametrize("dtype", [np.complex128, np.complex64])
+def test_sparse_vs_oracle(capi, n, density, dtype):
+    """Ragged rows (lane widths 1..32 are all reached over the sizes), empty rows,
+    unsorted and repeated columns, a row_map that does not start at zero."""
+    import scipy.sparse as sp
+    import lq_oracle as O
+    rng = np.random.default_rng(n)
+    N = 1 << n
+    A = sp.random(N, N, density=density, format="csr", random_state=n, dtype=np.float64)
+    A = (A + 1j * sp.random(N, N, density=density, format="csr", random_state=n + 1)).tocsr()
+    A.data[::5] = 0  # explicit zeros stay in the structure
+    indptr = A.indptr.astype(np.uint64) + 7
+    indices = A.indices.astype(np.uint64)
+    perm = np.concatenate([rng.permutation(np.arange(a, b)) for a, b in zip(A.indptr[:-1], A.indptr[1:])]
+                          or [np.zeros(0, int)]).astype(np.int64)
+    indices, data = indices[perm], A.data[perm].astype(dtype)
+    if len(indices) > 1:
+        indices[1] = indices[0]  # a repeated column inside a row is summed as given
+    st = random_state(rng, n, dtype)
+    sv = capi.StateVector(n, dtype)
+    sv.upload(st)
+    want_e = O.sparse_expval(st, indptr - 7, indices, data)
+    want_v = O.sparse_var(st, indptr - 7, indices, data)
+    tol = 1e-10 if dtype == np.complex128 else 1e-4
+    scale = max(1.0, abs(want_v))
+    assert abs(sv.expval_sparse(indptr, indices, data) - want_e) < tol * scale
+    assert abs(sv.var_sparse(indptr, indices, data) - want_v) < tol * scale
+
+
+def test_sparse_rejects_bad_csr(capi):
+    sv = capi.StateVector(2)
+    rows = np.array([0, 1, 2, 3, 4], dtype=np.uint64)
+    with pytest.raises(capi.B200Error, match="column index out of range"):
+        sv.expval_sparse(rows, np.array([0, 1, 2, 4], dtype=np.uint64), np.ones(4))
+    with pytest.raises(capi.B200Error, match="non-decreasing"):
+        sv.expval_sparse(np.array([0, 2, 1, 3, 4], dtype=np.uint64), np.zeros(4, dtype=np.uint64), np.ones(4))
+    with pytest.raises(capi.B200Error, match="more non-zeros"):
+        sv.expval_sparse(rows, np.zeros(3, dtype=np.uint64), np.ones(3))
+    assert sv.expval_sparse(np.zeros(5, dtype=np.uint64), np.zeros(0, dtype=np.uint64), np.zeros(0)) == 0.0

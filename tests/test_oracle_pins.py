@@ -191,3 +191,64 @@ def test_finite_difference_agrees_with_adjoint():
     adj = O.adjoint_jacobian(O.run_circuit(4, ops), ops, obs, tp)
     fd = O.finite_difference_jacobian(4, ops, obs, h=1e-5)
     assert np.abs(adj - fd).max() < 1e-8
+
+
+def test_vjp_state_matches_live_reference(ref_module):
+    import ref
+    from lightning_b200.workloads import layered_rotations
+    rng = np.random.default_rng(8)
+    ops, _, _ = layered_rotations(n=5, layers=2, seed=21)
+    ops = ops + [("CRY", [0, 3], True, [0.7]), ("IsingXY", [1, 4], False, [0.4]), ("PhaseShift", [2], True, [1.2])]
+    psi = O.run_circuit(5, ops)
+    dy = rng.normal(size=32) + 1j * rng.normal(size=32)
+    npar = sum(1 for op in ops if op[3])
+    tp = list(range(0, npar, 3))
+    a = O.vjp_state(psi, ops, dy, tp)
+    b = ref.vjp_state(ref_module, psi.copy(), ops, dy, tp)
+    assert np.abs(a - b).max() < 1e-13
+
+
+def test_sparse_golden_values():
+    """LQ/utils/tests/Test_SparseLinAlg.cpp:33-70 (CSR product) and
+    LQ/measurements/tests/Test_MeasurementsLQubitSparse.cpp:41-61 (expval, var) on the
+    periodic tridiagonal matrix of CS/utils/TestHelpers.hpp:430-470."""
+    indptr, indices, data = O.tridiagonal_periodic_csr(8)
+    v1 = np.array([0.33160916, 0.90944626, 0.81097291, 0.46112135, 0.42801563, 0.38077181, 0.23550137, 0.57416324])
+    r1 = [-1.15200034, -0.23313581, -0.5595947, -0.7778672, -0.41387753, -0.28274519, -0.71943368, 0.00705271]
+    v2 = np.array([0.26752544 + 0.00484225j, 0.49189265 + 0.21231633j, 0.28691029 + 0.87552205j,
+                   0.13499786 + 0.63862517j, 0.31748372 + 0.25701515j, 0.96968437 + 0.69821151j,
+                   0.53674213 + 0.58564544j, 0.02213429 + 0.3050882j])
+    r2 = np.array([-0.24650151 - 0.51256229j, -0.06254307 - 0.66804797j, -0.33998022 + 0.02458055j,
+                   -0.46939616 - 0.49391203j, -0.7871985 - 1.07982153j, 0.11545852 - 0.14444908j,
+                   -0.45507653 - 0.41765428j, -0.78213328 - 0.28539948j])
+    assert np.allclose(O.sparse_matvec(v1, indptr, indices, data), r1, atol=1e-6)
+    assert np.allclose(O.sparse_matvec(v2, indptr, indices, data), r2, atol=1e-6)
+    st = nontrivial_state()
+    assert abs(O.sparse_expval(st, indptr, indices, data) - 0.5930885) < 1e-6
+    assert abs(O.sparse_var(st, indptr, indices, data) - 2.4624654) < 1e-6
+    with pytest.raises(ValueError, match="incompatible sizes"):
+        O.sparse_expval(st, *O.tridiagonal_periodic_csr(16))
+
+
+def random_csr(n, rng, density=0.3, empty_rows=True):
+    """Random complex CSR matrix with ragged rows (some empty) and unsorted columns."""
+    N = 1 << n
+    rows, cols, vals = [0], [], []
+    for r in range(N):
+        k = 0 if (empty_rows and r % 7 == 3) else int(rng.integers(0, max(2, int(density * N)) + 1))
+        c = rng.choice(N, size=k, replace=False)
+        cols += list(c)
+        vals += list(rng.normal(size=k) + 1j * rng.normal(size=k))
+        rows.append(len(cols))
+    return (np.array(rows, dtype=np.uint64), np.array(cols, dtype=np.uint64), np.array(vals, dtype=np.complex128))
+
+
+def test_sparse_matches_live_reference(ref_module):
+    import ref
+    rng = np.random.default_rng(17)
+    for n in (1, 3, 6):
+        st = rng.normal(size=1 << n) + 1j * rng.normal(size=1 << n)
+        st /= np.linalg.norm(st)
+        csr = random_csr(n, rng)
+        assert abs(O.sparse_expval(st, *csr) - ref.sparse_expval(ref_module, st, *csr)) < 1e-12
+        assert abs(O.sparse_var(st, *csr) - ref.sparse_var(ref_module, st, *csr)) < 1e-12
