@@ -234,6 +234,28 @@ int b200sv_sample(b200sv_handle h, uint64_t nshots, const double *uniforms,
 int b200sv_sample_bits(b200sv_handle h, uint64_t nshots, const double *uniforms,
                        uint64_t seed, uint64_t *bits_out);
 
+/* Metropolis-Hastings sampling (generate_samples_metropolis,
+ * LQ/measurements/MeasurementsLQubit.hpp:387-434; metropolis_step :612-640;
+ * proposals LQ/measurements/TransitionKernels.hpp:56-160).  nchains independent
+ * chains start at basis index 0, take num_burnin steps, then chain c gives
+ * samples c, c + nchains, ... from consecutive steps; nchains = 1 is the
+ * reference's single chain.  A step accepts the proposal t from i when
+ * p_i == 0 or U * p_i < p_t (p = |amplitude|^2 in FP64), i.e.
+ * U < min(1, p_t / p_i).  Random numbers: Philox4x32-10, counter
+ * (step_lo, step_hi, chain, 0x4D434D43), key seed; the indices are a
+ * deterministic function of state, seed and nchains.
+ * proposal: B200SV_MCMC_LOCAL sets a uniformly chosen bit to a uniformly chosen
+ * value (LocalTransitionKernel); B200SV_MCMC_NONZERO draws uniformly among the
+ * basis states with |amplitude| > machine epsilon of the state's precision
+ * (NonZeroRandomTransitionKernel).  The reference binds its kernel names the
+ * other way round (kernel_factory, TransitionKernels.hpp:147-159): its "Local"
+ * name runs the non-zero proposal and "NonZeroRandom" the local one.
+ * idx_out: nshots basis indices. */
+enum b200sv_mcmc_proposal { B200SV_MCMC_LOCAL = 0, B200SV_MCMC_NONZERO = 1 };
+int b200sv_sample_mcmc(b200sv_handle h, int proposal, uint64_t num_burnin,
+                       uint64_t nshots, uint32_t nchains, uint64_t seed,
+                       uint64_t *idx_out);
+
 /* Allocation-free Pauli-word expectation values.  No counterpart in the
  * reference: this entry point exists for callers that cannot call cudaMalloc
  * when they need the result (device memory owned by another allocator such as

@@ -210,6 +210,23 @@ template <class T> void register_precision(py::module_ &m, py::module_ &obsm, py
                  std::copy(r.begin(), r.end(), a.mutable_data());
                  return a;
              })
+        .def("generate_mcmc_samples",  // LQ/bindings/LQubitBindings.hpp:162-182
+             [](M &ms, size_t num_wires, const std::string &kernelname, size_t num_burnin, size_t num_shots) {
+                 auto r = ms.generate_samples_metropolis(kernelname, num_burnin, num_shots);
+                 py::array_t<size_t> a({num_shots, num_wires});
+                 std::copy(r.begin(), r.end(), a.mutable_data());
+                 return a;
+             })
+        .def("generate_mcmc_samples",
+             [](M &ms, size_t num_wires, const std::string &kernelname, size_t num_burnin, size_t num_shots,
+                uint64_t seed, uint32_t num_chains) {
+                 auto r = ms.generate_samples_metropolis(kernelname, num_burnin, num_shots, seed, num_chains);
+                 py::array_t<size_t> a({num_shots, num_wires});
+                 std::copy(r.begin(), r.end(), a.mutable_data());
+                 return a;
+             },
+             py::arg("num_wires"), py::arg("kernelname"), py::arg("num_burnin"), py::arg("num_shots"),
+             py::arg("seed"), py::arg("num_chains") = 4096)
         .def("generate_samples_from_uniforms", [](M &ms, size_t num_wires,
                                                   const py::array_t<double, py::array::c_style | py::array::forcecast> &u) {
             auto b = u.request();

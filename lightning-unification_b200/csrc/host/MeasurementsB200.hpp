@@ -101,6 +101,26 @@ template <class StateVectorT> class Measurements {
     std::vector<size_t> generate_samples(size_t num_samples) const {
         return generate_samples(num_samples, std::random_device{}());
     }
+    // generate_samples_metropolis (:387-434): bits of num_samples indices, wire 0 first.
+    // The kernel name is bound to a proposal as the reference binds it (kernel_factory,
+    // TransitionKernels.hpp:147-159: "NonZeroRandom" runs the local proposal, any other
+    // name the non-zero one).  num_chains independent chains share the samples.
+    std::vector<size_t> generate_samples_metropolis(const std::string &kernelname, size_t num_burnin,
+                                                    size_t num_samples, uint64_t seed,
+                                                    uint32_t num_chains = 4096) const {
+        const size_t n = sv_.getNumQubits();
+        const int proposal = kernelname == "NonZeroRandom" ? B200SV_MCMC_LOCAL : B200SV_MCMC_NONZERO;
+        std::vector<uint64_t> idx(num_samples);
+        check(b200sv_sample_mcmc(sv_.handle(), proposal, num_burnin, num_samples, num_chains, seed, idx.data()));
+        std::vector<size_t> bits(num_samples * n);
+        for (size_t s = 0; s < num_samples; ++s)
+            for (size_t j = 0; j < n; ++j) bits[s * n + (n - 1 - j)] = (idx[s] >> j) & 1u;
+        return bits;
+    }
+    std::vector<size_t> generate_samples_metropolis(const std::string &kernelname, size_t num_burnin,
+                                                    size_t num_samples) const {
+        return generate_samples_metropolis(kernelname, num_burnin, num_samples, std::random_device{}());
+    }
     // seeded variant taking caller uniforms (bit-exact reproducibility)
     std::vector<size_t> generate_samples_from_uniforms(const std::vector<double> &u) const {
         const size_t n = sv_.getNumQubits();

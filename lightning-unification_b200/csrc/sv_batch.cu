@@ -719,25 +719,6 @@ __global__ void __launch_bounds__(512) k_batch(KArgs A) {
     }
 }
 
-// One fused segment over a single large state: every CTA takes tiles of the
-// segment's local bits, applies the segment's gates in shared memory and writes
-// the tile back — one HBM pass for the whole run of gates.
-template <typename R>
-__global__ void __launch_bounds__(512) k_segment(KArgs A, DSeg sg, void *state, uint64_t ntiles, int kt) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    C<R> *tile = reinterpret_cast<C<R> *>(smem_raw);
-    C<R> *sv = static_cast<C<R> *>(state);
-    C<R> *tiles[1] = {tile};
-    const uint32_t tn = 1u << kt;
-    for (uint64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
-        const uint64_t tbase = insert_zeros64(t, sg.lbits, sg.nl);
-        load_tile<R>(tile, sv, sg, tbase, tn);
-        exec_segment<R, 1, false>(A, tiles, kt, sg, true);
-        store_tile<R>(sv, tile, sg, tbase, tn);
-        __syncthreads();
-    }
-}
-
 // flag <- valid && all(a == b)   (the caller copies `valid` into `flag` first)
 __global__ void k_params_equal(const double *__restrict__ a, const double *__restrict__ b, uint64_t n, int *flag) {
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
@@ -1450,149 +1431,6 @@ template <class F> void run_maybe_graph(Batch &B, cudaGraphExec_t &exec, F &&enq
     B200SV_CUDA(cudaGraphLaunch(exec, st));
 }
 
-// ---- fused application of one op list to one state ---------------------------
-int fused_tile_bits(int dtype, uint32_t n) {
-    const int kt = dtype == B200SV_C64 ? 13 : 12;
-    return (int)std::min<uint32_t>(kt, n > 8 ? n - 8 : 1);
-}
-
-void apply_ops_fused(const StateView &v, const b200sv_op *ops, uint32_t nops) {
-    const uint32_t n = v.nq;
-    const int kt = fused_tile_bits(v.dtype, n);
-    const cudaStream_t st = v.stream;
-    const size_t amp = v.dtype == B200SV_C64 ? 8 : 16;
-    // which ops the tile forms cover
-    std::vector<HostOp> hops(nops);
-    std::vector<char> tiled(nops, 0);
-    for (uint32_t i = 0; i < nops; ++i) {
-        if (ops[i].gate == B200SV_OP_SKIP) continue;
-        try {
-            hops[i] = make_hostop(ops[i], -1, n, v.dtype);
-            tiled[i] = (int)hops[i].bits.size() <= kt ? 1 : 0;
-        } catch (const Unsupported &) {
-            tiled[i] = 0;
-        }
-    }
-    Planned P;
-    push_const(P, {});
-    struct Piece {
-        bool seg;
-        DSeg s;
-        uint32_t op;  // untiled op index
-    };
-    std::vector<Piece> pieces;
-    uint32_t i = 0;
-    while (i < nops) {
-        if (ops[i].gate == B200SV_OP_SKIP) { ++i; continue; }
-        if (!tiled[i]) {
-            pieces.push_back(Piece{false, DSeg{}, i});
-            ++i;
-            continue;
-        }
-        uint64_t used = 0;
-        const uint64_t low = low_reserve_mask(v.dtype, (uint32_t)kt);
-        uint32_t j = i;
-        while (j < nops && (tiled[j] || ops[j].gate == B200SV_OP_SKIP)) {
-            if (ops[j].gate == B200SV_OP_SKIP) { ++j; continue; }
-            uint64_t b = 0;
-            for (auto x : hops[j].bits) b |= uint64_t(1) << x;
-            if (popcount64(used | b) > kt || (popcount64(used | b | low) > kt && j > i)) break;
-            used |= b;
-            ++j;
-        }
-        std::vector<uint32_t> L;
-        for (uint32_t x = 0; x < n; ++x)
-            if (used & (uint64_t(1) << x)) L.push_back(x);
-        for (uint32_t x = 0; x < n && (int)L.size() < kt; ++x)
-            if (!(used & (uint64_t(1) << x))) L.push_back(x);
-        std::sort(L.begin(), L.end());
-        DSeg sg{};
-        sg.nl = (uint8_t)L.size();
-        std::vector<int> loc(n, -1);
-        for (size_t q = 0; q < L.size(); ++q) {
-            sg.lbits[q] = (uint8_t)L[q];
-            loc[L[q]] = (int)q;
-        }
-        uint8_t ng = 0;
-        for (uint32_t x = 0; x < n; ++x)
-            if (loc[x] < 0) sg.gbits[ng++] = (uint8_t)x;
-        sg.ng = ng;
-        sg.op_begin = (uint32_t)P.ops.size();
-        for (uint32_t q = i; q < j; ++q)
-            if (ops[q].gate != B200SV_OP_SKIP) P.ops.push_back(lower(P, hops[q], loc));
-        sg.nops = (uint32_t)(P.ops.size() - sg.op_begin);
-        mark_runs(P.ops.data() + sg.op_begin, sg.nops, P.consts.data());
-        pieces.push_back(Piece{true, sg, 0});
-        i = j;
-    }
-    DOp *d_ops = nullptr;
-    double2 *d_consts = nullptr;
-    void *d_mat = nullptr;
-    B200SV_CUDA(cudaMallocAsync((void **)&d_ops, std::max<size_t>(1, P.ops.size()) * sizeof(DOp), st));
-    B200SV_CUDA(cudaMallocAsync((void **)&d_consts, std::max<size_t>(1, P.consts.size()) * sizeof(double2), st));
-    struct Free {
-        DOp *&o;
-        double2 *&c;
-        void *&m;
-        cudaStream_t s;
-        ~Free() {
-            cudaFreeAsync(o, s);
-            cudaFreeAsync(c, s);
-            if (m) cudaFreeAsync(m, s);
-        }
-    } guard{d_ops, d_consts, d_mat, st};
-    if (!P.ops.empty())
-        B200SV_CUDA(cudaMemcpyAsync(d_ops, P.ops.data(), P.ops.size() * sizeof(DOp), cudaMemcpyHostToDevice, st));
-    B200SV_CUDA(cudaMemcpyAsync(d_consts, P.consts.data(), P.consts.size() * sizeof(double2), cudaMemcpyHostToDevice, st));
-    KArgs A{};
-    A.ops = d_ops;
-    A.consts = d_consts;
-    const int threads = 512;
-    const size_t smem = amp << kt;
-    int per_sm = 1;
-    if (v.dtype == B200SV_C64) {
-        B200SV_CUDA(cudaFuncSetAttribute(k_segment<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        B200SV_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_segment<float>, threads, smem));
-    } else {
-        B200SV_CUDA(cudaFuncSetAttribute(k_segment<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        B200SV_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_segment<double>, threads, smem));
-    }
-    const uint64_t ntiles = uint64_t(1) << (n - kt);
-    const unsigned grid = (unsigned)std::min<uint64_t>(ntiles, (uint64_t)sm_count() * std::max(1, per_sm));
-    for (const Piece &pc : pieces) {
-        if (pc.seg) {
-            if (v.dtype == B200SV_C64) k_segment<float><<<grid, threads, smem, st>>>(A, pc.s, v.state, ntiles, kt);
-            else k_segment<double><<<grid, threads, smem, st>>>(A, pc.s, v.state, ntiles, kt);
-            B200SV_CUDA(cudaGetLastError());
-            continue;
-        }
-        // a gate outside the tile forms: its own pass with the per-gate kernels
-        const b200sv_op &o = ops[pc.op];
-        GateDesc g;
-        if (o.gate == B200SV_OP_MATRIX) {
-            const size_t d = size_t(1) << o.nwires;
-            std::vector<cd> m(d * d);
-            for (size_t q = 0; q < d * d; ++q) {
-                if (v.dtype == B200SV_C64) {
-                    const float *f = static_cast<const float *>(o.matrix);
-                    m[q] = cd(f[2 * q], f[2 * q + 1]);
-                } else {
-                    const double *f = static_cast<const double *>(o.matrix);
-                    m[q] = cd(f[2 * q], f[2 * q + 1]);
-                }
-            }
-            g = compile_matrix(m.data(), o.wires, o.nwires, o.inverse != 0, n);
-        } else {
-            g = compile_gate(o.gate, o.wires, o.nwires, o.inverse != 0, o.params, o.nparams, n);
-        }
-        if (g.kind == Kind::Dense && g.k >= 4 && !d_mat)
-            B200SV_CUDA(cudaMallocAsync(&d_mat, amp << (2 * 11), st));
-        void *states[1] = {v.state};
-        if (v.dtype == B200SV_C64) launch_gate<float>(states, 1, n, g, d_mat, st);
-        else launch_gate<double>(states, 1, n, g, d_mat, st);
-    }
-}
-
 }  // namespace batch
 }  // namespace b200sv
 
@@ -1672,24 +1510,6 @@ int b200sv_batch_create(int dtype, const b200sv_batch_circuit *circuits, uint32_
         auto *h = new b200sv_batch;
         h->b = std::move(B);
         *out = h;
-    });
-}
-
-int b200sv_apply_ops_fused(b200sv_handle h, const b200sv_op *ops, uint32_t nops) {
-    return run_guarded([&] {
-        const StateView v = state_view(h);
-        if (nops && !ops) throw ArgError("operations pointer is NULL");
-        int cur = -1;
-        cudaGetDevice(&cur);
-        if (cur != v.device) B200SV_CUDA(cudaSetDevice(v.device));
-        if (v.nq < (uint32_t)fused_tile_bits(v.dtype, v.nq) + 8) {
-            // too narrow for enough tiles to fill the GPU: the per-gate path
-            const int rc = b200sv_apply_ops(h, ops, nops);
-            if (rc != B200SV_OK) throw ArgError(b200sv_last_error());
-        } else {
-            apply_ops_fused(v, ops, nops);
-        }
-        if (cur != v.device && cur >= 0) cudaSetDevice(cur);
     });
 }
 

@@ -374,11 +374,6 @@ void check_handle(b200sv_state *h) { need(h != nullptr, "NULL state handle"); }
 
 int b200sv::run_guarded(const std::function<void()> &f) { return guard(f); }
 
-b200sv::StateView b200sv::state_view(b200sv_handle h) {
-    need(h != nullptr, "NULL state handle");
-    return StateView{h->d_state, h->nq, h->dtype, h->stream(), h->device};
-}
-
 // =============================================================================
 extern "C" {
 
@@ -561,6 +556,25 @@ int b200sv_apply_ops(b200sv_handle h, const b200sv_op *ops, uint32_t nops) {
         for (auto &o : rec) descs.push_back(compile_op(o, o.inverse, h->nq));  // validate all first
         void *s[1] = {h->d_state};
         for (auto &g : descs) apply_desc(h, s, 1, g);
+    });
+}
+
+int b200sv_apply_ops_fused(b200sv_handle h, const b200sv_op *ops, uint32_t nops) {
+    return guard([&] {
+        check_handle(h);
+        DeviceGuard dg(h->device);
+        auto rec = read_ops(ops, nops, h->dtype);
+        std::vector<GateDesc> descs;
+        descs.reserve(rec.size());
+        for (auto &o : rec) descs.push_back(compile_op(o, o.inverse, h->nq));  // validate all first
+        void *s[1] = {h->d_state};
+        if (!fused_worthwhile(h->dtype, h->nq)) {
+            // too few tiles to fill the GPU: one launch per gate
+            for (auto &g : descs) apply_desc(h, s, 1, g);
+            return;
+        }
+        apply_fused(h->d_state, h->nq, h->dtype, descs, [&](const GateDesc &g) { apply_desc(h, s, 1, g); },
+                    h->stream());
     });
 }
 
@@ -810,6 +824,26 @@ int b200sv_sample_bits(b200sv_handle h, uint64_t nshots, const double *uniforms,
         // bits MSB (wire 0) first, as MeasurementsLQubit.hpp:549-554
         for (uint64_t s = 0; s < nshots; ++s)
             for (uint32_t j = 0; j < n; ++j) bits_out[s * n + (n - 1 - j)] = (idx[s] >> j) & 1u;
+    });
+}
+
+int b200sv_sample_mcmc(b200sv_handle h, int proposal, uint64_t num_burnin, uint64_t nshots, uint32_t nchains,
+                       uint64_t seed, uint64_t *idx_out) {
+    return guard([&] {
+        check_handle(h);
+        need(nshots == 0 || idx_out != nullptr, "NULL output");
+        DeviceGuard dg(h->device);
+        const cudaStream_t st = h->stream();
+        uint64_t *idx = nullptr;
+        B200SV_CUDA(cudaMallocAsync((void **)&idx, std::max<uint64_t>(1, nshots) * sizeof(uint64_t), st));
+        struct Free {
+            uint64_t *p;
+            cudaStream_t s;
+            ~Free() { cudaFreeAsync(p, s); }
+        } fr{idx, st};
+        sample_mcmc(h->d_state, h->nq, h->dtype, proposal, num_burnin, nshots, nchains, seed, idx, st);
+        if (nshots) B200SV_CUDA(cudaMemcpyAsync(idx_out, idx, nshots * sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
+        B200SV_CUDA(cudaStreamSynchronize(st));
     });
 }
 

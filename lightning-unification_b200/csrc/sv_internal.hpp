@@ -14,16 +14,6 @@
 
 namespace b200sv {
 
-// What the fused and batched paths need to see of a state handle (sv_capi.cu).
-struct StateView {
-    void *state;
-    uint32_t nq;
-    int dtype;
-    cudaStream_t stream;
-    int device;
-};
-StateView state_view(b200sv_handle h);
-
 struct CudaError : std::runtime_error {
     using std::runtime_error::runtime_error;
 };
@@ -92,6 +82,16 @@ template <typename R>
 void reduce_sparse(const void *psi, uint32_t nq, const uint64_t *row_map_dev, const uint64_t *cols_dev,
                    const void *vals_dev, uint64_t nnz, double *partials, double *out_dev, cudaStream_t st);
 int sparse_lanes(uint64_t nrows, uint64_t nnz);
+// Metropolis-Hastings chains (sv_mcmc.cu): nshots indices into a device buffer.
+void sample_mcmc(const void *state, uint32_t nq, int dtype, int proposal, uint64_t burnin, uint64_t nshots,
+                 uint64_t nchains, uint64_t seed, uint64_t *idx_dev, cudaStream_t st);
+// Fused application of compiled gates to one state (sv_fused.cu): runs of gates that
+// fit a shared-memory tile of 2^fused_tile_bits amplitudes share one pass over the
+// state; other gates go through apply_single, in order.
+int fused_tile_bits(int dtype, uint32_t nq);
+bool fused_worthwhile(int dtype, uint32_t nq);
+void apply_fused(void *state, uint32_t nq, int dtype, const std::vector<GateDesc> &descs,
+                 const std::function<void(const GateDesc &)> &apply_single, cudaStream_t st);
 // Marginal probabilities over `bits` (bits[0] = MSB of the output index).
 template <typename R>
 void reduce_probs(const void *psi, uint32_t nq, const std::vector<uint32_t> &bits, double *partials,

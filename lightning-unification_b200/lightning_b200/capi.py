@@ -41,6 +41,18 @@ GENERATOR_IDS = {
 }
 
 
+MCMC_LOCAL, MCMC_NONZERO = 0, 1
+
+
+def mcmc_proposal_for_name(kernel_name: str) -> int:
+    """The proposal the reference runs for a transition-kernel name: generate_samples_metropolis
+    (LQ/measurements/MeasurementsLQubit.hpp:387-400) maps "NonZeroRandom" to
+    TransitionKernelType::NonZeroRandom and every other name to ::Local, and kernel_factory
+    (TransitionKernels.hpp:147-159) builds the non-zero kernel for ::Local and the local
+    kernel for ::NonZeroRandom."""
+    return MCMC_LOCAL if kernel_name == "NonZeroRandom" else MCMC_NONZERO
+
+
 class B200Error(RuntimeError):
     """Raised when a libb200sv call returns a non-zero status."""
 
@@ -114,6 +126,8 @@ _SIGS = {
                              C.POINTER(C.c_double)], C.c_int),
     "b200sv_inner_product": ([C.c_void_p, C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double)], C.c_int),
     "b200sv_norm2": ([C.c_void_p, C.POINTER(C.c_double)], C.c_int),
+    "b200sv_sample_mcmc": ([C.c_void_p, C.c_int, C.c_uint64, C.c_uint64, C.c_uint32, C.c_uint64,
+                            C.POINTER(C.c_uint64)], C.c_int),
     "b200sv_expval_sparse": ([C.c_void_p, C.POINTER(C.c_uint64), C.c_uint64, C.POINTER(C.c_uint64), C.c_void_p,
                               C.c_uint64, C.POINTER(C.c_double)], C.c_int),
     "b200sv_var_sparse": ([C.c_void_p, C.POINTER(C.c_uint64), C.c_uint64, C.POINTER(C.c_uint64), C.c_void_p,
@@ -440,6 +454,21 @@ class StateVector:
             u, up = _f64(uniforms)
         check(lib().b200sv_sample_bits(self.h, nshots, up, seed, out.ctypes.data_as(C.POINTER(C.c_uint64))))
         return out[:nshots * self.num_qubits].reshape(nshots, self.num_qubits)
+
+    def sample_mcmc(self, proposal: int, num_burnin: int, nshots: int, nchains: int = 4096, seed: int = 0):
+        """Basis indices from Metropolis chains (proposal MCMC_LOCAL or MCMC_NONZERO)."""
+        out = np.empty(max(1, nshots), dtype=np.uint64)
+        check(lib().b200sv_sample_mcmc(self.h, int(proposal), int(num_burnin), int(nshots), int(nchains), int(seed),
+                                       out.ctypes.data_as(C.POINTER(C.c_uint64))))
+        return out[:nshots]
+
+    def sample_mcmc_bits(self, kernel_name: str, num_burnin: int, nshots: int, nchains: int = 4096, seed: int = 0):
+        """generate_mcmc_samples: (nshots, n) bits, wire 0 first, with the reference's
+        kernel-name binding (its "Local" name runs the non-zero proposal)."""
+        idx = self.sample_mcmc(mcmc_proposal_for_name(kernel_name), num_burnin, nshots, nchains, seed)
+        n = self.num_qubits
+        shifts = np.arange(n - 1, -1, -1, dtype=np.uint64)
+        return ((idx[:, None] >> shifts[None, :]) & np.uint64(1)).astype(np.uint64)
 
     def vjp_state(self, ops, dy, trainable, apply_operations=False):
         ol = OpList(ops, self.np_dtype)

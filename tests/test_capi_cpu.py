@@ -86,6 +86,24 @@ def test_no_cpu_fallback_without_gpu():
         m.StateVectorC128(np.zeros(8, np.complex128))
 
 
+def test_device_shim_without_gpu():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    from lightning_b200 import capi, device
+    with pytest.raises(capi.B200Error, match="no CUDA device"):
+        device.LightningQubit(3)
+    with pytest.raises(NotImplementedError, match="only 'Local' and 'NonZeroRandom'"):
+        device.LightningQubit(3, shots=1000, mcmc=True, kernel_name="Global")
+    with pytest.raises(ValueError, match="Shots should be greater than num_burnin"):
+        device.LightningQubit(3, shots=10, mcmc=True, num_burnin=100)
+    tape = device.Tape([device.Operation("RX", [0], [0.1]), device.Operation("Rot", [1], [1, 2, 3]),
+                        device.Operation("CNOT", [0, 1])], trainable_params=[3, 1])
+    assert tape.num_params == 4
+    assert tape.get_operation(0)[0].name == "Rot" and tape.get_operation(0)[2] == 0
+    assert tape.get_operation(1)[0].name == "Rot" and tape.get_operation(1)[2] == 2
+
+
 def test_oplist_packing():
     from lightning_b200 import capi
     ops = [("RX", [0], False, [0.5]), ("CNOT", [1, 2], True, []),

@@ -191,3 +191,66 @@ def test_sparse_rejects_bad_csr(capi):
     with pytest.raises(capi.B200Error, match="more non-zeros"):
         sv.expval_sparse(rows, np.zeros(3, dtype=np.uint64), np.ones(3))
     assert sv.expval_sparse(np.zeros(5, dtype=np.uint64), np.zeros(0, dtype=np.uint64), np.zeros(0)) == 0.0
+
+
+@pytest.mark.parametrize("dtype", [np.complex128, np.complex64])
+@pytest.mark.parametrize("proposal", [0, 1])
+@pytest.mark.parametrize("n,burnin,shots,chains", [(1, 0, 50, 1), (3, 13, 640, 7), (8, 50, 3000, 64),
+                                                   (11, 5, 5000, 4096)])
+def test_mcmc_bit_exact(capi, dtype, proposal, n, burnin, shots, chains):
+    """Metropolis chains: the same indices as the oracle's restatement for the same seed."""
+    import lq_oracle as O
+    rng = np.random.default_rng(n + 10 * proposal)
+    st = random_state(rng, n, np.complex128)
+    st[rng.integers(0, 1 << n, size=max(1, (1 << n) // 4))] = 0  # zero-probability states
+    st /= np.linalg.norm(st)
+    st = st.astype(dtype)
+    sv = capi.StateVector(n, dtype)
+    sv.upload(st)
+    got = sv.sample_mcmc(proposal, burnin, shots, chains, seed=1234 + n)
+    want = O.mcmc_chains(st, proposal, burnin, shots, chains, seed=1234 + n)
+    assert np.array_equal(got, want)
+
+
+def test_mcmc_distribution_and_errors(capi):
+    import lq_oracle as O
+    rng = np.random.default_rng(2)
+    n = 10
+    st = random_state(rng, n)
+    sv = capi.StateVector(n)
+    sv.upload(st)
+    p = O.probs(st)
+    for proposal in (0, 1):
+        # one sample per chain after burn-in: independent draws, so chi^2 needs no
+        # correction for the correlation between consecutive steps of a chain
+        idx = sv.sample_mcmc(proposal, 300, 200000, 200000, seed=5)
+        counts = np.bincount(idx.astype(np.int64), minlength=1 << n)
+        # coarse bins over the top 5 qubits: chi^2 per degree of freedom near 1
+        c5 = counts.reshape(32, -1).sum(1)
+        p5 = p.reshape(32, -1).sum(1) * len(idx)
+        chi2 = ((c5 - p5) ** 2 / p5).sum() / 31
+        assert chi2 < 3.0, (proposal, chi2)
+    z = capi.StateVector(3)
+    z.upload(np.zeros(8))
+    with pytest.raises(capi.B200Error, match="no basis state has a non-zero amplitude"):
+        z.sample_mcmc(1, 10, 100)
+    with pytest.raises(capi.B200Error, match="chains must be positive"):
+        sv.sample_mcmc(0, 10, 100, 0)
+
+
+@pytest.mark.parametrize("kernel", ["Local", "NonZeroRandom"])
+def test_mcmc_reference_golden(kernel):
+    """Test_MeasurementsLQubit.cpp:199-320 through the module surface
+    (generate_mcmc_samples(num_wires, kernelname, num_burnin, num_shots))."""
+    import lightning_b200.lightning_qubit_ops as m
+    st = np.zeros(8, dtype=np.complex128)
+    st[0] = 1
+    sv = m.StateVectorC128(st)
+    for op in nontrivial_state_ops():
+        getattr(sv, op[0])(op[1], False, op[3])
+    bits = np.asarray(m.MeasurementsC128(sv).generate_mcmc_samples(3, kernel, 1000, 100000))
+    assert bits.shape == (100000, 3)
+    idx = bits[:, 0] * 4 + bits[:, 1] * 2 + bits[:, 2]
+    got = np.bincount(idx, minlength=8) / 100000
+    want = [0.67078706, 0.03062806, 0.0870997, 0.00397696, 0.17564072, 0.00801973, 0.02280642, 0.00104134]
+    assert np.abs(got - want).max() < 0.05

@@ -252,3 +252,44 @@ def test_sparse_matches_live_reference(ref_module):
         csr = random_csr(n, rng)
         assert abs(O.sparse_expval(st, *csr) - ref.sparse_expval(ref_module, st, *csr)) < 1e-12
         assert abs(O.sparse_var(st, *csr) - ref.sparse_var(ref_module, st, *csr)) < 1e-12
+
+
+@pytest.mark.parametrize("proposal", [O.MCMC_LOCAL, O.MCMC_NONZERO])
+def test_mcmc_chains_match_reference_histogram(proposal):
+    """LQ/measurements/tests/Test_MeasurementsLQubit.cpp:199-320: 10^5 Metropolis samples
+    after 1000 burn-in steps on the non-trivial state reproduce its probabilities within 0.05."""
+    st = nontrivial_state()
+    want = [0.67078706, 0.03062806, 0.0870997, 0.00397696, 0.17564072, 0.00801973, 0.02280642, 0.00104134]
+    idx = O.mcmc_chains(st, proposal, 1000, 100000, 256, seed=3)
+    got = np.bincount(idx.astype(np.int64), minlength=8) / 100000
+    assert np.abs(got - want).max() < 0.05
+    assert np.abs(got - O.probs(st)).max() < 0.01
+
+
+def test_mcmc_kernel_name_binding():
+    """kernel_factory (TransitionKernels.hpp:147-159) builds the non-zero kernel for the name
+    "Local" and the local kernel for "NonZeroRandom"."""
+    assert O.mcmc_kernel_for_name("Local") == O.MCMC_NONZERO
+    assert O.mcmc_kernel_for_name("NonZeroRandom") == O.MCMC_LOCAL
+    assert O.mcmc_kernel_for_name("anything") == O.MCMC_NONZERO
+
+
+def test_mcmc_local_chain_stays_in_support():
+    """From |0...0>, local moves to zero-probability states are never accepted (p_t = 0 < U p_i)."""
+    st = np.zeros(16, dtype=np.complex128)
+    st[0] = st[5] = 1 / np.sqrt(2)
+    idx = O.mcmc_chains(st, O.MCMC_LOCAL, 10, 500, 5, seed=9)
+    assert set(idx.tolist()) <= {0}
+    idx = O.mcmc_chains(st, O.MCMC_NONZERO, 10, 2000, 5, seed=9)
+    assert set(idx.tolist()) == {0, 5}
+
+
+def test_mcmc_reference_module_histogram(ref_module):
+    """The reference's own generate_mcmc_samples (unseeded) gives the same distribution."""
+    st = nontrivial_state()
+    for name in ("Local", "NonZeroRandom"):
+        sv = ref_module.StateVectorC128(st.copy())
+        bits = np.asarray(ref_module.MeasurementsC128(sv).generate_mcmc_samples(3, name, 1000, 50000))
+        idx = bits[:, 0] * 4 + bits[:, 1] * 2 + bits[:, 2]
+        got = np.bincount(idx, minlength=8) / 50000
+        assert np.abs(got - O.probs(st)).max() < 0.02, name
