@@ -158,13 +158,16 @@ __global__ void k_trig(const double *__restrict__ params, uint64_t n, double4 *_
 }
 
 // Coefficients of a gate (or of its adjoint): MAT1 -> 4, MAT2 -> 16, DIAG -> 2^nt, PARITY -> 2.
-template <typename R>
+// NM: 16 for two-wire dense steps (F_MAT2), 4 for every other form; an array of exactly
+// that size keeps the coefficients of the common steps in few registers.
+template <typename R, int NM>
 __device__ __forceinline__ void op_coeffs(const DOp &op, const double4 *__restrict__ cs,
-                                          const double2 *__restrict__ consts, bool adj, C<R> *m) {
+                                          const double2 *__restrict__ consts, bool adj, C<R> (&m)[NM]) {
     if (op.gate == kConstGate) {
         const double2 *c = consts + (size_t)op.cidx * 16;
-        if (op.form == F_MAT1 || op.form == F_MAT2) {
-            const int D = op.form == F_MAT1 ? 2 : 4;
+        // NM == 4: D is 2 at compile time; NM == 16 serves every form (D chosen at run time)
+        const int D = (NM == 16 && op.form == F_MAT2) ? 4 : 2;
+        if (op.form == F_MAT1 || (NM == 16 && op.form == F_MAT2)) {
             for (int r = 0; r < D; ++r)
                 for (int q = 0; q < D; ++q) {
                     const double2 z = adj ? c[q * D + r] : c[r * D + q];
@@ -190,26 +193,29 @@ __device__ __forceinline__ void op_coeffs(const DOp &op, const double4 *__restri
     case B200SV_IsingZZ:
         m[0] = mk<R>(cr, -sr); m[1] = mk<R>(cr, sr); m[2] = mk<R>(cr, sr); m[3] = mk<R>(cr, -sr); break;
     default: {
-        for (int i = 0; i < 16; ++i) m[i] = mk<R>(z, z);
-        if (op.gate == B200SV_IsingXX) {
-            m[0] = m[5] = m[10] = m[15] = mk<R>(cr, z);
-            m[3] = m[6] = m[9] = m[12] = mk<R>(z, -sr);
-        } else if (op.gate == B200SV_IsingYY) {
-            m[0] = m[5] = m[10] = m[15] = mk<R>(cr, z);
-            m[3] = m[12] = mk<R>(z, sr);
-            m[6] = m[9] = mk<R>(z, -sr);
-        } else if (op.gate == B200SV_IsingXY) {
-            m[0] = m[15] = mk<R>(one, z);
-            m[5] = m[10] = mk<R>(cr, z);
-            m[6] = m[9] = mk<R>(z, sr);
-        } else {  // SingleExcitation (+/-)
-            m[5] = m[10] = mk<R>(cr, z);
-            m[6] = mk<R>(-sr, z);
-            m[9] = mk<R>(sr, z);
-            C<R> e = mk<R>(one, z);
-            if (op.gate == B200SV_SingleExcitationMinus) e = mk<R>(cr, -sr);
-            if (op.gate == B200SV_SingleExcitationPlus) e = mk<R>(cr, sr);
-            m[0] = m[15] = e;
+        if constexpr (NM == 16) {  // two-wire dense gates (F_MAT2)
+#pragma unroll
+            for (int i = 0; i < NM; ++i) m[i] = mk<R>(z, z);
+            if (op.gate == B200SV_IsingXX) {
+                m[0] = m[5] = m[10] = m[15] = mk<R>(cr, z);
+                m[3] = m[6] = m[9] = m[12] = mk<R>(z, -sr);
+            } else if (op.gate == B200SV_IsingYY) {
+                m[0] = m[5] = m[10] = m[15] = mk<R>(cr, z);
+                m[3] = m[12] = mk<R>(z, sr);
+                m[6] = m[9] = mk<R>(z, -sr);
+            } else if (op.gate == B200SV_IsingXY) {
+                m[0] = m[15] = mk<R>(one, z);
+                m[5] = m[10] = mk<R>(cr, z);
+                m[6] = m[9] = mk<R>(z, sr);
+            } else {  // SingleExcitation (+/-)
+                m[5] = m[10] = mk<R>(cr, z);
+                m[6] = mk<R>(-sr, z);
+                m[9] = mk<R>(sr, z);
+                C<R> e = mk<R>(one, z);
+                if (op.gate == B200SV_SingleExcitationMinus) e = mk<R>(cr, -sr);
+                if (op.gate == B200SV_SingleExcitationPlus) e = mk<R>(cr, sr);
+                m[0] = m[15] = e;
+            }
         }
     }
     }
@@ -224,8 +230,8 @@ __device__ __forceinline__ void member_mat(const DOp &op, const double4 *__restr
         m[0] = zero; m[1] = one; m[2] = one; m[3] = zero;
         return;
     }
-    C<R> t[16];
-    op_coeffs<R>(op, cs, consts, adj, t);
+    C<R> t[4];
+    op_coeffs<R, 4>(op, cs, consts, adj, t);
     if (op.form == F_MAT1) {
         m[0] = t[0]; m[1] = t[1]; m[2] = t[2]; m[3] = t[3];
     } else if (op.nt == 1) {  // diagonal on the bit
@@ -256,14 +262,39 @@ __device__ __forceinline__ Range groups(int kt, int wl, int nb, bool wloc) {
     return r;
 }
 
-// apply one gate (coefficients already adjointed when needed) to NS tiles
+// two-wire dense step (F_MAT2) with its 16 coefficients
 template <typename R, int NS>
-__device__ __forceinline__ void apply_op(C<R> *const (&s)[NS], int kt, int wl, bool wloc, const DOp &op, const C<R> *m) {
+__device__ __forceinline__ void apply_mat2(C<R> *const (&s)[NS], int kt, int wl, bool wloc, const DOp &op,
+                                           const C<R> (&m)[16]) {
+    const Range rg = groups(kt, wl, op.nb, wloc);
+    for (uint32_t g = rg.g0; g < rg.g1; g += rg.gs) {
+        const uint32_t base = ins_local(g, op.low, op.nb) | op.cmask;
+#pragma unroll
+        for (int q = 0; q < NS; ++q) {
+            C<R> *t = s[q];
+            C<R> v[4];
+#pragma unroll
+            for (int r = 0; r < 4; ++r) v[r] = t[base + op.off[r]];
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+                CAcc<R> a;
+#pragma unroll
+                for (int c = 0; c < 4; ++c) a.add(m[r * 4 + c], v[c]);
+                t[base + op.off[r]] = a.get();
+            }
+        }
+    }
+}
+
+// apply one gate of any other form (coefficients already adjointed when needed) to NS tiles
+template <typename R, int NS>
+__device__ __forceinline__ void apply_op(C<R> *const (&s)[NS], int kt, int wl, bool wloc, const DOp &op,
+                                         const C<R> (&m)[4]) {
     if (op.form == F_NOOP) return;
     if (op.form == F_PARITY) {
         const Range rg = groups(kt, wl, 0, wloc);
         for (uint32_t i = rg.g0; i < rg.g1; i += rg.gs) {
-            const C<R> f = m[__popc(i & op.pmask) & 1];
+            const C<R> f = (__popc(i & op.pmask) & 1) ? m[1] : m[0];
 #pragma unroll
             for (int q = 0; q < NS; ++q) {
                 CAcc<R> a;
@@ -287,19 +318,6 @@ __device__ __forceinline__ void apply_op(C<R> *const (&s)[NS], int kt, int wl, b
                 b.add(m[2], v0); b.add(m[3], v1);
                 t[base + op.off[0]] = a.get();
                 t[base + op.off[1]] = b.get();
-                break;
-            }
-            case F_MAT2: {
-                C<R> v[4];
-#pragma unroll
-                for (int r = 0; r < 4; ++r) v[r] = t[base + op.off[r]];
-#pragma unroll
-                for (int r = 0; r < 4; ++r) {
-                    CAcc<R> a;
-#pragma unroll
-                    for (int c = 0; c < 4; ++c) a.add(m[r * 4 + c], v[c]);
-                    t[base + op.off[r]] = a.get();
-                }
                 break;
             }
             case F_DIAG: {
@@ -326,8 +344,63 @@ __device__ __forceinline__ void apply_op(C<R> *const (&s)[NS], int kt, int wl, b
     }
 }
 
+// apply a step of any form with coefficients in a 16-entry array (kernels built with the
+// two-wire dense paths); the parity phase is picked by index, as those kernels keep the
+// array in local memory anyway
+template <typename R, int NS>
+__device__ __forceinline__ void apply_op_general(C<R> *const (&s)[NS], int kt, int wl, bool wloc, const DOp &op,
+                                                 const C<R> (&m)[16]) {
+    if (op.form == F_MAT2) {
+        apply_mat2<R, NS>(s, kt, wl, wloc, op, m);
+        return;
+    }
+    if (op.form == F_PARITY) {
+        const Range rg = groups(kt, wl, 0, wloc);
+        for (uint32_t i = rg.g0; i < rg.g1; i += rg.gs) {
+            const C<R> f = m[__popc(i & op.pmask) & 1];
+#pragma unroll
+            for (int q = 0; q < NS; ++q) {
+                CAcc<R> a;
+                a.add(f, s[q][i]);
+                s[q][i] = a.get();
+            }
+        }
+        return;
+    }
+    const C<R>(&m4)[4] = reinterpret_cast<const C<R>(&)[4]>(m);
+    apply_op<R, NS>(s, kt, wl, wloc, op, m4);
+}
+
 // per-thread part of Im<bra|G|ket> on one tile, FP64
-template <typename R>
+// sum over groups of Im(conj(bra) . G ket) for a 2^K x 2^K generator G (FP64)
+template <typename R, int K>
+__device__ __forceinline__ double gen_inner_k(const C<R> *bra, const C<R> *ket, const Range &rg, const DOp &op,
+                                              const double2 *__restrict__ G) {
+    constexpr int D = 1 << K;
+    double acc = 0.0;
+    for (uint32_t g = rg.g0; g < rg.g1; g += rg.gs) {
+        const uint32_t base = ins_local(g, op.glow, op.gnb);
+        double2 v[D];
+#pragma unroll
+        for (int r = 0; r < D; ++r) v[r] = widen<R>(ket[base + op.goff[r]]);
+#pragma unroll
+        for (int r = 0; r < D; ++r) {
+            double wr = 0, wi = 0;
+#pragma unroll
+            for (int c = 0; c < D; ++c) {
+                const double2 x = G[r * D + c];
+                wr += x.x * v[c].x - x.y * v[c].y;
+                wi += x.x * v[c].y + x.y * v[c].x;
+            }
+            const double2 b = widen<R>(bra[base + op.goff[r]]);
+            acc += b.x * wi - b.y * wr;
+        }
+    }
+    return acc;
+}
+
+// FULL: the batch holds two-wire dense steps or generators (compiled only into the full kernel)
+template <typename R, bool FULL>
 __device__ __forceinline__ double gen_inner(const C<R> *bra, const C<R> *ket, int kt, int wl, bool wloc, const DOp &op,
                                             const double2 *__restrict__ consts) {
     double acc = 0.0;
@@ -341,24 +414,28 @@ __device__ __forceinline__ double gen_inner(const C<R> *bra, const C<R> *ket, in
         return acc;
     }
     const double2 *G = consts + (size_t)op.gcidx * 16;
-    const int D = 1 << op.gk;
     const Range rg = groups(kt, wl, op.gnb, wloc);
-    for (uint32_t g = rg.g0; g < rg.g1; g += rg.gs) {
-        const uint32_t base = ins_local(g, op.glow, op.gnb);
-        double2 v[4];
-        for (int r = 0; r < D; ++r) v[r] = widen<R>(ket[base + op.goff[r]]);
-        for (int r = 0; r < D; ++r) {
-            double wr = 0, wi = 0;
-            for (int c = 0; c < D; ++c) {
-                const double2 x = G[r * D + c];
-                wr += x.x * v[c].x - x.y * v[c].y;
-                wi += x.x * v[c].y + x.y * v[c].x;
+    if constexpr (FULL) {
+        // general size (one or two wires), loops over the run-time size
+        const int D = 1 << op.gk;
+        for (uint32_t g = rg.g0; g < rg.g1; g += rg.gs) {
+            const uint32_t base = ins_local(g, op.glow, op.gnb);
+            double2 v[4];
+            for (int r = 0; r < D; ++r) v[r] = widen<R>(ket[base + op.goff[r]]);
+            for (int r = 0; r < D; ++r) {
+                double wr = 0, wi = 0;
+                for (int c = 0; c < D; ++c) {
+                    const double2 x = G[r * D + c];
+                    wr += x.x * v[c].x - x.y * v[c].y;
+                    wi += x.x * v[c].y + x.y * v[c].x;
+                }
+                const double2 b = widen<R>(bra[base + op.goff[r]]);
+                acc += b.x * wi - b.y * wr;
             }
-            const double2 b = widen<R>(bra[base + op.goff[r]]);
-            acc += b.x * wi - b.y * wr;
         }
+        return acc;
     }
-    return acc;
+    return gen_inner_k<R, 1>(bra, ket, rg, op, G);
 }
 
 __device__ __forceinline__ void add_grad(double *gradw, int32_t gslot, double p, bool first) {
@@ -495,7 +572,9 @@ __device__ void expval_terms(const C<R> *psi, uint64_t n_amp, const DTerm *__res
             }
             a += (__popcll(i & tm.zmask) & 1) ? -r : r;
         }
-        acc[tm.obs] += tm.coeff * a;
+#pragma unroll
+        for (int o = 0; o < kMaxObsPerCircuit; ++o)  // constant indices keep acc in registers
+            if (o == (int)tm.obs) acc[o] += tm.coeff * a;
     }
 }
 
@@ -540,7 +619,6 @@ struct KArgs {
     double *gradw;        // VJP: [ngslots * nwarps]
     void *pool_a, *pool_b;
     const int *reuse;     // VJP: nonzero when pool A still holds this step's forward states
-    int mode;             // 0 forward, 1 vjp
     int max_kt;
 };
 
@@ -586,10 +664,9 @@ __device__ void store_tile(C<R> *__restrict__ dst, const C<R> *src, const DSeg &
 
 // Apply the gates of one segment to the tile(s): forward (NS = 1) or the adjoint
 // sweep over (lambda, bra) with gradient products (NS = 2, REV).
-template <typename R, int NS, bool REV>
+template <typename R, int NS, bool REV, bool FULL>
 __device__ void exec_segment(const KArgs &A, C<R> *const (&tiles)[NS], int kt, const DSeg &sg, bool first_tile) {
     const int wl = kt - (31 - __clz((int)(blockDim.x >> 5)));  // bits owned by one warp's block
-    C<R> m[16];
     bool prev_wloc = false;
     int o = REV ? (int)sg.nops - 1 : 0;
     while (REV ? o >= 0 : o < (int)sg.nops) {
@@ -617,13 +694,20 @@ __device__ void exec_segment(const KArgs &A, C<R> *const (&tiles)[NS], int kt, c
         } else {
             const DOp op = *op0;
             if (REV && op.gslot >= 0) {
-                add_grad(A.gradw, op.gslot, gen_inner<R>(tiles[NS - 1], tiles[0], kt, wl, wloc, op, A.consts),
+                add_grad(A.gradw, op.gslot, gen_inner<R, FULL>(tiles[NS - 1], tiles[0], kt, wl, wloc, op, A.consts),
                          first_tile);
                 if (wloc) __syncwarp();
                 else __syncthreads();
             }
-            op_coeffs<R>(op, A.cs, A.consts, REV, m);
-            apply_op<R, NS>(tiles, kt, wl, wloc, op, m);
+            if constexpr (FULL) {
+                C<R> m[16];
+                op_coeffs<R, 16>(op, A.cs, A.consts, REV, m);
+                apply_op_general<R, NS>(tiles, kt, wl, wloc, op, m);
+            } else {
+                C<R> m[4];
+                op_coeffs<R, 4>(op, A.cs, A.consts, REV, m);
+                apply_op<R, NS>(tiles, kt, wl, wloc, op, m);
+            }
         }
         prev_wloc = wloc;
         o = REV ? head - 1 : head + len;
@@ -632,7 +716,7 @@ __device__ void exec_segment(const KArgs &A, C<R> *const (&tiles)[NS], int kt, c
 }
 
 // one circuit, forward: state ends in tile 0 (resident) or pool A (global)
-template <typename R>
+template <typename R, bool FULL>
 __device__ void run_forward(const KArgs &A, const DCirc &c, C<R> *sm, C<R> *pa) {
     const uint32_t tn = 1u << c.kt;
     C<R> *tiles[1] = {sm};
@@ -640,7 +724,7 @@ __device__ void run_forward(const KArgs &A, const DCirc &c, C<R> *sm, C<R> *pa) 
         zero_tile<R>(sm, tn);
         __syncthreads();
         if (threadIdx.x == 0) sm[0] = mk<R>(1, 0);
-        exec_segment<R, 1, false>(A, tiles, c.kt, A.segs[c.seg_begin], true);
+        exec_segment<R, 1, false, FULL>(A, tiles, c.kt, A.segs[c.seg_begin], true);
         return;
     }
     const uint64_t ntiles = uint64_t(1) << (c.n - c.kt);
@@ -655,14 +739,17 @@ __device__ void run_forward(const KArgs &A, const DCirc &c, C<R> *sm, C<R> *pa) 
             } else {
                 load_tile<R>(sm, pa, sg, tbase, tn);
             }
-            exec_segment<R, 1, false>(A, tiles, c.kt, sg, true);
+            exec_segment<R, 1, false, FULL>(A, tiles, c.kt, sg, true);
             store_tile<R>(pa, sm, sg, tbase, tn);
             __syncthreads();
         }
     }
 }
 
-template <typename R>
+// MODE 0: forward expectation values; MODE 1: forward (unless reused) and the VJP sweep.
+// FULL: compiled with the two-wire dense step and generator paths (only batches that
+// hold such gates launch it; the others get a kernel without them, in fewer registers).
+template <typename R, int MODE, bool FULL>
 __global__ void __launch_bounds__(512) k_batch(KArgs A) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ uint32_t s_next;
@@ -679,17 +766,20 @@ __global__ void __launch_bounds__(512) k_batch(KArgs A) {
         C<R> *pa = static_cast<C<R> *>(A.pool_a) + c.off_a;
         C<R> *pb = static_cast<C<R> *>(A.pool_b) + c.off_b;
         const uint64_t namp = uint64_t(1) << c.n;
-        const bool reuse = A.mode == 1 && !c.resident && A.reuse && *A.reuse != 0;
-        if (!reuse) run_forward<R>(A, c, sm0, pa);
+        const bool reuse = MODE == 1 && !c.resident && A.reuse && *A.reuse != 0;
+        if (!reuse) run_forward<R, FULL>(A, c, sm0, pa);
         const C<R> *psi = c.resident ? sm0 : pa;
-        if (A.mode == 0) {
+        if (MODE == 0) {
             double acc[kMaxObsPerCircuit];
 #pragma unroll
             for (int o = 0; o < kMaxObsPerCircuit; ++o) acc[o] = 0.0;
             expval_terms<R>(psi, namp, A.terms + c.term_begin, c.nterms, acc);
             block_reduce<kMaxObsPerCircuit>(acc, s_red);
-            if (threadIdx.x == 0)
-                for (uint32_t o = 0; o < c.nobs; ++o) A.out[c.out_begin + o] = acc[o];
+            if (threadIdx.x == 0) {
+#pragma unroll
+                for (int o = 0; o < kMaxObsPerCircuit; ++o)
+                    if (o < (int)c.nobs) A.out[c.out_begin + o] = acc[o];
+            }
             __syncthreads();
             continue;
         }
@@ -699,7 +789,7 @@ __global__ void __launch_bounds__(512) k_batch(KArgs A) {
         __syncthreads();
         C<R> *tiles[2] = {sm0, sm1};
         if (c.resident) {
-            exec_segment<R, 2, true>(A, tiles, c.kt, A.segs[c.seg_begin], true);
+            exec_segment<R, 2, true, FULL>(A, tiles, c.kt, A.segs[c.seg_begin], true);
             continue;
         }
         const uint64_t ntiles = uint64_t(1) << (c.n - c.kt);
@@ -710,7 +800,7 @@ __global__ void __launch_bounds__(512) k_batch(KArgs A) {
                 const uint64_t tbase = insert_zeros64(t, sg.lbits, sg.nl);
                 load_tile<R>(sm0, pa, sg, tbase, tn);
                 load_tile<R>(sm1, pb, sg, tbase, tn);
-                exec_segment<R, 2, true>(A, tiles, c.kt, sg, t == 0);
+                exec_segment<R, 2, true, FULL>(A, tiles, c.kt, sg, t == 0);
                 store_tile<R>(pa, sm0, sg, tbase, tn);
                 store_tile<R>(pb, sm1, sg, tbase, tn);
                 __syncthreads();
@@ -790,6 +880,7 @@ struct Batch {
     uint32_t ncirc = 0;
     Config cfg;
     bool use_graphs = false;
+    bool full = false;  // the program holds two-wire dense steps or generators
     uint32_t last_launches = 0;
 
     // circuit descriptions kept for re-planning
@@ -1251,6 +1342,14 @@ Planned plan(const Batch &B, const Config &cfg, bool vjp) {
     return P;
 }
 
+template <typename R> const void *batch_kernel_r(int mode, bool full) {
+    if (full) return mode ? (const void *)k_batch<R, 1, true> : (const void *)k_batch<R, 0, true>;
+    return mode ? (const void *)k_batch<R, 1, false> : (const void *)k_batch<R, 0, false>;
+}
+const void *batch_kernel(int dtype, int mode, bool full) {
+    return dtype == B200SV_C64 ? batch_kernel_r<float>(mode, full) : batch_kernel_r<double>(mode, full);
+}
+
 template <typename T> void upload(Batch &B, T *&dst, const std::vector<T> &src) {
     dst = B.dalloc<T>(src.size());
     if (!src.empty())
@@ -1324,15 +1423,17 @@ void build_program(Batch &B, const Config &cfg) {
     const size_t static_smem = kMaxObsPerCircuit * 32 * 8 + 2 * 16 * 16 + 64;
     if (B.smem_bytes + static_smem > (size_t)maxsm)
         throw Unsupported("batch: tile does not fit in shared memory; lower kt");
-    if (B.dtype == B200SV_C64)
-        B200SV_CUDA(cudaFuncSetAttribute(k_batch<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)B.smem_bytes));
-    else
-        B200SV_CUDA(cudaFuncSetAttribute(k_batch<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)B.smem_bytes));
-    int per_sm = 0;
-    if (B.dtype == B200SV_C64)
-        B200SV_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch<float>, cfg.threads, B.smem_bytes));
-    else
-        B200SV_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch<double>, cfg.threads, B.smem_bytes));
+    B.full = false;
+    for (const DOp &d : P.ops)
+        if (d.form == F_MAT2 || (d.gform == G_MAT && d.gk == 2)) B.full = true;
+    int per_sm = 1 << 30;
+    for (int mode = 0; mode < 2; ++mode) {
+        const void *k = batch_kernel(B.dtype, mode, B.full);
+        B200SV_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)B.smem_bytes));
+        int m = 0;
+        B200SV_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&m, k, cfg.threads, B.smem_bytes));
+        per_sm = std::min(per_sm, m);
+    }
     if (per_sm < 1) throw Unsupported("batch: launch configuration does not fit on an SM");
     B.grid = std::max(1, std::min<int>((int)B.ncirc, nsm * per_sm));
     B200SV_CUDA(cudaDeviceSynchronize());
@@ -1363,14 +1464,13 @@ void launch_main(Batch &B, int mode, const double *dy, double *out, const int *r
     A.pool_a = B.d_pool_a;
     A.pool_b = B.d_pool_b;
     A.reuse = reuse;
-    A.mode = mode;
     int mk = 1;
     for (auto &c : B.h_circs) mk = std::max<int>(mk, (int)c.kt);
     A.max_kt = mk;
     B200SV_CUDA(cudaMemsetAsync(B.d_counter, 0, sizeof(uint32_t), st));
-    if (B.dtype == B200SV_C64) k_batch<float><<<B.grid, B.cfg.threads, B.smem_bytes, st>>>(A);
-    else k_batch<double><<<B.grid, B.cfg.threads, B.smem_bytes, st>>>(A);
-    B200SV_CUDA(cudaGetLastError());
+    void *args[] = {&A};
+    B200SV_CUDA(cudaLaunchKernel(batch_kernel(B.dtype, mode, B.full), dim3(B.grid), dim3(B.cfg.threads), args,
+                                 B.smem_bytes, st));
 }
 
 // Forward: expectation values; the final states of circuits wider than a tile stay
