@@ -240,6 +240,13 @@ def run_case(args):
         print(json.dumps({"case": "gate", "kernel": "k_dense<double,1>", "qubits": args.qubits, "ms": ms,
                           "gbs": gbs}))
         return
+    if args.case == "precision":
+        res = {"case": "precision",
+               "c64_33q": precision_case(33, np.complex64),
+               "c128_32q": precision_case(32, np.complex128),
+               "c64_vs_c128_32q": precision_compare(32)}
+        print(json.dumps(res))
+        return
     if args.case == "fused":
         from lightning_b200.workloads import gate_sweep, random_state
         ops = gate_sweep(args.qubits, 200, seed=7)
@@ -334,6 +341,70 @@ def sampling_case(nq: int, shots: int = 10_000_000):
             "chi2_per_dof": chi2 / max(dof, 1)}
 
 
+def precision_case(nq: int, dtype, shots: int = 10_000_000):
+    """Full-size precision and sampling run: RY layer + QFT ladder (fused) on an nq-qubit
+    state, probs over every wire into device memory (2^nq doubles), then `shots` samples by
+    the fixed-order inverse CDF.  Size-independent checks: |norm^2 - 1|, |sum(probs) - 1|,
+    chi-squared of the sampled top-10-wire marginal."""
+    import torch
+    from lightning_b200 import capi
+    from lightning_b200.workloads import qft_circuit
+    sv = capi.StateVector(nq, dtype)
+    st = torch.cuda.current_stream()
+    sv.set_stream(st.cuda_stream)
+    ops = qft_circuit(nq, seed=9)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    sv.apply_ops_fused(ops)
+    e1.record(st)
+    torch.cuda.synchronize()
+    t_gates = e0.elapsed_time(e1) / 1e3
+    norm_err = abs(sv.norm2() - 1.0)
+    probs = torch.empty(1 << nq, dtype=torch.float64, device="cuda")
+    e0.record(st)
+    sv.probs_device(probs.data_ptr())
+    e1.record(st)
+    torch.cuda.synchronize()
+    t_probs = e0.elapsed_time(e1) / 1e3
+    psum_err = abs(float(probs.sum().item()) - 1.0)
+    del probs
+    torch.cuda.empty_cache()
+    t0 = time.perf_counter()
+    idx = sv.sample(shots, seed=2024)
+    t_sample = time.perf_counter() - t0
+    k = 10
+    marg = sv.probs(list(range(k)))
+    hist = np.bincount((idx >> np.uint64(nq - k)).astype(np.int64), minlength=1 << k)
+    expct = marg * shots
+    mask = expct > 5
+    chi2 = float(((hist[mask] - expct[mask]) ** 2 / expct[mask]).sum())
+    dof = int(mask.sum()) - 1
+    amp = np.dtype(dtype).itemsize
+    sv.close()
+    return {"qubits": nq, "dtype": "c64" if np.dtype(dtype) == np.complex64 else "c128",
+            "state_gib": (amp << nq) / 2**30, "gates": len(ops), "gates_fused_s": t_gates,
+            "norm2_err": norm_err, "probs_s": t_probs, "probs_gbs": ((amp + 8) << nq) / t_probs / 1e9,
+            "probs_sum_err": psum_err, "shots": shots, "sample_s": t_sample, "shots_per_s": shots / t_sample,
+            "chi2_per_dof": chi2 / max(dof, 1), "chi2_dof": dof}
+
+
+def precision_compare(nq: int = 32, k: int = 16):
+    """complex64 vs complex128 on the same nq-qubit circuit: max |difference| of the top-k-wire
+    marginal probabilities (the complex128 path is pinned to the FP64 oracle at small sizes)."""
+    from lightning_b200 import capi
+    from lightning_b200.workloads import qft_circuit
+    ops = qft_circuit(nq, seed=9)
+    out = {}
+    for dt in (np.complex128, np.complex64):
+        sv = capi.StateVector(nq, dt)
+        sv.apply_ops_fused(ops)
+        out[np.dtype(dt).name] = sv.probs(list(range(k)))
+        sv.close()
+    return {"qubits": nq, "marginal_wires": k,
+            "max_abs_diff_c64_vs_c128": float(np.abs(out["complex64"] - out["complex128"]).max())}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -342,7 +413,7 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--sweep-qubits", type=int, default=30)
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--case", default="full", choices=["full", "gate", "batch", "fused"],
+    ap.add_argument("--case", default="full", choices=["full", "gate", "batch", "fused", "precision"],
                     help="gate / batch: one kernel family on a small case (profiling)")
     ap.add_argument("--qubits", type=int, default=28, help="--case gate: state width (complex128)")
     ap.add_argument("--ncirc", type=int, default=148, help="--case batch: number of circuits")

@@ -66,6 +66,8 @@ struct DSeg {
     uint8_t nl, ng;
 };
 
+static_assert(sizeof(DSeg) % 4 == 0, "segments are staged in shared memory as 32-bit words");
+
 struct DCirc {
     uint32_t n, kt, resident;
     uint32_t seg_begin, nseg;
@@ -715,9 +717,19 @@ __device__ void exec_segment(const KArgs &A, C<R> *const (&tiles)[NS], int kt, c
     __syncthreads();
 }
 
+// Stage segment `idx` in shared memory: its bit tables are indexed by loop variables in the
+// tile moves, which would put a register copy of the record in local memory.
+__device__ __forceinline__ const DSeg &stage_segment(DSeg *s_seg, const DSeg *segs, uint32_t idx) {
+    __syncthreads();
+    if (threadIdx.x < sizeof(DSeg) / 4)
+        reinterpret_cast<uint32_t *>(s_seg)[threadIdx.x] = reinterpret_cast<const uint32_t *>(segs + idx)[threadIdx.x];
+    __syncthreads();
+    return *s_seg;
+}
+
 // one circuit, forward: state ends in tile 0 (resident) or pool A (global)
 template <typename R, bool FULL>
-__device__ void run_forward(const KArgs &A, const DCirc &c, C<R> *sm, C<R> *pa) {
+__device__ void run_forward(const KArgs &A, const DCirc &c, C<R> *sm, C<R> *pa, DSeg *s_seg) {
     const uint32_t tn = 1u << c.kt;
     C<R> *tiles[1] = {sm};
     if (c.resident) {
@@ -729,7 +741,7 @@ __device__ void run_forward(const KArgs &A, const DCirc &c, C<R> *sm, C<R> *pa) 
     }
     const uint64_t ntiles = uint64_t(1) << (c.n - c.kt);
     for (uint32_t si = 0; si < c.nseg; ++si) {
-        const DSeg sg = A.segs[c.seg_begin + si];
+        const DSeg &sg = stage_segment(s_seg, A.segs, c.seg_begin + si);
         for (uint64_t t = 0; t < ntiles; ++t) {
             const uint64_t tbase = insert_zeros64(t, sg.lbits, sg.nl);
             if (si == 0) {
@@ -754,6 +766,7 @@ __global__ void __launch_bounds__(512) k_batch(KArgs A) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ uint32_t s_next;
     __shared__ double s_red[kMaxObsPerCircuit * 32];
+    __shared__ __align__(8) DSeg s_seg;
     C<R> *sm0 = reinterpret_cast<C<R> *>(smem_raw);
     C<R> *sm1 = sm0 + (size_t(1) << A.max_kt);
     for (;;) {
@@ -767,7 +780,7 @@ __global__ void __launch_bounds__(512) k_batch(KArgs A) {
         C<R> *pb = static_cast<C<R> *>(A.pool_b) + c.off_b;
         const uint64_t namp = uint64_t(1) << c.n;
         const bool reuse = MODE == 1 && !c.resident && A.reuse && *A.reuse != 0;
-        if (!reuse) run_forward<R, FULL>(A, c, sm0, pa);
+        if (!reuse) run_forward<R, FULL>(A, c, sm0, pa, &s_seg);
         const C<R> *psi = c.resident ? sm0 : pa;
         if (MODE == 0) {
             double acc[kMaxObsPerCircuit];
@@ -795,7 +808,7 @@ __global__ void __launch_bounds__(512) k_batch(KArgs A) {
         const uint64_t ntiles = uint64_t(1) << (c.n - c.kt);
         const uint32_t tn = 1u << c.kt;
         for (int32_t si = (int32_t)c.nseg - 1; si >= 0; --si) {
-            const DSeg sg = A.segs[c.seg_begin + si];
+            const DSeg &sg = stage_segment(&s_seg, A.segs, c.seg_begin + si);
             for (uint64_t t = 0; t < ntiles; ++t) {
                 const uint64_t tbase = insert_zeros64(t, sg.lbits, sg.nl);
                 load_tile<R>(sm0, pa, sg, tbase, tn);

@@ -433,6 +433,11 @@ class StateVector:
         check(lib().b200sv_inner_product(self.h, ket.h, C.byref(re), C.byref(im)))
         return complex(re.value, im.value)
 
+    def probs_device(self, out_ptr: int, wires=None):
+        """probs(wires) into a caller-owned device buffer of 2^len(wires) doubles (all wires when None)."""
+        w, wp = _u32([] if wires is None else wires)
+        check(lib().b200sv_probs_device(self.h, wp, len(w), C.c_void_p(out_ptr)))
+
     def norm2(self) -> float:
         r = C.c_double()
         check(lib().b200sv_norm2(self.h, C.byref(r)))
