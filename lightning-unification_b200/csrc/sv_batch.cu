@@ -99,41 +99,44 @@ template <typename R> __device__ __forceinline__ R dot2r(R a, R x, R b, R y) {
     return fma(a, x, w) + e;
 }
 
-// Apply a single-wire matrix m (given its structure) to the pair (v0, v1) in place.
-template <typename R> __device__ __forceinline__ void apply_pair(int kind, const C<R> (&m)[4], C<R> &v0, C<R> &v1) {
-    switch (kind) {
-    case MK_DIAG:
+// Apply a single-wire matrix m with structure KIND to the pair (v0, v1) in place.
+template <typename R, int KIND>
+__device__ __forceinline__ void apply_pair_k(const C<R> (&m)[4], C<R> &v0, C<R> &v1) {
+    if constexpr (KIND == MK_DIAG) {
         v0 = cmul1<R>(m[0], v0);
         v1 = cmul1<R>(m[3], v1);
-        break;
-    case MK_PHASE1:
+    } else if constexpr (KIND == MK_PHASE1) {
         v1 = cmul1<R>(m[3], v1);
-        break;
-    case MK_SWAP: {
+    } else if constexpr (KIND == MK_SWAP) {
         const C<R> t = v0;
         v0 = v1;
         v1 = t;
-        break;
-    }
-    case MK_REAL: {  // m real
+    } else if constexpr (KIND == MK_REAL) {  // m real
         const C<R> a = v0, b = v1;
         v0 = mk<R>(dot2r<R>(m[0].x, a.x, m[1].x, b.x), dot2r<R>(m[0].x, a.y, m[1].x, b.y));
         v1 = mk<R>(dot2r<R>(m[2].x, a.x, m[3].x, b.x), dot2r<R>(m[2].x, a.y, m[3].x, b.y));
-        break;
-    }
-    case MK_RX: {  // real diagonal, imaginary off-diagonal
+    } else if constexpr (KIND == MK_RX) {  // real diagonal, imaginary off-diagonal
         const C<R> a = v0, b = v1;
         v0 = mk<R>(dot2r<R>(m[0].x, a.x, -m[1].y, b.y), dot2r<R>(m[0].x, a.y, m[1].y, b.x));
         v1 = mk<R>(dot2r<R>(-m[2].y, a.y, m[3].x, b.x), dot2r<R>(m[2].y, a.x, m[3].x, b.y));
-        break;
-    }
-    default: {
+    } else {
         CAcc<R> p, q;
         p.add(m[0], v0); p.add(m[1], v1);
         q.add(m[2], v0); q.add(m[3], v1);
         v0 = p.get();
         v1 = q.get();
     }
+}
+
+// the same with the structure known only at run time (uniform across the block)
+template <typename R> __device__ __forceinline__ void apply_pair(int kind, const C<R> (&m)[4], C<R> &v0, C<R> &v1) {
+    switch (kind) {
+    case MK_DIAG: apply_pair_k<R, MK_DIAG>(m, v0, v1); break;
+    case MK_PHASE1: apply_pair_k<R, MK_PHASE1>(m, v0, v1); break;
+    case MK_SWAP: apply_pair_k<R, MK_SWAP>(m, v0, v1); break;
+    case MK_REAL: apply_pair_k<R, MK_REAL>(m, v0, v1); break;
+    case MK_RX: apply_pair_k<R, MK_RX>(m, v0, v1); break;
+    default: apply_pair_k<R, MK_GENERAL>(m, v0, v1); break;
     }
 }
 
@@ -453,21 +456,82 @@ __device__ __forceinline__ void add_grad(double *gradw, int32_t gslot, double p,
 // complex128: in FP64.  complex64: the pair's value is formed in FP32 with FMAs
 // (two roundings at most) and returned as a double; the sums over pairs, warps,
 // tiles and the state are FP64.
-template <typename R>
-__device__ __forceinline__ double pair_gen_im(int code, C<R> a0, C<R> a1, C<R> b0, C<R> b1) {
+template <typename R, int CODE>
+__device__ __forceinline__ double pair_gen_im_k(C<R> a0, C<R> a1, C<R> b0, C<R> b1) {
     // w = G a;  Im(conj(b) w) = b.x w.y - b.y w.x
     R r;
-    switch (code) {
-    case 1: r = fma(b0.x, a1.y, -(b0.y * a1.x)) + fma(b1.x, a0.y, -(b1.y * a0.x)); break;   // w = (a1, a0)
-    case 2: r = fma(b1.x, a0.x, b1.y * a0.y) - fma(b0.x, a1.x, b0.y * a1.y); break;         // w = (-i a1, i a0)
-    case 3: r = fma(b0.x, a0.y, -(b0.y * a0.x)) - fma(b1.x, a1.y, -(b1.y * a1.x)); break;   // w = (a0, -a1)
-    default: r = fma(b1.x, a1.y, -(b1.y * a1.x)); break;                                   // w = (0, a1)
-    }
+    if constexpr (CODE == 1) r = fma(b0.x, a1.y, -(b0.y * a1.x)) + fma(b1.x, a0.y, -(b1.y * a0.x));  // w = (a1, a0)
+    else if constexpr (CODE == 2) r = fma(b1.x, a0.x, b1.y * a0.y) - fma(b0.x, a1.x, b0.y * a1.y);   // w = (-i a1, i a0)
+    else if constexpr (CODE == 3) r = fma(b0.x, a0.y, -(b0.y * a0.x)) - fma(b1.x, a1.y, -(b1.y * a1.x));  // (a0, -a1)
+    else r = fma(b1.x, a1.y, -(b1.y * a1.x));                                                          // w = (0, a1)
     return (double)r;
+}
+template <typename R>
+__device__ __forceinline__ double pair_gen_im(int code, C<R> a0, C<R> a1, C<R> b0, C<R> b1) {
+    switch (code) {
+    case 1: return pair_gen_im_k<R, 1>(a0, a1, b0, b1);
+    case 2: return pair_gen_im_k<R, 2>(a0, a1, b0, b1);
+    case 3: return pair_gen_im_k<R, 3>(a0, a1, b0, b1);
+    default: return pair_gen_im_k<R, 4>(a0, a1, b0, b1);
+    }
+}
+
+// Run signature: length and, per member in application order, structure and generator
+// code (0: no gradient).  The common signatures get pair loops with both known at compile
+// time (no per-pair dispatch); the others use the run-time loops below.
+__host__ __device__ constexpr int run_sig(int len, int k0, int g0, int k1 = 0, int g1 = 0, int k2 = 0, int g2 = 0) {
+    return len | (k0 << 2) | (g0 << 5) | (k1 << 8) | (g1 << 11) | (k2 << 14) | (g2 << 17);
+}
+
+// forward pair loop: members applied one by one in their structured forms
+template <typename R, int NS, int LEN, int K0, int K1, int K2>
+__device__ __forceinline__ void run_fwd_fixed(C<R> *const (&s)[NS], const Range &rg, uint32_t low, uint32_t bit,
+                                              const C<R> (&m)[kMaxRun][4]) {
+    for (uint32_t g = rg.g0; g < rg.g1; g += rg.gs) {
+        const uint32_t i0 = ((g & ~low) << 1) | (g & low), i1 = i0 | bit;
+#pragma unroll
+        for (int q = 0; q < NS; ++q) {
+            C<R> a0 = s[q][i0], a1 = s[q][i1];
+            apply_pair_k<R, K0>(m[0], a0, a1);
+            if constexpr (LEN > 1) apply_pair_k<R, K1>(m[1], a0, a1);
+            if constexpr (LEN > 2) apply_pair_k<R, K2>(m[2], a0, a1);
+            s[q][i0] = a0;
+            s[q][i1] = a1;
+        }
+    }
+}
+
+// adjoint pair loop over (lambda, bra): per member (in reverse op order) the generator
+// product, then the member's inverse on both states
+template <typename R, int NS, int LEN, int K0, int G0, int K1, int G1, int K2, int G2>
+__device__ __forceinline__ void run_rev_fixed(C<R> *const (&s)[NS], const Range &rg, uint32_t low, uint32_t bit,
+                                              const C<R> (&m)[kMaxRun][4], double (&ip)[kMaxRun]) {
+    for (uint32_t g = rg.g0; g < rg.g1; g += rg.gs) {
+        const uint32_t i0 = ((g & ~low) << 1) | (g & low), i1 = i0 | bit;
+        C<R> a0 = s[0][i0], a1 = s[0][i1], b0 = s[NS - 1][i0], b1 = s[NS - 1][i1];
+        if constexpr (G0 != 0) ip[0] += pair_gen_im_k<R, G0>(a0, a1, b0, b1);
+        apply_pair_k<R, K0>(m[0], a0, a1);
+        apply_pair_k<R, K0>(m[0], b0, b1);
+        if constexpr (LEN > 1) {
+            if constexpr (G1 != 0) ip[1] += pair_gen_im_k<R, G1>(a0, a1, b0, b1);
+            apply_pair_k<R, K1>(m[1], a0, a1);
+            apply_pair_k<R, K1>(m[1], b0, b1);
+        }
+        if constexpr (LEN > 2) {
+            if constexpr (G2 != 0) ip[2] += pair_gen_im_k<R, G2>(a0, a1, b0, b1);
+            apply_pair_k<R, K2>(m[2], a0, a1);
+            apply_pair_k<R, K2>(m[2], b0, b1);
+        }
+        s[0][i0] = a0;
+        s[0][i1] = a1;
+        s[NS - 1][i0] = b0;
+        s[NS - 1][i1] = b1;
+    }
 }
 
 // A run of `len` single-wire gates on bit rb, applied per amplitude pair in registers.
-// Forward: the run's product is formed once in FP64 and applied as one 2x2 matrix.
+// Forward: structured members are applied one by one; a run with a general member has its
+// product formed once in FP64 and applied as one 2x2 matrix.
 // Adjoint: the members are undone one by one with the generator products between them.
 template <typename R, int NS, bool REV>
 __device__ void exec_run(C<R> *const (&s)[NS], int kt, int wl, bool wloc, const DOp *__restrict__ ops, int len,
@@ -478,6 +542,47 @@ __device__ void exec_run(C<R> *const (&s)[NS], int kt, int wl, bool wloc, const 
     const uint32_t bit = 1u << rb;
     const Range rg = groups(kt, wl, 1, wloc);
     if (!REV) {
+        // structured members (no general 2x2 among them) are cheaper one by one than their
+        // product, which is a general 2x2
+        C<R> mm[kMaxRun][4];
+        int kinds[kMaxRun];
+        bool all_structured = true;
+#pragma unroll
+        for (int k = 0; k < kMaxRun; ++k) {
+            kinds[k] = MK_GENERAL;
+            if (k < len) {
+                member_mat<R>(ops[k], cs, consts, false, mm[k]);
+                kinds[k] = ops[k].mkind;
+                all_structured = all_structured && kinds[k] != MK_GENERAL;
+            }
+        }
+        if (all_structured) {
+            switch (run_sig(len, kinds[0], 0, kinds[1], 0, kinds[2], 0)) {
+            case run_sig(3, MK_DIAG, 0, MK_REAL, 0, MK_DIAG, 0):
+                run_fwd_fixed<R, NS, 3, MK_DIAG, MK_REAL, MK_DIAG>(s, rg, low, bit, mm);
+                return;
+            case run_sig(2, MK_REAL, 0, MK_DIAG, 0):
+                run_fwd_fixed<R, NS, 2, MK_REAL, MK_DIAG, MK_GENERAL>(s, rg, low, bit, mm);
+                return;
+            case run_sig(2, MK_DIAG, 0, MK_REAL, 0):
+                run_fwd_fixed<R, NS, 2, MK_DIAG, MK_REAL, MK_GENERAL>(s, rg, low, bit, mm);
+                return;
+            default:
+                for (uint32_t g = rg.g0; g < rg.g1; g += rg.gs) {
+                    const uint32_t i0 = ((g & ~low) << 1) | (g & low), i1 = i0 | bit;
+#pragma unroll
+                    for (int q = 0; q < NS; ++q) {
+                        C<R> a0 = s[q][i0], a1 = s[q][i1];
+#pragma unroll
+                        for (int k = 0; k < kMaxRun; ++k)
+                            if (k < len) apply_pair<R>(kinds[k], mm[k], a0, a1);
+                        s[q][i0] = a0;
+                        s[q][i1] = a1;
+                    }
+                }
+                return;
+            }
+        }
         // product M = m_{len-1} ... m_0 in FP64
         double2 P[4] = {make_double2(1, 0), make_double2(0, 0), make_double2(0, 0), make_double2(1, 0)};
         for (int k = 0; k < len; ++k) {
@@ -525,21 +630,33 @@ __device__ void exec_run(C<R> *const (&s)[NS], int kt, int wl, bool wloc, const 
             if (op.gslot >= 0) gc[kk] = op.gcode;
         }
     }
-    for (uint32_t g = rg.g0; g < rg.g1; g += rg.gs) {
-        const uint32_t i0 = ((g & ~low) << 1) | (g & low), i1 = i0 | bit;
-        C<R> a0 = s[0][i0], a1 = s[0][i1], b0 = s[NS - 1][i0], b1 = s[NS - 1][i1];
+    switch (run_sig(len, mk_[0], gc[0], mk_[1], gc[1], mk_[2], gc[2])) {
+    case run_sig(3, MK_DIAG, 3, MK_REAL, 2, MK_DIAG, 3):  // Rot = RZ RY RZ, every angle trained
+        run_rev_fixed<R, NS, 3, MK_DIAG, 3, MK_REAL, 2, MK_DIAG, 3>(s, rg, low, bit, m, ip);
+        break;
+    case run_sig(2, MK_DIAG, 3, MK_REAL, 2):  // RY then RZ
+        run_rev_fixed<R, NS, 2, MK_DIAG, 3, MK_REAL, 2, MK_GENERAL, 0>(s, rg, low, bit, m, ip);
+        break;
+    case run_sig(2, MK_REAL, 2, MK_DIAG, 3):  // RZ then RY
+        run_rev_fixed<R, NS, 2, MK_REAL, 2, MK_DIAG, 3, MK_GENERAL, 0>(s, rg, low, bit, m, ip);
+        break;
+    default:
+        for (uint32_t g = rg.g0; g < rg.g1; g += rg.gs) {
+            const uint32_t i0 = ((g & ~low) << 1) | (g & low), i1 = i0 | bit;
+            C<R> a0 = s[0][i0], a1 = s[0][i1], b0 = s[NS - 1][i0], b1 = s[NS - 1][i1];
 #pragma unroll
-        for (int kk = 0; kk < kMaxRun; ++kk) {
-            if (kk < len) {
-                if (gc[kk]) ip[kk] += pair_gen_im<R>(gc[kk], a0, a1, b0, b1);
-                apply_pair<R>(mk_[kk], m[kk], a0, a1);
-                apply_pair<R>(mk_[kk], m[kk], b0, b1);
+            for (int kk = 0; kk < kMaxRun; ++kk) {
+                if (kk < len) {
+                    if (gc[kk]) ip[kk] += pair_gen_im<R>(gc[kk], a0, a1, b0, b1);
+                    apply_pair<R>(mk_[kk], m[kk], a0, a1);
+                    apply_pair<R>(mk_[kk], m[kk], b0, b1);
+                }
             }
+            s[0][i0] = a0;
+            s[0][i1] = a1;
+            s[NS - 1][i0] = b0;
+            s[NS - 1][i1] = b1;
         }
-        s[0][i0] = a0;
-        s[0][i1] = a1;
-        s[NS - 1][i0] = b0;
-        s[NS - 1][i1] = b1;
     }
 #pragma unroll
     for (int kk = 0; kk < kMaxRun; ++kk)
