@@ -250,12 +250,13 @@ def run_case(args):
     if args.case == "fused":
         from lightning_b200.workloads import gate_sweep, random_state
         ops = gate_sweep(args.qubits, 200, seed=7)
-        sv = capi.StateVector(args.qubits, np.complex128)
-        sv.upload(random_state(args.qubits, seed=3))
+        dt = np.complex64 if args.dtype == "c64" else np.complex128
+        sv = capi.StateVector(args.qubits, dt)
+        sv.upload(random_state(args.qubits, seed=3, dtype=dt))
         st = torch.cuda.current_stream()
         sv.set_stream(st.cuda_stream)
-        ol = capi.OpList(ops)
-        res = {"case": "fused", "qubits": args.qubits, "gates": len(ops)}
+        ol = capi.OpList(ops, dt)
+        res = {"case": "fused", "qubits": args.qubits, "dtype": args.dtype, "gates": len(ops)}
         for name, fn in (("fused", sv.apply_ops_fused), ("unfused", sv.apply_ops)):
             res[name + "_ms"] = timed(lambda: fn(ol), args.steps, args.warmup, st)
         print(json.dumps(res))
@@ -417,6 +418,7 @@ def main():
                     help="gate / batch: one kernel family on a small case (profiling)")
     ap.add_argument("--qubits", type=int, default=28, help="--case gate: state width (complex128)")
     ap.add_argument("--ncirc", type=int, default=148, help="--case batch: number of circuits")
+    ap.add_argument("--dtype", default="c128", choices=["c64", "c128"], help="--case fused: state precision")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.case != "full":

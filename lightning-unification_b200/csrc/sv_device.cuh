@@ -70,13 +70,28 @@ __device__ __forceinline__ void two_sum_acc(float &s, float &c, float t) {
     c += (s - (u - z)) + (t - z);
     s = u;
 }
+// Paired FP32 arithmetic (sm_100 FFMA2 / FADD2 / FMUL2): the real and imaginary parts go
+// through one instruction each step, with the same rounded operations per component as the
+// scalar forms, so results are bit-identical to them.
+__device__ __forceinline__ float2 neg2(float2 a) { return make_float2(-a.x, -a.y); }
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __fadd2_rn(a, neg2(b)); }
+// complex product m * v with FMA-formed components:
+// (fma(m.x, v.x, -(m.y v.y)), fma(m.x, v.y, m.y v.x))
+__device__ __forceinline__ float2 cmul2(float2 m, float2 v) {
+    const float2 q = __fmul2_rn(make_float2(m.y, m.y), make_float2(v.y, v.x));
+    return __ffma2_rn(make_float2(m.x, m.x), v, make_float2(-q.x, q.y));
+}
+// two_sum_acc on both components at once
+__device__ __forceinline__ void two_sum_acc2(float2 &s, float2 &c, float2 t) {
+    const float2 u = __fadd2_rn(s, t);
+    const float2 z = sub2(u, s);
+    c = __fadd2_rn(c, __fadd2_rn(sub2(s, sub2(u, z)), sub2(t, z)));
+    s = u;
+}
 template <> struct CAcc<float> {
-    float sr = 0.0f, si = 0.0f, cr = 0.0f, ci = 0.0f;
-    __device__ __forceinline__ void add(float2 m, float2 v) {
-        two_sum_acc(sr, cr, fmaf(m.x, v.x, -(m.y * v.y)));
-        two_sum_acc(si, ci, fmaf(m.x, v.y, m.y * v.x));
-    }
-    __device__ __forceinline__ float2 get() const { return make_float2(sr + cr, si + ci); }
+    float2 s = make_float2(0.0f, 0.0f), c = make_float2(0.0f, 0.0f);
+    __device__ __forceinline__ void add(float2 m, float2 v) { two_sum_acc2(s, c, cmul2(m, v)); }
+    __device__ __forceinline__ float2 get() const { return __fadd2_rn(s, c); }
 };
 
 // ---- deterministic FP64 block reduction -----------------------------------
