@@ -757,6 +757,29 @@ __device__ __forceinline__ uint64_t deposit_bits(uint32_t v, const uint8_t *bits
 template <typename R, bool LOAD>
 __device__ __forceinline__ void move_tile(C<R> *sm, C<R> *gm, const DSeg &sg, uint64_t tbase, uint32_t nt) {
     const int bl = 31 - __clz((int)blockDim.x);
+    // 16-byte chunks of V consecutive amplitudes, contiguous in both memories when the tile
+    // holds state bit 0 (the planner keeps the lowest state bits in every tile).  The thread's
+    // bits are deposited once; a chunk's higher bits are an OR of precomputed masks.
+    constexpr int LV = sizeof(C<R>) == 8 ? 1 : 0;
+    const int hb0 = LV + bl;
+    if ((LV == 0 || sg.lbits[0] == 0) && (nt >> LV) >= blockDim.x && sg.nl - hb0 <= 6) {
+        const uint64_t lo = tbase | deposit_bits(threadIdx.x << LV, sg.lbits, 0, hb0);
+        uint64_t hm[6];
+#pragma unroll
+        for (int i = 0; i < 6; ++i) hm[i] = hb0 + i < sg.nl ? uint64_t(1) << sg.lbits[hb0 + i] : 0;
+        const uint32_t per = (nt >> LV) >> bl;
+        for (uint32_t j = 0; j < per; ++j) {
+            uint64_t hi = 0;
+#pragma unroll
+            for (int i = 0; i < 6; ++i)
+                if ((j >> i) & 1u) hi |= hm[i];
+            float4 *g4 = reinterpret_cast<float4 *>(gm + (lo | hi));
+            float4 *s4 = reinterpret_cast<float4 *>(sm + ((threadIdx.x + (j << bl)) << LV));
+            if (LOAD) *s4 = *g4;
+            else *g4 = *s4;
+        }
+        return;
+    }
     if (nt <= blockDim.x) {
         if (threadIdx.x < nt) {
             const uint64_t a = tbase | deposit_bits(threadIdx.x, sg.lbits, 0, sg.nl);
