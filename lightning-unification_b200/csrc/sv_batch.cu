@@ -775,10 +775,15 @@ __device__ __forceinline__ void move_tile(C<R> *sm, C<R> *gm, const DSeg &sg, ui
                 if ((j >> i) & 1u) hi |= hm[i];
             float4 *g4 = reinterpret_cast<float4 *>(gm + (lo | hi));
             float4 *s4 = reinterpret_cast<float4 *>(sm + ((threadIdx.x + (j << bl)) << LV));
-            if (LOAD) *s4 = *g4;
-            else *g4 = *s4;
+            if (LOAD) {
+                // straight to shared memory: every chunk of the tile is in flight at once
+                const unsigned sa = (unsigned)__cvta_generic_to_shared(s4);
+                asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(g4) : "memory");
+            } else {
+                *g4 = *s4;
+            }
         }
-        return;
+        return;  // loads: the caller waits (tile_wait) and then synchronises
     }
     if (nt <= blockDim.x) {
         if (threadIdx.x < nt) {
@@ -795,6 +800,8 @@ __device__ __forceinline__ void move_tile(C<R> *sm, C<R> *gm, const DSeg &sg, ui
         else gm[a] = sm[l];
     }
 }
+// completes this thread's tile loads (cp.async); a barrier must follow before other threads read
+__device__ __forceinline__ void tile_wait() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 template <typename R>
 __device__ void load_tile(C<R> *dst, const C<R> *__restrict__ src, const DSeg &sg, uint64_t tbase, uint32_t nt) {
     move_tile<R, true>(dst, const_cast<C<R> *>(src), sg, tbase, nt);
@@ -890,6 +897,7 @@ __device__ void run_forward(const KArgs &A, const DCirc &c, C<R> *sm, C<R> *pa, 
                 if (threadIdx.x == 0 && tbase == 0) sm[0] = mk<R>(1, 0);
             } else {
                 load_tile<R>(sm, pa, sg, tbase, tn);
+                tile_wait();
             }
             exec_segment<R, 1, false, FULL>(A, tiles, c.kt, sg, true);
             store_tile<R>(pa, sm, sg, tbase, tn);
@@ -953,6 +961,7 @@ __global__ void __launch_bounds__(512) k_batch(KArgs A) {
                 const uint64_t tbase = insert_zeros64(t, sg.lbits, sg.nl);
                 load_tile<R>(sm0, pa, sg, tbase, tn);
                 load_tile<R>(sm1, pb, sg, tbase, tn);
+                tile_wait();
                 exec_segment<R, 2, true, FULL>(A, tiles, c.kt, sg, t == 0);
                 store_tile<R>(pa, sm0, sg, tbase, tn);
                 store_tile<R>(pb, sm1, sg, tbase, tn);
