@@ -84,6 +84,7 @@ struct DTerm {
 };
 
 constexpr int kMaxRun = 3;
+constexpr int kMaxSegOpsStaged = 160;  // ops of a segment staged in shared memory (planner cap)
 // structure of a single-wire matrix, used to spend fewer instructions per amplitude pair
 enum MKind : uint8_t { MK_GENERAL = 0, MK_DIAG = 1, MK_PHASE1 = 2, MK_REAL = 3, MK_SWAP = 4, MK_RX = 5 };
 
@@ -814,7 +815,8 @@ __device__ void store_tile(C<R> *__restrict__ dst, const C<R> *src, const DSeg &
 // Apply the gates of one segment to the tile(s): forward (NS = 1) or the adjoint
 // sweep over (lambda, bra) with gradient products (NS = 2, REV).
 template <typename R, int NS, bool REV, bool FULL>
-__device__ void exec_segment(const KArgs &A, C<R> *const (&tiles)[NS], int kt, const DSeg &sg, bool first_tile) {
+__device__ void exec_segment(const KArgs &A, C<R> *const (&tiles)[NS], int kt, const DSeg &sg, const DOp *ops,
+                             bool first_tile) {
     const int wl = kt - (31 - __clz((int)(blockDim.x >> 5)));  // bits owned by one warp's block
     bool prev_wloc = false;
     int o = REV ? (int)sg.nops - 1 : 0;
@@ -824,17 +826,17 @@ __device__ void exec_segment(const KArgs &A, C<R> *const (&tiles)[NS], int kt, c
         if (REV) {
             // walk back to the head of a run that ends at o
             int h = o;
-            while (h > 0 && A.ops[sg.op_begin + h].run == 0) --h;
-            const DOp &hd = A.ops[sg.op_begin + h];
+            while (h > 0 && ops[h].run == 0) --h;
+            const DOp &hd = ops[h];
             if (hd.run >= 2 && h + hd.run - 1 == o) {
                 head = h;
                 len = hd.run;
             }
         } else {
-            const DOp &hd = A.ops[sg.op_begin + o];
+            const DOp &hd = ops[o];
             if (hd.run >= 2) len = hd.run;
         }
-        const DOp *op0 = A.ops + sg.op_begin + head;
+        const DOp *op0 = ops + head;
         const bool wloc = wl >= 1 && op0->maxbit < wl && (len >= 2 || op0->nb <= wl);
         if (prev_wloc && wloc) __syncwarp();
         else __syncthreads();
@@ -866,29 +868,37 @@ __device__ void exec_segment(const KArgs &A, C<R> *const (&tiles)[NS], int kt, c
 
 // Stage segment `idx` in shared memory: its bit tables are indexed by loop variables in the
 // tile moves, which would put a register copy of the record in local memory.
-__device__ __forceinline__ const DSeg &stage_segment(DSeg *s_seg, const DSeg *segs, uint32_t idx) {
+// Its op records go to shared memory too: every step of every tile reads them.
+__device__ __forceinline__ const DSeg &stage_segment(DSeg *s_seg, DOp *s_ops, const KArgs &A, uint32_t idx) {
     __syncthreads();
     if (threadIdx.x < sizeof(DSeg) / 4)
-        reinterpret_cast<uint32_t *>(s_seg)[threadIdx.x] = reinterpret_cast<const uint32_t *>(segs + idx)[threadIdx.x];
+        reinterpret_cast<uint32_t *>(s_seg)[threadIdx.x] = reinterpret_cast<const uint32_t *>(A.segs + idx)[threadIdx.x];
+    const DSeg &g = A.segs[idx];
+    const uint32_t words = g.nops * (uint32_t)(sizeof(DOp) / 4);
+    const uint32_t *src = reinterpret_cast<const uint32_t *>(A.ops + g.op_begin);
+    for (uint32_t i = threadIdx.x; i < words; i += blockDim.x) reinterpret_cast<uint32_t *>(s_ops)[i] = src[i];
     __syncthreads();
     return *s_seg;
 }
 
 // one circuit, forward: state ends in tile 0 (resident) or pool A (global)
 template <typename R, bool FULL>
-__device__ void run_forward(const KArgs &A, const DCirc &c, C<R> *sm, C<R> *pa, DSeg *s_seg) {
+__device__ void run_forward(const KArgs &A, const DCirc &c, C<R> *sm, C<R> *pa, DSeg *s_seg, DOp *s_ops) {
     const uint32_t tn = 1u << c.kt;
     C<R> *tiles[1] = {sm};
     if (c.resident) {
         zero_tile<R>(sm, tn);
         __syncthreads();
         if (threadIdx.x == 0) sm[0] = mk<R>(1, 0);
-        exec_segment<R, 1, false, FULL>(A, tiles, c.kt, A.segs[c.seg_begin], true);
+        for (uint32_t si = 0; si < c.nseg; ++si) {
+            const DSeg &sg = stage_segment(s_seg, s_ops, A, c.seg_begin + si);
+            exec_segment<R, 1, false, FULL>(A, tiles, c.kt, sg, s_ops, true);
+        }
         return;
     }
     const uint64_t ntiles = uint64_t(1) << (c.n - c.kt);
     for (uint32_t si = 0; si < c.nseg; ++si) {
-        const DSeg &sg = stage_segment(s_seg, A.segs, c.seg_begin + si);
+        const DSeg &sg = stage_segment(s_seg, s_ops, A, c.seg_begin + si);
         for (uint64_t t = 0; t < ntiles; ++t) {
             const uint64_t tbase = insert_zeros64(t, sg.lbits, sg.nl);
             if (si == 0) {
@@ -899,7 +909,7 @@ __device__ void run_forward(const KArgs &A, const DCirc &c, C<R> *sm, C<R> *pa, 
                 load_tile<R>(sm, pa, sg, tbase, tn);
                 tile_wait();
             }
-            exec_segment<R, 1, false, FULL>(A, tiles, c.kt, sg, true);
+            exec_segment<R, 1, false, FULL>(A, tiles, c.kt, sg, s_ops, true);
             store_tile<R>(pa, sm, sg, tbase, tn);
             __syncthreads();
         }
@@ -915,6 +925,7 @@ __global__ void __launch_bounds__(512) k_batch(KArgs A) {
     __shared__ uint32_t s_next;
     __shared__ double s_red[kMaxObsPerCircuit * 32];
     __shared__ __align__(8) DSeg s_seg;
+    __shared__ __align__(8) DOp s_ops[kMaxSegOpsStaged];
     C<R> *sm0 = reinterpret_cast<C<R> *>(smem_raw);
     C<R> *sm1 = sm0 + (size_t(1) << A.max_kt);
     for (;;) {
@@ -928,7 +939,7 @@ __global__ void __launch_bounds__(512) k_batch(KArgs A) {
         C<R> *pb = static_cast<C<R> *>(A.pool_b) + c.off_b;
         const uint64_t namp = uint64_t(1) << c.n;
         const bool reuse = MODE == 1 && !c.resident && A.reuse && *A.reuse != 0;
-        if (!reuse) run_forward<R, FULL>(A, c, sm0, pa, &s_seg);
+        if (!reuse) run_forward<R, FULL>(A, c, sm0, pa, &s_seg, s_ops);
         const C<R> *psi = c.resident ? sm0 : pa;
         if (MODE == 0) {
             double acc[kMaxObsPerCircuit];
@@ -950,19 +961,22 @@ __global__ void __launch_bounds__(512) k_batch(KArgs A) {
         __syncthreads();
         C<R> *tiles[2] = {sm0, sm1};
         if (c.resident) {
-            exec_segment<R, 2, true, FULL>(A, tiles, c.kt, A.segs[c.seg_begin], true);
+            for (int32_t si = (int32_t)c.nseg - 1; si >= 0; --si) {
+                const DSeg &sg = stage_segment(&s_seg, s_ops, A, c.seg_begin + si);
+                exec_segment<R, 2, true, FULL>(A, tiles, c.kt, sg, s_ops, true);
+            }
             continue;
         }
         const uint64_t ntiles = uint64_t(1) << (c.n - c.kt);
         const uint32_t tn = 1u << c.kt;
         for (int32_t si = (int32_t)c.nseg - 1; si >= 0; --si) {
-            const DSeg &sg = stage_segment(&s_seg, A.segs, c.seg_begin + si);
+            const DSeg &sg = stage_segment(&s_seg, s_ops, A, c.seg_begin + si);
             for (uint64_t t = 0; t < ntiles; ++t) {
                 const uint64_t tbase = insert_zeros64(t, sg.lbits, sg.nl);
                 load_tile<R>(sm0, pa, sg, tbase, tn);
                 load_tile<R>(sm1, pb, sg, tbase, tn);
                 tile_wait();
-                exec_segment<R, 2, true, FULL>(A, tiles, c.kt, sg, t == 0);
+                exec_segment<R, 2, true, FULL>(A, tiles, c.kt, sg, s_ops, t == 0);
                 store_tile<R>(pa, sm0, sg, tbase, tn);
                 store_tile<R>(pb, sm1, sg, tbase, tn);
                 __syncthreads();
@@ -1442,6 +1456,7 @@ Planned plan(const Batch &B, const Config &cfg, bool vjp) {
                 uint64_t b = 0;
                 for (auto x : ops[j].bits) b |= uint64_t(1) << x;
                 if (popcount64(used | b) > (int)dc.kt || (popcount64(used | b | low) > (int)dc.kt && j > i)) break;
+                if (j - i >= (size_t)kMaxSegOpsStaged) break;
                 used |= b;
                 ++j;
             }
@@ -1582,7 +1597,7 @@ void build_program(Batch &B, const Config &cfg) {
     int dev = 0, maxsm = 0, nsm = sm_count();
     B200SV_CUDA(cudaGetDevice(&dev));
     B200SV_CUDA(cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-    const size_t static_smem = kMaxObsPerCircuit * 32 * 8 + 2 * 16 * 16 + 64;
+    const size_t static_smem = kMaxObsPerCircuit * 32 * 8 + 2 * 16 * 16 + 64 + sizeof(DSeg) + kMaxSegOpsStaged * sizeof(DOp);
     if (B.smem_bytes + static_smem > (size_t)maxsm)
         throw Unsupported("batch: tile does not fit in shared memory; lower kt");
     B.full = false;
