@@ -247,6 +247,21 @@ __device__ __forceinline__ void member_mat(const DOp &op, const double4 *__restr
     }
 }
 
+// The same from the op's precomputed coefficients t (op_coeffs<R, 4> in the same direction).
+template <typename R>
+__device__ __forceinline__ void member_from(const DOp &op, const C<R> (&t)[4], C<R> (&m)[4]) {
+    const C<R> zero = mk<R>(0, 0), one = mk<R>(1, 0);
+    if (op.form == F_SWAP) {
+        m[0] = zero; m[1] = one; m[2] = one; m[3] = zero;
+    } else if (op.form == F_MAT1) {
+        m[0] = t[0]; m[1] = t[1]; m[2] = t[2]; m[3] = t[3];
+    } else if (op.nt == 1) {
+        m[0] = t[0]; m[1] = zero; m[2] = zero; m[3] = t[1];
+    } else {
+        m[0] = one; m[1] = zero; m[2] = zero; m[3] = t[0];
+    }
+}
+
 // Iteration range of a step's groups: warp-local steps (every touched bit below
 // wl) keep each warp inside its own 2^wl-amplitude block, so consecutive
 // warp-local steps only need __syncwarp; other steps spread over the block.
@@ -535,7 +550,8 @@ __device__ __forceinline__ void run_rev_fixed(C<R> *const (&s)[NS], const Range 
 // product formed once in FP64 and applied as one 2x2 matrix.
 // Adjoint: the members are undone one by one with the generator products between them.
 template <typename R, int NS, bool REV>
-__device__ void exec_run(C<R> *const (&s)[NS], int kt, int wl, bool wloc, const DOp *__restrict__ ops, int len,
+__device__ void exec_run(C<R> *const (&s)[NS], int kt, int wl, bool wloc, const DOp *__restrict__ ops,
+                         const C<R> (*cf)[4], int len,
                          const double4 *__restrict__ cs, const double2 *__restrict__ consts, double *gradw,
                          bool first_tile) {
     const int rb = ops[0].rbit;
@@ -552,7 +568,7 @@ __device__ void exec_run(C<R> *const (&s)[NS], int kt, int wl, bool wloc, const 
         for (int k = 0; k < kMaxRun; ++k) {
             kinds[k] = MK_GENERAL;
             if (k < len) {
-                member_mat<R>(ops[k], cs, consts, false, mm[k]);
+                member_from<R>(ops[k], cf[k], mm[k]);
                 kinds[k] = ops[k].mkind;
                 all_structured = all_structured && kinds[k] != MK_GENERAL;
             }
@@ -626,7 +642,7 @@ __device__ void exec_run(C<R> *const (&s)[NS], int kt, int wl, bool wloc, const 
         mk_[kk] = MK_GENERAL;
         if (kk < len) {
             const DOp &op = ops[len - 1 - kk];
-            member_mat<R>(op, cs, consts, true, m[kk]);
+            member_from<R>(op, cf[len - 1 - kk], m[kk]);
             mk_[kk] = op.mkind;
             if (op.gslot >= 0) gc[kk] = op.gcode;
         }
@@ -816,7 +832,7 @@ __device__ void store_tile(C<R> *__restrict__ dst, const C<R> *src, const DSeg &
 // sweep over (lambda, bra) with gradient products (NS = 2, REV).
 template <typename R, int NS, bool REV, bool FULL>
 __device__ void exec_segment(const KArgs &A, C<R> *const (&tiles)[NS], int kt, const DSeg &sg, const DOp *ops,
-                             bool first_tile) {
+                             const C<R> (*cf)[4], bool first_tile) {
     const int wl = kt - (31 - __clz((int)(blockDim.x >> 5)));  // bits owned by one warp's block
     bool prev_wloc = false;
     int o = REV ? (int)sg.nops - 1 : 0;
@@ -841,7 +857,7 @@ __device__ void exec_segment(const KArgs &A, C<R> *const (&tiles)[NS], int kt, c
         if (prev_wloc && wloc) __syncwarp();
         else __syncthreads();
         if (len >= 2) {
-            exec_run<R, NS, REV>(tiles, kt, wl, wloc, op0, len, A.cs, A.consts, A.gradw, first_tile);
+            exec_run<R, NS, REV>(tiles, kt, wl, wloc, op0, cf + head, len, A.cs, A.consts, A.gradw, first_tile);
         } else {
             const DOp op = *op0;
             if (REV && op.gslot >= 0) {
@@ -856,7 +872,8 @@ __device__ void exec_segment(const KArgs &A, C<R> *const (&tiles)[NS], int kt, c
                 apply_op_general<R, NS>(tiles, kt, wl, wloc, op, m);
             } else {
                 C<R> m[4];
-                op_coeffs<R, 4>(op, A.cs, A.consts, REV, m);
+#pragma unroll
+                for (int r = 0; r < 4; ++r) m[r] = cf[head][r];
                 apply_op<R, NS>(tiles, kt, wl, wloc, op, m);
             }
         }
@@ -868,8 +885,11 @@ __device__ void exec_segment(const KArgs &A, C<R> *const (&tiles)[NS], int kt, c
 
 // Stage segment `idx` in shared memory: its bit tables are indexed by loop variables in the
 // tile moves, which would put a register copy of the record in local memory.
-// Its op records go to shared memory too: every step of every tile reads them.
-__device__ __forceinline__ const DSeg &stage_segment(DSeg *s_seg, DOp *s_ops, const KArgs &A, uint32_t idx) {
+// Its op records go to shared memory too, with each op's coefficients (forward or adjoint,
+// `adj`) computed once per segment instead of by every thread at every step of every tile.
+template <typename R>
+__device__ __forceinline__ const DSeg &stage_segment(DSeg *s_seg, DOp *s_ops, C<R> (*s_cf)[4], const KArgs &A,
+                                                     uint32_t idx, bool adj) {
     __syncthreads();
     if (threadIdx.x < sizeof(DSeg) / 4)
         reinterpret_cast<uint32_t *>(s_seg)[threadIdx.x] = reinterpret_cast<const uint32_t *>(A.segs + idx)[threadIdx.x];
@@ -877,13 +897,22 @@ __device__ __forceinline__ const DSeg &stage_segment(DSeg *s_seg, DOp *s_ops, co
     const uint32_t words = g.nops * (uint32_t)(sizeof(DOp) / 4);
     const uint32_t *src = reinterpret_cast<const uint32_t *>(A.ops + g.op_begin);
     for (uint32_t i = threadIdx.x; i < words; i += blockDim.x) reinterpret_cast<uint32_t *>(s_ops)[i] = src[i];
+    for (uint32_t o = threadIdx.x; o < g.nops; o += blockDim.x) {
+        const DOp &op = A.ops[g.op_begin + o];
+        if (op.form == F_MAT2) continue;  // sixteen coefficients: formed where they are used
+        C<R> t[4];
+        op_coeffs<R, 4>(op, A.cs, A.consts, adj, t);
+#pragma unroll
+        for (int r = 0; r < 4; ++r) s_cf[o][r] = t[r];
+    }
     __syncthreads();
     return *s_seg;
 }
 
 // one circuit, forward: state ends in tile 0 (resident) or pool A (global)
 template <typename R, bool FULL>
-__device__ void run_forward(const KArgs &A, const DCirc &c, C<R> *sm, C<R> *pa, DSeg *s_seg, DOp *s_ops) {
+__device__ void run_forward(const KArgs &A, const DCirc &c, C<R> *sm, C<R> *pa, DSeg *s_seg, DOp *s_ops,
+                            C<R> (*s_cf)[4]) {
     const uint32_t tn = 1u << c.kt;
     C<R> *tiles[1] = {sm};
     if (c.resident) {
@@ -891,14 +920,14 @@ __device__ void run_forward(const KArgs &A, const DCirc &c, C<R> *sm, C<R> *pa, 
         __syncthreads();
         if (threadIdx.x == 0) sm[0] = mk<R>(1, 0);
         for (uint32_t si = 0; si < c.nseg; ++si) {
-            const DSeg &sg = stage_segment(s_seg, s_ops, A, c.seg_begin + si);
-            exec_segment<R, 1, false, FULL>(A, tiles, c.kt, sg, s_ops, true);
+            const DSeg &sg = stage_segment<R>(s_seg, s_ops, s_cf, A, c.seg_begin + si, false);
+            exec_segment<R, 1, false, FULL>(A, tiles, c.kt, sg, s_ops, s_cf, true);
         }
         return;
     }
     const uint64_t ntiles = uint64_t(1) << (c.n - c.kt);
     for (uint32_t si = 0; si < c.nseg; ++si) {
-        const DSeg &sg = stage_segment(s_seg, s_ops, A, c.seg_begin + si);
+        const DSeg &sg = stage_segment<R>(s_seg, s_ops, s_cf, A, c.seg_begin + si, false);
         for (uint64_t t = 0; t < ntiles; ++t) {
             const uint64_t tbase = insert_zeros64(t, sg.lbits, sg.nl);
             if (si == 0) {
@@ -909,7 +938,7 @@ __device__ void run_forward(const KArgs &A, const DCirc &c, C<R> *sm, C<R> *pa, 
                 load_tile<R>(sm, pa, sg, tbase, tn);
                 tile_wait();
             }
-            exec_segment<R, 1, false, FULL>(A, tiles, c.kt, sg, s_ops, true);
+            exec_segment<R, 1, false, FULL>(A, tiles, c.kt, sg, s_ops, s_cf, true);
             store_tile<R>(pa, sm, sg, tbase, tn);
             __syncthreads();
         }
@@ -926,6 +955,7 @@ __global__ void __launch_bounds__(512) k_batch(KArgs A) {
     __shared__ double s_red[kMaxObsPerCircuit * 32];
     __shared__ __align__(8) DSeg s_seg;
     __shared__ __align__(8) DOp s_ops[kMaxSegOpsStaged];
+    __shared__ __align__(16) C<R> s_cf[kMaxSegOpsStaged][4];
     C<R> *sm0 = reinterpret_cast<C<R> *>(smem_raw);
     C<R> *sm1 = sm0 + (size_t(1) << A.max_kt);
     for (;;) {
@@ -939,7 +969,7 @@ __global__ void __launch_bounds__(512) k_batch(KArgs A) {
         C<R> *pb = static_cast<C<R> *>(A.pool_b) + c.off_b;
         const uint64_t namp = uint64_t(1) << c.n;
         const bool reuse = MODE == 1 && !c.resident && A.reuse && *A.reuse != 0;
-        if (!reuse) run_forward<R, FULL>(A, c, sm0, pa, &s_seg, s_ops);
+        if (!reuse) run_forward<R, FULL>(A, c, sm0, pa, &s_seg, s_ops, s_cf);
         const C<R> *psi = c.resident ? sm0 : pa;
         if (MODE == 0) {
             double acc[kMaxObsPerCircuit];
@@ -962,21 +992,21 @@ __global__ void __launch_bounds__(512) k_batch(KArgs A) {
         C<R> *tiles[2] = {sm0, sm1};
         if (c.resident) {
             for (int32_t si = (int32_t)c.nseg - 1; si >= 0; --si) {
-                const DSeg &sg = stage_segment(&s_seg, s_ops, A, c.seg_begin + si);
-                exec_segment<R, 2, true, FULL>(A, tiles, c.kt, sg, s_ops, true);
+                const DSeg &sg = stage_segment<R>(&s_seg, s_ops, s_cf, A, c.seg_begin + si, true);
+                exec_segment<R, 2, true, FULL>(A, tiles, c.kt, sg, s_ops, s_cf, true);
             }
             continue;
         }
         const uint64_t ntiles = uint64_t(1) << (c.n - c.kt);
         const uint32_t tn = 1u << c.kt;
         for (int32_t si = (int32_t)c.nseg - 1; si >= 0; --si) {
-            const DSeg &sg = stage_segment(&s_seg, s_ops, A, c.seg_begin + si);
+            const DSeg &sg = stage_segment<R>(&s_seg, s_ops, s_cf, A, c.seg_begin + si, true);
             for (uint64_t t = 0; t < ntiles; ++t) {
                 const uint64_t tbase = insert_zeros64(t, sg.lbits, sg.nl);
                 load_tile<R>(sm0, pa, sg, tbase, tn);
                 load_tile<R>(sm1, pb, sg, tbase, tn);
                 tile_wait();
-                exec_segment<R, 2, true, FULL>(A, tiles, c.kt, sg, s_ops, t == 0);
+                exec_segment<R, 2, true, FULL>(A, tiles, c.kt, sg, s_ops, s_cf, t == 0);
                 store_tile<R>(pa, sm0, sg, tbase, tn);
                 store_tile<R>(pb, sm1, sg, tbase, tn);
                 __syncthreads();
@@ -1597,7 +1627,8 @@ void build_program(Batch &B, const Config &cfg) {
     int dev = 0, maxsm = 0, nsm = sm_count();
     B200SV_CUDA(cudaGetDevice(&dev));
     B200SV_CUDA(cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-    const size_t static_smem = kMaxObsPerCircuit * 32 * 8 + 2 * 16 * 16 + 64 + sizeof(DSeg) + kMaxSegOpsStaged * sizeof(DOp);
+    const size_t static_smem = kMaxObsPerCircuit * 32 * 8 + 2 * 16 * 16 + 64 + sizeof(DSeg) +
+                               kMaxSegOpsStaged * (sizeof(DOp) + 4 * B.amp());
     if (B.smem_bytes + static_smem > (size_t)maxsm)
         throw Unsupported("batch: tile does not fit in shared memory; lower kt");
     B.full = false;
