@@ -150,6 +150,23 @@ def run_reference_arm(args):
 
 
 # ----------------------------------------------------------------------------
+def max_over_ranks(value: float, dist=None) -> float:
+    """The largest per-rank value (step times are reported as the max over ranks); every
+    rank must call it.  Works with NCCL (a CUDA tensor) and gloo (a CPU tensor)."""
+    if dist is None:
+        return value
+    import torch
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([value], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def aggregate_rate(world: int, units_per_rank: int, ms_per_step: float) -> float:
+    """Whole-job throughput of `world` replicas each processing `units_per_rank` per step."""
+    return world * units_per_rank / (ms_per_step / 1e3)
+
+
 def timed(fn, steps, warmup, stream=None):
     import torch
     for _ in range(warmup):
@@ -474,13 +491,10 @@ def main():
             out, g = step()
         e1.record()
         torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1) / args.steps
+    ms = max_over_ranks(e0.elapsed_time(e1) / args.steps, dist)
     if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
         dist.barrier()
-    value = world * ncirc / (ms / 1e3)
+    value = aggregate_rate(world, ncirc, ms)
 
     # end to end through the public API: params from pinned host memory, results back to the host
     params_host = torch.tensor(params_np, dtype=torch.float64).pin_memory()
@@ -495,7 +509,7 @@ def main():
         (gg,) = torch.autograd.grad(o, p, d)
         out_host.copy_(o.detach(), non_blocking=True)
         grad_host.copy_(gg, non_blocking=True)
-    e2e_ms = timed(e2e_step, args.steps, args.warmup)
+    e2e_ms = max_over_ranks(timed(e2e_step, args.steps, args.warmup), dist)
     h2d = (params_host.numel() + dy_host.numel()) * 8
     d2h = (out_host.numel() + grad_host.numel()) * 8
 
@@ -562,7 +576,7 @@ def main():
         "sampling": samp,
         "roofline": roof,
         "cpu_baseline": cpu,
-        "e2e": {"value": world * ncirc / (e2e_ms / 1e3), "unit": "circuits/s", "h2d_bytes_per_step": h2d,
+        "e2e": {"value": aggregate_rate(world, ncirc, e2e_ms), "unit": "circuits/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
         "gpu_launches": 3 * args.steps,
         "clocks": clk.summary(),
