@@ -480,6 +480,11 @@ def main():
 
     for _ in range(args.warmup):
         step()
+    # the engine's own kernel launches per step, read back from the engine (untimed step)
+    out_l = batched_expval(params, eng)
+    launches_fwd = eng.last_launches()
+    torch.autograd.grad(out_l, params, dy)
+    launches_vjp = eng.last_launches()
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
@@ -578,7 +583,7 @@ def main():
         "cpu_baseline": cpu,
         "e2e": {"value": aggregate_rate(world, ncirc, e2e_ms), "unit": "circuits/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
-        "gpu_launches": 3 * args.steps,
+        "gpu_launches": (launches_fwd + launches_vjp) * args.steps,
         "clocks": clk.summary(),
     }
     print(json.dumps(line), flush=True)

@@ -195,3 +195,68 @@ def test_batch_vjp_tiled_rot_ring(dtype):
     assert np.abs(out.detach().cpu().numpy() - want_out).max() < tol_out
     assert np.abs(g.cpu().numpy() - want_g).max() < tol_g
     assert np.abs(g2.cpu().numpy() - want_g).max() < tol_g
+
+
+def edge_batch(seed=21):
+    """Edge shapes: an empty circuit, one-qubit circuits, a circuit without parameters, and
+    circuits longer than one staged segment (160 ops) both on-chip (10 qubits) and tiled
+    (15 qubits complex64 / 14 complex128)."""
+    rng = np.random.default_rng(seed)
+    params = []
+    circuits = []
+
+    def obs_for(n):
+        return [[(1.0, "Z", [0])], [(0.7, "X", [n - 1])]]
+
+    circuits.append({"num_qubits": 2, "ops": [], "param_index": [], "observables": obs_for(2)})
+    for name in ("RX", "RY", "PhaseShift"):
+        circuits.append({"num_qubits": 1, "ops": [("Hadamard", [0], False, []), (name, [0], True, [])],
+                         "param_index": [-1, len(params)], "observables": [[(1.0, "Z", [0])], [(1.0, "Y", [0])]]})
+        params.append(float(rng.uniform(0, 6)))
+    circuits.append({"num_qubits": 3, "ops": [("Hadamard", [0], False, []), ("CNOT", [0, 2], False, []),
+                                              ("S", [2], False, [])], "param_index": [-1, -1, -1],
+                     "observables": obs_for(3)})
+    for n in (10, 15):
+        ops, pidx = [], []
+        for layer in range(12):
+            for q in range(n):
+                for g in ("RZ", "RY", "RZ"):
+                    ops.append((g, [q], False, []))
+                    pidx.append(len(params))
+                    params.append(float(rng.uniform(0, 2 * np.pi)))
+            for q in range(n):
+                ops.append(("CNOT", [q, (q + 1 + layer % (n - 1)) % n], False, []))
+                pidx.append(-1)
+        circuits.append({"num_qubits": n, "ops": ops, "param_index": pidx, "observables": obs_for(n)})
+    return circuits, np.array(params)
+
+
+@pytest.mark.parametrize("dtype", [np.complex128, np.complex64])
+def test_batch_edge_shapes(dtype):
+    import torch
+    from lightning_b200.batch import BatchedCircuits
+    from lightning_b200.autograd import batched_expval
+    circuits, params = edge_batch()
+    if dtype == np.complex128:
+        circuits[-1] = dict(circuits[-1], num_qubits=14,
+                            ops=[op for op in circuits[-1]["ops"] if max(op[1]) < 14],
+                            param_index=[p for op, p in zip(circuits[-1]["ops"], circuits[-1]["param_index"])
+                                         if max(op[1]) < 14],
+                            observables=[[(1.0, "Z", [0])], [(0.7, "X", [13])]])
+        used = sorted({p for c in circuits for p in c["param_index"] if p >= 0})
+        remap = {p: i for i, p in enumerate(used)}
+        for c in circuits:
+            c["param_index"] = [remap[p] if p >= 0 else -1 for p in c["param_index"]]
+        params = params[used]
+    assert max(len(c["ops"]) for c in circuits) > 160
+    eng = BatchedCircuits(circuits, len(params), dtype=dtype, use_graphs=False)
+    p = torch.tensor(params, dtype=torch.float64, device="cuda", requires_grad=True)
+    out = batched_expval(p, eng)
+    want = oracle_outputs(circuits, params)
+    tol = 1e-11 if dtype == np.complex128 else 5e-5
+    assert np.abs(out.detach().cpu().numpy() - want).max() < tol
+    rng = np.random.default_rng(2)
+    dy = rng.normal(size=out.numel())
+    (out * torch.tensor(dy, device="cuda")).sum().backward()
+    gwant = oracle_vjp(circuits, params, dy)
+    assert np.abs(p.grad.cpu().numpy() - gwant).max() < (1e-10 if dtype == np.complex128 else 2e-4)
