@@ -63,21 +63,46 @@ __device__ __forceinline__ uint32_t ins_group(uint32_t g, const uint32_t *low, i
     return g;
 }
 
+// The op's masks and offsets (and the coefficients of one- and two-wire gates) are copied
+// to registers before the group loop: the tile and the op records share shared memory, so
+// without the copies every store to the tile would force them to be read again.
+struct OpRegs {
+    uint32_t low[kMaxGroupBits];
+    uint32_t off[16];
+    uint32_t cmask;
+    int nb;
+};
+template <int D> __device__ __forceinline__ OpRegs op_regs(const FOp &op) {
+    OpRegs r;
+#pragma unroll
+    for (int j = 0; j < kMaxGroupBits; ++j) r.low[j] = op.low[j];
+#pragma unroll
+    for (int j = 0; j < 16; ++j) r.off[j] = j < D ? op.off[j] : 0u;
+    r.cmask = op.cmask;
+    r.nb = op.nb;
+    return r;
+}
+
 template <typename R, int K>
 __device__ __forceinline__ void f_dense(C<R> *s, const FOp &op, const C<R> *cf, int kt) {
     constexpr int D = 1 << K;
-    const uint32_t ng = 1u << (kt - op.nb);
+    constexpr int NCR = K <= 2 ? D * D : 1;  // coefficients held in registers
+    const OpRegs o = op_regs<D>(op);
+    C<R> m[NCR];
+#pragma unroll
+    for (int i = 0; i < NCR; ++i) m[i] = cf[i];
+    const uint32_t ng = 1u << (kt - o.nb);
     for (uint32_t g = threadIdx.x; g < ng; g += blockDim.x) {
-        const uint32_t b = ins_group(g, op.low, op.nb) | op.cmask;
+        const uint32_t b = ins_group(g, o.low, o.nb) | o.cmask;
         C<R> v[D];
 #pragma unroll
-        for (int r = 0; r < D; ++r) v[r] = s[b + op.off[r]];
+        for (int r = 0; r < D; ++r) v[r] = s[b + o.off[r]];
 #pragma unroll
         for (int r = 0; r < D; ++r) {
             CAcc<R> a;
 #pragma unroll
-            for (int c = 0; c < D; ++c) a.add(cf[r * D + c], v[c]);
-            s[b + op.off[r]] = a.get();
+            for (int c = 0; c < D; ++c) a.add(K <= 2 ? m[(r * D + c) % NCR] : cf[r * D + c], v[c]);
+            s[b + o.off[r]] = a.get();
         }
     }
 }
@@ -85,24 +110,29 @@ __device__ __forceinline__ void f_dense(C<R> *s, const FOp &op, const C<R> *cf, 
 template <typename R, int K>
 __device__ __forceinline__ void f_diag(C<R> *s, const FOp &op, const C<R> *cf, int kt) {
     constexpr int D = 1 << K;
-    const uint32_t ng = 1u << (kt - op.nb);
+    const OpRegs o = op_regs<D>(op);
+    C<R> m[D];
+#pragma unroll
+    for (int r = 0; r < D; ++r) m[r] = cf[r];
+    const uint32_t ng = 1u << (kt - o.nb);
     for (uint32_t g = threadIdx.x; g < ng; g += blockDim.x) {
-        const uint32_t b = ins_group(g, op.low, op.nb) | op.cmask;
+        const uint32_t b = ins_group(g, o.low, o.nb) | o.cmask;
 #pragma unroll
         for (int r = 0; r < D; ++r) {
             CAcc<R> a;
-            a.add(cf[r], s[b + op.off[r]]);
-            s[b + op.off[r]] = a.get();
+            a.add(m[r], s[b + o.off[r]]);
+            s[b + o.off[r]] = a.get();
         }
     }
 }
 
 template <typename R>
 __device__ __forceinline__ void f_swap(C<R> *s, const FOp &op, int kt) {
-    const uint32_t ng = 1u << (kt - op.nb);
+    const OpRegs o = op_regs<1>(op);
+    const uint32_t ng = 1u << (kt - o.nb);
     const uint32_t oa = op.off[op.ra], ob = op.off[op.rb];
     for (uint32_t g = threadIdx.x; g < ng; g += blockDim.x) {
-        const uint32_t b = ins_group(g, op.low, op.nb) | op.cmask;
+        const uint32_t b = ins_group(g, o.low, o.nb) | o.cmask;
         const C<R> t = s[b + oa];
         s[b + oa] = s[b + ob];
         s[b + ob] = t;
@@ -111,25 +141,30 @@ __device__ __forceinline__ void f_swap(C<R> *s, const FOp &op, int kt) {
 
 template <typename R>
 __device__ __forceinline__ void f_pair(C<R> *s, const FOp &op, const C<R> *cf, int kt) {
-    const uint32_t ng = 1u << (kt - op.nb);
-    const int D = 1 << op.k;
-    const uint32_t oa = op.off[op.ra], ob = op.off[op.rb];
+    const OpRegs o = op_regs<16>(op);
+    const int D = 1 << op.k, ra = op.ra, rb = op.rb, rest = op.rest;
+    C<R> m[5];
+#pragma unroll
+    for (int i = 0; i < 5; ++i) m[i] = cf[i];
+    const uint32_t ng = 1u << (kt - o.nb);
+    const uint32_t oa = op.off[ra], ob = op.off[rb];  // run-time rows: read from the record, once
     for (uint32_t g = threadIdx.x; g < ng; g += blockDim.x) {
-        const uint32_t b = ins_group(g, op.low, op.nb) | op.cmask;
+        const uint32_t b = ins_group(g, o.low, o.nb) | o.cmask;
         const C<R> va = s[b + oa], vb = s[b + ob];
         CAcc<R> x, y;
-        x.add(cf[0], va);
-        x.add(cf[1], vb);
-        y.add(cf[2], va);
-        y.add(cf[3], vb);
+        x.add(m[0], va);
+        x.add(m[1], vb);
+        y.add(m[2], va);
+        y.add(m[3], vb);
         s[b + oa] = x.get();
         s[b + ob] = y.get();
-        if (op.rest) {
-            for (int r = 0; r < D; ++r) {
-                if (r == op.ra || r == op.rb) continue;
+        if (rest) {
+#pragma unroll
+            for (int r = 0; r < 16; ++r) {
+                if (r >= D || r == ra || r == rb) continue;
                 CAcc<R> z;
-                z.add(cf[4], s[b + op.off[r]]);
-                s[b + op.off[r]] = z.get();
+                z.add(m[4], s[b + o.off[r]]);
+                s[b + o.off[r]] = z.get();
             }
         }
     }
@@ -139,9 +174,11 @@ template <typename R>
 __device__ __forceinline__ void f_parity(C<R> *s, const FOp &op, const C<R> *cf, int kt, uint64_t tbase) {
     const uint32_t n = 1u << kt;
     const int tp = __popcll(tbase & op.pm_global) & 1;
+    const uint32_t pm = op.pm_local;
+    const C<R> ph0 = cf[tp], ph1 = cf[tp ^ 1];
     for (uint32_t l = threadIdx.x; l < n; l += blockDim.x) {
         CAcc<R> a;
-        a.add(cf[(__popc(l & op.pm_local) + tp) & 1], s[l]);
+        a.add((__popc(l & pm) & 1) ? ph1 : ph0, s[l]);
         s[l] = a.get();
     }
 }
