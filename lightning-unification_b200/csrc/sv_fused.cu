@@ -381,6 +381,119 @@ FOp lower_fop(const GateDesc &g, const std::vector<int> &loc, std::vector<C<R>> 
     return f;
 }
 
+// ---- composing consecutive gates on at most three bits (complex128) ---------------------
+// A step costs one read and one write of the tile in shared memory, which bounds complex128
+// segments; gates whose bits together span at most three tile bits are multiplied into one
+// 8x8 (or smaller) matrix on the host in FP64 and applied as one dense step.  The FP64 work
+// per amplitude grows (8 complex products for three bits) but the FP64 pipe has room.
+
+bool fusable(const GateDesc &g) {
+    uint64_t b;
+    return (g.kind == Kind::Dense || g.kind == Kind::Diag || g.kind == Kind::Swap || g.kind == Kind::Pair) &&
+           tile_bits(g, b) && __builtin_popcountll(b) <= 3;
+}
+
+// apply g to a vector over the state bits pb (small index bit k-1-j <-> state bit pb[j])
+void apply_small(const GateDesc &g, const std::vector<uint32_t> &pb, std::vector<cd> &v) {
+    const int k = (int)pb.size();
+    auto small = [&](uint32_t sb) {
+        for (int j = 0; j < k; ++j)
+            if (pb[j] == sb) return 1u << (k - 1 - j);
+        return 0u;
+    };
+    uint32_t cm = 0, tall = 0;
+    for (auto c : g.cbits) cm |= small(c);
+    const int kg = (int)g.tbits.size();
+    std::vector<uint32_t> tm(kg);
+    for (int j = 0; j < kg; ++j) tall |= (tm[j] = small(g.tbits[j]));
+    auto off = [&](uint32_t r) {
+        uint32_t o = 0;
+        for (int j = 0; j < kg; ++j)
+            if ((r >> (kg - 1 - j)) & 1u) o |= tm[j];
+        return o;
+    };
+    const uint32_t D = 1u << kg;
+    for (uint32_t base = 0; base < (1u << k); ++base) {
+        if ((base & cm) != cm || (base & tall) != 0) continue;
+        switch (g.kind) {
+        case Kind::Dense: {
+            std::vector<cd> u(D), w(D, cd(0, 0));
+            for (uint32_t r = 0; r < D; ++r) u[r] = v[base | off(r)];
+            for (uint32_t r = 0; r < D; ++r)
+                for (uint32_t c = 0; c < D; ++c) w[r] += g.m[r * D + c] * u[c];
+            for (uint32_t r = 0; r < D; ++r) v[base | off(r)] = w[r];
+            break;
+        }
+        case Kind::Diag:
+            for (uint32_t r = 0; r < D; ++r) v[base | off(r)] *= g.m[r];
+            break;
+        case Kind::Swap:
+            std::swap(v[base | off(g.sa)], v[base | off(g.sb)]);
+            break;
+        case Kind::Pair: {
+            const cd a = v[base | off(g.pa)], b = v[base | off(g.pb)];
+            v[base | off(g.pa)] = g.m2[0] * a + g.m2[1] * b;
+            v[base | off(g.pb)] = g.m2[2] * a + g.m2[3] * b;
+            for (uint32_t r = 0; r < D; ++r)
+                if (r != g.pa && r != g.pb) v[base | off(r)] *= g.gamma;
+            break;
+        }
+        default: break;
+        }
+    }
+}
+
+GateDesc compose(const std::vector<const GateDesc *> &gs, uint64_t bits) {
+    GateDesc out;
+    for (int b = 63; b >= 0; --b)
+        if ((bits >> b) & 1) out.tbits.push_back((uint32_t)b);
+    const int k = (int)out.tbits.size();
+    const uint32_t D = 1u << k;
+    std::vector<cd> M(D * D);
+    for (uint32_t col = 0; col < D; ++col) {
+        std::vector<cd> e(D, cd(0, 0));
+        e[col] = cd(1, 0);
+        for (const GateDesc *g : gs) apply_small(*g, out.tbits, e);
+        for (uint32_t row = 0; row < D; ++row) M[row * D + col] = e[row];
+    }
+    bool diagonal = k <= 2;
+    for (uint32_t r = 0; r < D && diagonal; ++r)
+        for (uint32_t c = 0; c < D; ++c)
+            if (r != c && M[r * D + c] != cd(0, 0)) diagonal = false;
+    out.k = k;
+    if (diagonal) {
+        out.kind = Kind::Diag;
+        for (uint32_t r = 0; r < D; ++r) out.m.push_back(M[r * D + r]);
+    } else {
+        out.kind = Kind::Dense;
+        out.m = M;
+    }
+    return out;
+}
+
+// the segment's gates with runs on at most three bits composed
+std::vector<GateDesc> compose_passes(const std::vector<const GateDesc *> &in) {
+    std::vector<GateDesc> out;
+    size_t a = 0;
+    while (a < in.size()) {
+        if (!fusable(*in[a])) {
+            out.push_back(*in[a++]);
+            continue;
+        }
+        uint64_t bits = 0, b1 = 0;
+        tile_bits(*in[a], bits);
+        size_t b = a + 1;
+        while (b < in.size() && fusable(*in[b]) && tile_bits(*in[b], b1) && __builtin_popcountll(bits | b1) <= 3) {
+            bits |= b1;
+            ++b;
+        }
+        if (b - a == 1) out.push_back(*in[a]);
+        else out.push_back(compose(std::vector<const GateDesc *>(in.begin() + a, in.begin() + b), bits));
+        a = b;
+    }
+    return out;
+}
+
 template <typename R>
 void run_fused(void *state, uint32_t nq, const std::vector<GateDesc> &descs,
                const std::function<void(const GateDesc &)> &apply_single, cudaStream_t st) {
@@ -440,10 +553,21 @@ void run_fused(void *state, uint32_t nq, const std::vector<GateDesc> &descs,
         sg.op_begin = (uint32_t)ops.size();
         sg.coef_begin = (uint32_t)coefs.size();
         std::vector<C<R>> local;
-        for (size_t q = i; q < j; ++q) {
-            if (descs[q].kind == Kind::Noop) continue;
-            ops.push_back(lower_fop<R>(descs[q], loc, local));
+        std::vector<const GateDesc *> seg;
+        for (size_t q = i; q < j; ++q)
+            if (descs[q].kind != Kind::Noop) seg.push_back(&descs[q]);
+        bool composed = false;
+        if constexpr (sizeof(R) == 8) {
+            const std::vector<GateDesc> fused = compose_passes(seg);
+            size_t nc = 0;
+            for (auto &g : fused) nc += coef_count(g);
+            if (fused.size() < seg.size() && nc <= (size_t)kMaxSegCoefs) {
+                for (auto &g : fused) ops.push_back(lower_fop<R>(g, loc, local));
+                composed = true;
+            }
         }
+        if (!composed)
+            for (const GateDesc *g : seg) ops.push_back(lower_fop<R>(*g, loc, local));
         sg.nops = (uint32_t)(ops.size() - sg.op_begin);
         sg.ncoef = (uint32_t)local.size();
         coefs.insert(coefs.end(), local.begin(), local.end());
