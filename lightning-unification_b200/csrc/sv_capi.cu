@@ -908,6 +908,8 @@ int b200sv_adjoint_jacobian(b200sv_handle psi, const b200sv_op *ops, uint32_t no
         int64_t tp_pos = (int64_t)ntp - 1;  // reverse iterator over trainable
         int64_t trainable_number = (int64_t)ntp - 1;
         int64_t current_param_idx = (int64_t)num_param_ops - 1;
+        std::vector<void *> lambda_and_bras{lambda};
+        lambda_and_bras.insert(lambda_and_bras.end(), bras.begin(), bras.end());
         for (int64_t op_idx = (int64_t)rec.size() - 1; op_idx >= 0; --op_idx) {
             const OpRec &op = rec[op_idx];
             if (op.params.size() > 1)
@@ -938,9 +940,7 @@ int b200sv_adjoint_jacobian(b200sv_handle psi, const b200sv_op *ops, uint32_t no
                 --current_param_idx;
             }
             GateDesc adj = compile_op(op, !op.inverse, h->nq);
-            void *s[1] = {lambda};
-            apply_desc(h, s, 1, adj);
-            apply_desc_multi(h, bras, adj);
+            apply_desc_multi(h, lambda_and_bras, adj);  // lambda and every bra in one launch
         }
         std::vector<double> jt((size_t)ntp * nobs);
         if (!jt.empty())
