@@ -293,37 +293,42 @@ def run_case(args):
     print(json.dumps({"case": "batch", "ncirc": args.ncirc, "ms": ms, "circuits_per_s": args.ncirc / (ms / 1e3)}))
 
 
-def hea_forward(steps: int, warmup: int, ncirc: int = 4096):
+def hea_forward(steps: int, warmup: int, ncirc: int = 4096, dtype=np.complex64):
     """Batched hardware-efficient-ansatz forward (n ~ U[10, 20], depth ~ U[4, 16], 3n-term
-    Hamiltonian), complex64, one persistent launch replayed as a CUDA graph, vs a per-circuit loop
-    through the plain C ABI on a sample."""
+    Hamiltonian) in `dtype`, one persistent launch replayed as a CUDA graph, vs a per-circuit
+    loop through the plain C ABI on a sample (after one untimed circuit per width)."""
     import torch
     from lightning_b200 import capi
     from lightning_b200.batch import BatchedCircuits
     from lightning_b200.workloads import hea_batch, bind
     circuits, params_np = hea_batch(ncirc=ncirc, seed=11)
-    eng = BatchedCircuits(circuits, len(params_np), dtype=np.complex64, use_graphs=True)
+    eng = BatchedCircuits(circuits, len(params_np), dtype=dtype, use_graphs=True)
     params = torch.tensor(params_np, dtype=torch.float64, device="cuda")
     ms = timed(lambda: eng.forward(params), steps, warmup)
     out = eng.forward(params).cpu().numpy()
     nsample = 16
-    t0 = time.perf_counter()
-    plain, handles = [], {}
-    for c in circuits[:nsample]:
+    handles = {}
+
+    def one(c):
         n = c["num_qubits"]
         if n not in handles:
-            handles[n] = capi.StateVector(n, np.complex64)
+            handles[n] = capi.StateVector(n, dtype)
         sv = handles[n]
         sv.set_basis_state(0)
         sv.apply_ops(bind(c, params_np))
         words = [(w, ws) for _, w, ws in c["observables"][0]]
         coeffs = [cf for cf, _, _ in c["observables"][0]]
-        plain.append(sv.expval_pauli(words, coeffs)[1])
+        return sv.expval_pauli(words, coeffs)[1]
+    for c in circuits[:nsample]:
+        one(c)  # warm-up: handles created, kernels loaded
+    t0 = time.perf_counter()
+    plain = [one(c) for c in circuits[:nsample]]
     plain_s = time.perf_counter() - t0
     for sv in handles.values():
         sv.close()
     err = float(np.abs(np.array(plain) - out[:nsample]).max())
-    return {"circuits": ncirc, "dtype": "c64", "value": ncirc / (ms / 1e3), "unit": "circuits/s",
+    return {"circuits": ncirc, "dtype": "c64" if np.dtype(dtype) == np.complex64 else "c128",
+            "value": ncirc / (ms / 1e3), "unit": "circuits/s",
             "ms_per_step": ms, "per_circuit_loop": nsample / plain_s, "ratio": (ncirc / (ms / 1e3)) / (nsample / plain_s),
             "max_abs_diff_vs_loop": err}
 
@@ -559,6 +564,7 @@ def main():
     del eng
     torch.cuda.empty_cache()
     hea = hea_forward(3, 3)
+    hea128 = hea_forward(3, 3, dtype=np.complex128)
     samp = sampling_case(28)
     line = {
         "metric": METRIC, "value": value, "unit": "circuits/s", "n_gpus": world, "steps": args.steps,
@@ -578,6 +584,7 @@ def main():
                        "sweep_200_gates_ms": sweep_ms,
                        "fused_speedup": sweep_ms["unfused"] / sweep_ms["fused"]},
         "hea_batch_forward": hea,
+        "hea_batch_forward_c128": hea128,
         "sampling": samp,
         "roofline": roof,
         "cpu_baseline": cpu,
