@@ -326,6 +326,23 @@ __device__ __forceinline__ void apply_op(C<R> *const (&s)[NS], int kt, int wl, b
         return;
     }
     const Range rg = groups(kt, wl, op.nb, wloc);
+    if (op.form == F_SWAP && op.nb == 2) {  // CNOT, SWAP: two inserted bits, masks held in registers
+        const uint32_t l0 = op.low[0], l1 = op.low[1], cm = op.cmask, oa = op.off[0], ob = op.off[1];
+        for (uint32_t g = rg.g0; g < rg.g1; g += rg.gs) {
+            uint32_t lo = g & l0;
+            uint32_t i = ((g ^ lo) << 1) | lo;
+            lo = i & l1;
+            i = (((i ^ lo) << 1) | lo) | cm;
+#pragma unroll
+            for (int q = 0; q < NS; ++q) {
+                C<R> *t = s[q];
+                const C<R> a = t[i + oa];
+                t[i + oa] = t[i + ob];
+                t[i + ob] = a;
+            }
+        }
+        return;
+    }
     for (uint32_t g = rg.g0; g < rg.g1; g += rg.gs) {
         const uint32_t base = ins_local(g, op.low, op.nb) | op.cmask;
 #pragma unroll
