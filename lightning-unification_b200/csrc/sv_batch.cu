@@ -712,6 +712,17 @@ __device__ void expval_terms(const C<R> *psi, uint64_t n_amp, const DTerm *__res
     for (uint32_t t = 0; t < nterms; ++t) {
         const DTerm tm = terms[t];
         double a = 0.0;
+        if (tm.xmask == 0) {  // diagonal word (ny is 0): sum of +-|psi_i|^2, one read per amplitude
+            for (uint64_t i = threadIdx.x; i < n_amp; i += blockDim.x) {
+                const double2 v = widen<R>(psi[i]);
+                const double p = v.x * v.x + v.y * v.y;
+                a += (__popcll(i & tm.zmask) & 1) ? -p : p;
+            }
+#pragma unroll
+            for (int o = 0; o < kMaxObsPerCircuit; ++o)
+                if (o == (int)tm.obs) acc[o] += tm.coeff * a;
+            continue;
+        }
         for (uint64_t i = threadIdx.x; i < n_amp; i += blockDim.x) {
             // Re conj(psi_{i^X}) i^ny (-1)^{|i&Z|} psi_i
             const double2 vi = widen<R>(psi[i]), vj = widen<R>(psi[i ^ tm.xmask]);
@@ -734,13 +745,18 @@ __device__ void expval_terms(const C<R> *psi, uint64_t n_amp, const DTerm *__res
 // bra_j = sum_t w_t (P_t psi)_j,  (P psi)_j = i^ny (-1)^{|(j^X)&Z|} psi_{j^X}
 template <typename R>
 __device__ void init_bra(C<R> *bra, const C<R> *psi, uint64_t n_amp, const DTerm *__restrict__ terms,
-                         uint32_t nterms, const double *__restrict__ dy) {
+                         uint32_t nterms, const double *__restrict__ dy, bool weighted) {
     for (uint64_t j = threadIdx.x; j < n_amp; j += blockDim.x) {
         double br = 0.0, bi = 0.0;
+        double fd = 0.0;  // diagonal words: bra_j gets (sum of +-w) * psi_j, psi_j read once
         for (uint32_t t = 0; t < nterms; ++t) {
             const DTerm tm = terms[t];
-            const double w = tm.coeff * dy[tm.obs];
+            const double w = weighted ? tm.coeff : tm.coeff * dy[tm.obs];
             if (w == 0.0) continue;
+            if (tm.xmask == 0 && (tm.ny & 3) == 0) {
+                fd += (__popcll(j & tm.zmask) & 1) ? -w : w;
+                continue;
+            }
             const uint64_t i = j ^ tm.xmask;
             const double2 v = widen<R>(psi[i]);
             double fr = (__popcll(i & tm.zmask) & 1) ? -w : w, fi = 0.0;
@@ -752,6 +768,11 @@ __device__ void init_bra(C<R> *bra, const C<R> *psi, uint64_t n_amp, const DTerm
             }
             br += fr * v.x - fi * v.y;
             bi += fr * v.y + fi * v.x;
+        }
+        if (fd != 0.0) {
+            const double2 v = widen<R>(psi[j]);
+            br += fd * v.x;
+            bi += fd * v.y;
         }
         bra[j] = mk<R>((R)br, (R)bi);
     }
@@ -926,6 +947,23 @@ __device__ __forceinline__ const DSeg &stage_segment(DSeg *s_seg, DOp *s_ops, C<
     return *s_seg;
 }
 
+// Stage a circuit's observable terms in shared memory (the op-record buffer, free between
+// segments) when they fit; with dy given, each coefficient is multiplied by its output's dy.
+// Returns where the terms are to be read.
+__device__ __forceinline__ const DTerm *stage_terms(DTerm *s_terms, const KArgs &A, const DCirc &c,
+                                                    const double *dy) {
+    const DTerm *g = A.terms + c.term_begin;
+    if (c.nterms > kMaxSegOpsStaged * sizeof(DOp) / sizeof(DTerm)) return g;
+    __syncthreads();
+    for (uint32_t t = threadIdx.x; t < c.nterms; t += blockDim.x) {
+        DTerm x = g[t];
+        if (dy) x.coeff *= dy[x.obs];
+        s_terms[t] = x;
+    }
+    __syncthreads();
+    return s_terms;
+}
+
 // one circuit, forward: state ends in tile 0 (resident) or pool A (global)
 template <typename R, bool FULL>
 __device__ void run_forward(const KArgs &A, const DCirc &c, C<R> *sm, C<R> *pa, DSeg *s_seg, DOp *s_ops,
@@ -992,7 +1030,8 @@ __global__ void __launch_bounds__(512) k_batch(KArgs A) {
             double acc[kMaxObsPerCircuit];
 #pragma unroll
             for (int o = 0; o < kMaxObsPerCircuit; ++o) acc[o] = 0.0;
-            expval_terms<R>(psi, namp, A.terms + c.term_begin, c.nterms, acc);
+            expval_terms<R>(psi, namp, stage_terms(reinterpret_cast<DTerm *>(s_ops), A, c, nullptr), c.nterms,
+                            acc);
             block_reduce<kMaxObsPerCircuit>(acc, s_red);
             if (threadIdx.x == 0) {
 #pragma unroll
@@ -1004,7 +1043,8 @@ __global__ void __launch_bounds__(512) k_batch(KArgs A) {
         }
         // ---- VJP: bra = sum_o dy_o O_o psi, then the reverse sweep ----
         C<R> *bra = c.resident ? sm1 : pb;
-        init_bra<R>(bra, psi, namp, A.terms + c.term_begin, c.nterms, A.dy + c.out_begin);
+        const DTerm *T = stage_terms(reinterpret_cast<DTerm *>(s_ops), A, c, A.dy + c.out_begin);
+        init_bra<R>(bra, psi, namp, T, c.nterms, A.dy + c.out_begin, T != A.terms + c.term_begin);
         __syncthreads();
         C<R> *tiles[2] = {sm0, sm1};
         if (c.resident) {
