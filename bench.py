@@ -257,6 +257,9 @@ def run_case(args):
         print(json.dumps({"case": "gate", "kernel": "k_dense<double,1>", "qubits": args.qubits, "ms": ms,
                           "gbs": gbs}))
         return
+    if args.case == "plain":
+        print(json.dumps({"case": "plain", **plain_layered(not args.no_cpu)}))
+        return
     if args.case == "precision":
         res = {"case": "precision",
                "c64_33q": precision_case(33, np.complex64),
@@ -331,6 +334,57 @@ def hea_forward(steps: int, warmup: int, ncirc: int = 4096, dtype=np.complex64):
             "value": ncirc / (ms / 1e3), "unit": "circuits/s",
             "ms_per_step": ms, "per_circuit_loop": nsample / plain_s, "ratio": (ncirc / (ms / 1e3)) / (nsample / plain_s),
             "max_abs_diff_vs_loop": err}
+
+
+def plain_layered(cpu: bool, reps: int = 3):
+    """The plain single-circuit configuration: 20 qubits complex128, 10 layers of RX RY RZ on
+    every qubit + CNOT ladder (790 gates), <Z0> and the 600-parameter adjoint Jacobian, through
+    the C ABI (one launch per gate), timed as the host sees each call (median of `reps`);
+    beside it the reference module compiled from its sources, when present, on the host cores."""
+    from lightning_b200 import capi
+    from lightning_b200.workloads import layered_rotations
+    ops, obs, tp = layered_rotations()
+    sv = capi.StateVector(20, np.complex128)
+
+    def fwd():
+        sv.set_basis_state(0)
+        sv.apply_ops(ops)
+        return sv.expval(obs[0])
+
+    def fused():
+        sv.set_basis_state(0)
+        sv.apply_ops_fused(ops)
+        return sv.expval(obs[0])
+
+    res = {"qubits": 20, "dtype": "c128", "gates": len(ops), "params": len(tp)}
+    for label, fn in (("forward_expval_ms", fwd), ("forward_fused_expval_ms", fused),
+                      ("adjoint_ms", lambda: sv.adjoint_jacobian(ops, obs, tp))):
+        fwd()
+        fn()
+        ts = []
+        for _ in range(reps):
+            if label == "adjoint_ms":
+                fwd()
+            t0 = time.perf_counter()
+            fn()
+            ts.append((time.perf_counter() - t0) * 1e3)
+        res[label] = float(np.median(ts))
+    jac = sv.adjoint_jacobian(ops, obs, tp)
+    sv.close()
+    if cpu:
+        import ref  # the reference module built from its sources: the CPU baseline only
+        m = ref.load()
+        if m is not None:
+            t0 = time.perf_counter()
+            psi = ref.run_circuit(m, 20, ops)
+            ez = ref.expval(m, psi.copy(), obs[0])
+            t1 = time.perf_counter()
+            want = ref.adjoint_jacobian(m, psi, ops, obs, tp)
+            t2 = time.perf_counter()
+            res["reference_cpu"] = {"forward_expval_ms": (t1 - t0) * 1e3, "adjoint_ms": (t2 - t1) * 1e3,
+                                    "threads": os.environ.get("OMP_NUM_THREADS", f"unset ({os.cpu_count()} cores)"),
+                                    "max_abs_jac_diff": float(np.abs(jac - want).max()), "expval": ez}
+    return res
 
 
 def sampling_case(nq: int, shots: int = 10_000_000):
@@ -436,7 +490,7 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--sweep-qubits", type=int, default=30)
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--case", default="full", choices=["full", "gate", "batch", "fused", "precision"],
+    ap.add_argument("--case", default="full", choices=["full", "gate", "batch", "fused", "precision", "plain"],
                     help="gate / batch: one kernel family on a small case (profiling)")
     ap.add_argument("--qubits", type=int, default=28, help="--case gate: state width (complex128)")
     ap.add_argument("--ncirc", type=int, default=148, help="--case batch: number of circuits")
@@ -566,6 +620,7 @@ def main():
     hea = hea_forward(3, 3)
     hea128 = hea_forward(3, 3, dtype=np.complex128)
     samp = sampling_case(28)
+    plain20 = plain_layered(not args.no_cpu)
     line = {
         "metric": METRIC, "value": value, "unit": "circuits/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
@@ -586,6 +641,7 @@ def main():
         "hea_batch_forward": hea,
         "hea_batch_forward_c128": hea128,
         "sampling": samp,
+        "plain_20q_layered": plain20,
         "roofline": roof,
         "cpu_baseline": cpu,
         "e2e": {"value": aggregate_rate(world, ncirc, e2e_ms), "unit": "circuits/s", "h2d_bytes_per_step": h2d,

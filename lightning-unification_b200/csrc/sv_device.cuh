@@ -124,6 +124,15 @@ __device__ __forceinline__ void block_reduce(double (&v)[NV], double *smem /* NV
     __syncthreads();
 }
 
+// ---- asynchronous global -> shared copies (16 bytes, both addresses 16-byte aligned) ----
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait0() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
 // widen an amplitude to FP64 for reductions
 template <typename R> __device__ __forceinline__ double2 widen(C<R> a) {
     return make_double2((double)a.x, (double)a.y);

@@ -209,14 +209,6 @@ __device__ __forceinline__ uint64_t deposit(uint64_t x, const uint8_t *pos, int 
     return r;
 }
 
-__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
-    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait0() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
-
 // One segment over all tiles.  Shared memory: two tile buffers, the segment's ops and
 // coefficients.  A tile is moved in 16-byte chunks (V amplitudes each, V = 16 / the
 // amplitude size); chunk c of a thread is c = threadIdx.x + j * blockDim.x.

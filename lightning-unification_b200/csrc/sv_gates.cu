@@ -111,12 +111,29 @@ __global__ void __launch_bounds__(kThreads) k_dense(States s, DenseP<R, K> p) {
         C<R> v[D];
 #pragma unroll
         for (int r = 0; r < D; ++r) v[r] = sv[base + p.off[r]];
+        if constexpr (K >= 3) {
+            // two output rows per trip of a rolled loop: two accumulators live instead of
+            // 2^K, so more warps fit on an SM (72 vs 108 registers for complex128 at K = 3,
+            // which moves a 30-qubit 3-wire unitary from 4.5 to 6.1 TB/s); same FMA order
+#pragma unroll 1
+            for (int r = 0; r < D; r += 2) {
+                CAcc<R> a, b;
 #pragma unroll
-        for (int r = 0; r < D; ++r) {
-            CAcc<R> a;
+                for (int c = 0; c < D; ++c) {
+                    a.add(p.m[r * D + c], v[c]);
+                    b.add(p.m[r * D + D + c], v[c]);
+                }
+                sv[base + p.off[r]] = a.get();
+                sv[base + p.off[r + 1]] = b.get();
+            }
+        } else {
 #pragma unroll
-            for (int c = 0; c < D; ++c) a.add(p.m[r * D + c], v[c]);
-            sv[base + p.off[r]] = a.get();
+            for (int r = 0; r < D; ++r) {
+                CAcc<R> a;
+#pragma unroll
+                for (int c = 0; c < D; ++c) a.add(p.m[r * D + c], v[c]);
+                sv[base + p.off[r]] = a.get();
+            }
         }
     }
 }
@@ -131,16 +148,123 @@ __global__ void __launch_bounds__(kThreads) k_dense_dev(States s, DenseDevP<R, K
         C<R> v[D];
 #pragma unroll
         for (int r = 0; r < D; ++r) v[r] = sv[base + p.off[r]];
-        for (int r = 0; r < D; ++r) {
-            CAcc<R> a;
+#pragma unroll 1
+        for (int r = 0; r < D; r += 2) {
+            CAcc<R> a, b;
 #pragma unroll
-            for (int c = 0; c < D; ++c) a.add(__ldg(&p.m[r * D + c]), v[c]);
+            for (int c = 0; c < D; ++c) {
+                a.add(__ldg(&p.m[r * D + c]), v[c]);
+                b.add(__ldg(&p.m[r * D + D + c]), v[c]);
+            }
             sv[base + p.off[r]] = a.get();
+            sv[base + p.off[r + 1]] = b.get();
         }
     }
 }
 
-// Large dense blocks (k = 7..11): one CTA per group, the group staged in shared memory.
+// Dense blocks on K = 5..7 target bits (compute-bound from K = 5 in FP64): a register-tiled
+// complex matrix product.  Each CTA takes tiles of 4096 amplitudes — TG = 4096 / 2^K
+// consecutive groups times all 2^K rows — staged in shared memory with coalesced loads
+// (consecutive threads take consecutive groups), and each thread accumulates a 4 x 4 block
+// of outputs: rows tr + i * RB and groups tg + j * TG / 4, so a warp's shared-memory reads
+// are contiguous.  The matrix is passed transposed (mt[c * 2^K + r] = M[r][c]) and staged in
+// chunks of CK columns (TiledShape); every output is the same ordered sum over c as in k_dense_dev, so
+// results are bit-identical to it.  The outputs go back through the tile for coalesced
+// stores, which also makes the in-place update safe (a tile's groups belong to one CTA).
+constexpr int kTileAmps = 4096;
+constexpr int kTiledThreads = 256;
+template <int K> struct TiledShape {
+    static constexpr int D = 1 << K;
+    static constexpr int TG = kTileAmps / D;        // groups per tile
+    static constexpr int RB = D / 4;                // row blocks
+    // matrix columns per staged chunk: the whole matrix when 2^K <= 32, else two buffers of
+    // 1024 entries, filled with cp.async one chunk ahead of the one being multiplied
+    static constexpr bool kResident = D <= 32;
+    static constexpr int CK = kResident ? D : 1024 / D;
+    static constexpr int MSH = kResident ? D * D : 2 * 1024;  // staged matrix entries
+    static_assert(kTiledThreads % TG == 0 && RB * (TG / 4) == kTiledThreads, "tile shape");
+};
+template <typename R, int K> struct TiledP {
+    Insert ins;
+    uint64_t cmask, ntiles;
+    uint64_t off[1 << K];
+    const C<R> *mt;
+};
+template <typename R, int K>
+__global__ void __launch_bounds__(kTiledThreads, 2) k_dense_tiled(States s, TiledP<R, K> p) {
+    using S = TiledShape<K>;
+    constexpr int D = S::D, TG = S::TG, RB = S::RB, CK = S::CK, TG4 = TG / 4;
+    constexpr bool kResident = S::kResident;
+    constexpr int kPieces = CK * D * (int)sizeof(C<R>) / 16;  // 16-byte pieces per chunk
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C<R> *tile = reinterpret_cast<C<R> *>(smem_raw);
+    C<R> *msh = tile + kTileAmps;
+    C<R> *__restrict__ sv = static_cast<C<R> *>(s.p[blockIdx.y]);
+    const int t = threadIdx.x;
+    const int tr = t % RB, tg = t / RB;
+    // Thread t moves tile elements e = t + 256 q: group e % TG = t % TG (TG divides 256) and
+    // row t / TG + q * 256 / TG.  Tiles start at multiples of TG, so the bit insertion splits
+    // into a per-tile part and this per-thread part (the two touch disjoint bits).
+    constexpr int QS = kTiledThreads / TG;
+    const uint64_t lo = p.ins((uint64_t)(t % TG));
+    const int r0 = t / TG;
+    if constexpr (kResident)
+        for (int e = t; e < D * D; e += kTiledThreads) msh[e] = p.mt[e];
+    auto stage = [&](int ci) {  // chunk ci (columns ci * CK ...) into buffer ci & 1
+        const char *src = reinterpret_cast<const char *>(p.mt + (size_t)ci * CK * D);
+        char *dst = reinterpret_cast<char *>(msh + (ci & 1) * CK * D);
+        for (int e = t; e < kPieces; e += kTiledThreads) cp_async16(dst + 16 * e, src + 16 * e);
+        cp_async_commit();
+    };
+    for (uint64_t ti = blockIdx.x; ti < p.ntiles; ti += gridDim.x) {
+        const uint64_t base = p.ins(ti * TG) | p.cmask | lo;
+        __syncthreads();  // the previous tile has been stored and its chunks read
+        if constexpr (!kResident) stage(0);  // in flight during the tile load
+#pragma unroll
+        for (int q = 0; q < kTileAmps / kTiledThreads; ++q)
+            tile[t + q * kTiledThreads] = sv[base + p.off[r0 + q * QS]];
+        __syncthreads();
+        CAcc<R> acc[4][4];
+        for (int ci = 0; ci < D / CK; ++ci) {
+            if constexpr (!kResident) {
+                if (ci + 1 < D / CK) {
+                    stage(ci + 1);
+                    cp_async_wait1();  // chunk ci has landed (this thread's pieces)
+                } else {
+                    cp_async_wait0();
+                }
+                __syncthreads();  // ... and every thread's
+            }
+            const C<R> *mc = msh + (kResident ? 0 : (ci & 1) * CK * D);
+            const C<R> *vc = tile + ci * CK * TG;
+#pragma unroll 4
+            for (int c = 0; c < CK; ++c) {
+                C<R> m[4], v[4];
+#pragma unroll
+                for (int i = 0; i < 4; ++i) m[i] = mc[c * D + tr + i * RB];
+#pragma unroll
+                for (int j = 0; j < 4; ++j) v[j] = vc[c * TG + tg + j * TG4];
+#pragma unroll
+                for (int i = 0; i < 4; ++i)
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) acc[i][j].add(m[i], v[j]);
+            }
+            if constexpr (!kResident) __syncthreads();  // buffer ci & 1 is refilled by stage(ci + 2)
+        }
+        __syncthreads();  // every thread has read the whole tile
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) tile[(tr + i * RB) * TG + tg + j * TG4] = acc[i][j].get();
+        __syncthreads();
+#pragma unroll
+        for (int q = 0; q < kTileAmps / kTiledThreads; ++q)
+            sv[base + p.off[r0 + q * QS]] = tile[t + q * kTiledThreads];
+    }
+}
+
+// Large dense blocks (k = 8..11, and 7 on states under 12 qubits): one CTA per group, the
+// group staged in shared memory.
 struct BigDenseP {
     Insert ins;
     uint64_t ngroups;
@@ -269,12 +393,40 @@ __global__ void __launch_bounds__(kThreads) k_parity(States s, ParityP<R> p) {
 
 template <typename R> C<R> cvt(const cd &z) { return mk<R>((R)z.real(), (R)z.imag()); }
 
+// Returns false when no kernel of this family takes the gate (K = 7 on a state too small
+// for one tile); the caller then uses k_dense_big.
 template <typename R, int K>
-void launch_dense_k(const States &S, int ns, uint32_t nq, const GateDesc &g, void *scratch,
+bool launch_dense_k(const States &S, int ns, uint32_t nq, const GateDesc &g, void *scratch,
                     cudaStream_t st) {
     std::vector<uint32_t> all = g.tbits;
     all.insert(all.end(), g.cbits.begin(), g.cbits.end());
     const uint64_t ngroups = uint64_t(1) << (nq - all.size());
+    // the tiled kernel where it measured faster than k_dense_dev on a 30-qubit state:
+    // complex128 from K = 5 (17.3 vs 21.0 ms at K = 5; 10.8 vs 9.8 ms at K = 4), complex64,
+    // whose compensated sums cost twice the FP64 ones, from K = 6 (42 vs 61 ms)
+    if constexpr (K >= (sizeof(R) == 8 ? 5 : 6)) {
+        using Sh = TiledShape<K>;
+        if (ngroups >= (uint64_t)Sh::TG) {
+            constexpr int D = Sh::D;
+            std::vector<C<R>> mt((size_t)D * D);
+            for (int r = 0; r < D; ++r)
+                for (int c = 0; c < D; ++c) mt[(size_t)c * D + r] = cvt<R>(g.m[(size_t)r * D + c]);
+            // pageable source: cudaMemcpyAsync stages it before returning
+            B200SV_CUDA(cudaMemcpyAsync(scratch, mt.data(), mt.size() * sizeof(C<R>), cudaMemcpyHostToDevice, st));
+            TiledP<R, K> p{};
+            p.ins = make_insert(all);
+            p.cmask = ctrl_mask(g.cbits);
+            p.ntiles = ngroups / Sh::TG;
+            fill_offsets(p.off, g.tbits);
+            p.mt = static_cast<const C<R> *>(scratch);
+            const int smem = (int)((kTileAmps + Sh::MSH) * sizeof(C<R>));
+            B200SV_CUDA(cudaFuncSetAttribute(k_dense_tiled<R, K>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+            const uint64_t grid = std::min<uint64_t>(p.ntiles, uint64_t(sm_count()) * 2);
+            k_dense_tiled<R, K><<<dim3((unsigned)grid, ns), kTiledThreads, smem, st>>>(S, p);
+            return true;
+        }
+        if constexpr (K > 6) return false;
+    }
     if constexpr (K <= 3) {
         DenseP<R, K> p{};
         p.ins = make_insert(all);
@@ -283,7 +435,7 @@ void launch_dense_k(const States &S, int ns, uint32_t nq, const GateDesc &g, voi
         fill_offsets(p.off, g.tbits);
         for (int i = 0; i < (1 << K) * (1 << K); ++i) p.m[i] = cvt<R>(g.m[i]);
         k_dense<R, K><<<grid_for(ngroups, ns), kThreads, 0, st>>>(S, p);
-    } else {
+    } else if constexpr (K <= 6) {
         DenseDevP<R, K> p{};
         p.ins = make_insert(all);
         p.cmask = ctrl_mask(g.cbits);
@@ -296,6 +448,7 @@ void launch_dense_k(const States &S, int ns, uint32_t nq, const GateDesc &g, voi
         p.m = static_cast<const C<R> *>(scratch);
         k_dense_dev<R, K><<<grid_for(ngroups, ns), kThreads, 0, st>>>(S, p);
     }
+    return true;
 }
 
 template <typename R, int K>
@@ -345,6 +498,9 @@ void launch_gate(void *const *states, int nstates, uint32_t nq, const GateDesc &
         case 4: launch_dense_k<R, 4>(S, nstates, nq, g, scratch, st); break;
         case 5: launch_dense_k<R, 5>(S, nstates, nq, g, scratch, st); break;
         case 6: launch_dense_k<R, 6>(S, nstates, nq, g, scratch, st); break;
+        case 7:
+            if (launch_dense_k<R, 7>(S, nstates, nq, g, scratch, st)) break;
+            [[fallthrough]];
         default: {
             if (g.k > 11 || !g.cbits.empty()) throw Unsupported("dense matrices act on at most 11 wires");
             BigDenseP p{};

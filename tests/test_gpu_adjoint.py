@@ -151,6 +151,25 @@ def test_layered_rotations_vs_fd(capi):
     assert np.abs(got - fd).max() < 1e-8
 
 
+def test_layered_rotations_full_size_vs_reference(capi, ref_module):
+    """The plain configuration at its full size: 20 qubits, 10 layers of RX RY RZ + CNOT ladder
+    (790 gates), <Z0> and the 600-parameter Jacobian, complex128, against the reference's own
+    AdjointJacobianC128 (AdjointJacobianLQubit.hpp:212-335) to 1e-12."""
+    import ref
+    from lightning_b200.workloads import layered_rotations
+    ops, obs, tp = layered_rotations()
+    assert len(ops) == 790 and len(tp) == 600
+    sv = capi.StateVector(20, np.complex128)
+    sv.apply_ops(ops)
+    ez = sv.expval(obs[0])
+    got = sv.adjoint_jacobian(ops, obs, tp)
+    psi = ref.run_circuit(ref_module, 20, ops)
+    assert abs(ez - ref.expval(ref_module, psi.copy(), obs[0])) < 1e-12
+    want = ref.adjoint_jacobian(ref_module, psi, ops, obs, tp)
+    assert got.shape == (1, 600)
+    assert np.abs(got - want).max() < 1e-12
+
+
 def test_adjoint_errors(capi):
     with pytest.raises(capi.B200Error, match="not supported using the adjoint"):
         jac(capi, 1, [("Rot", [0], False, [0.1, 0.2, 0.3])], [Zs(0)], [0])

@@ -103,6 +103,26 @@ def test_apply_matrix(capi, k, dtype):
         assert np.abs(sv.download() - want).max() < TOL[dtype] * 20 * (1 << k)
 
 
+@pytest.mark.parametrize("dtype", [np.complex128, np.complex64])
+@pytest.mark.parametrize("k", [4, 5, 6, 7])
+def test_apply_matrix_tiled(capi, k, dtype):
+    """Matrices on 4..7 wires of a state wide enough for the tiled kernel (tiles of 4096
+    amplitudes), wires in the lowest, highest and scattered positions."""
+    import lq_oracle as O
+    from lightning_b200.workloads import random_unitary
+    rng = np.random.default_rng(200 + k)
+    n = 14
+    st = random_state(rng, n, dtype)
+    placements = [list(range(n - k, n)), list(range(k)), [int(w) for w in rng.choice(n, k, replace=False)]]
+    for wires, inverse in zip(placements, (False, True, False)):
+        u = random_unitary(rng, k)
+        sv = capi.StateVector(n, dtype)
+        sv.upload(st)
+        sv.apply_matrix(u.astype(dtype), wires, inverse)
+        want = O.apply_matrix(st.astype(np.complex128), u.astype(dtype).astype(np.complex128), wires, inverse)
+        assert np.abs(sv.download() - want).max() < TOL[dtype] * 20 * (1 << k)
+
+
 GENS = ["PhaseShift", "RX", "RY", "RZ", "IsingXX", "IsingXY", "IsingYY", "IsingZZ", "CRX", "CRY", "CRZ",
         "ControlledPhaseShift", "SingleExcitation", "SingleExcitationMinus", "SingleExcitationPlus",
         "DoubleExcitation", "DoubleExcitationMinus", "DoubleExcitationPlus", "MultiRZ"]
