@@ -339,8 +339,9 @@ int b200sv_batch_jacobian(b200sv_batch_handle b, const double *params_device,
 /* Record the forward / vjp of this batch as CUDA graphs on first use and
  * replay them afterwards (0 = launch directly). */
 int b200sv_batch_use_graphs(b200sv_batch_handle b, int enable);
-/* Cost model / autotuner: times candidate launch shapes on the batch once and
- * keeps the fastest; *chosen receives the chosen configuration id. */
+/* Autotuner: times a forward + VJP step (best of three) for each candidate
+ * launch shape (threads per CTA x tile width) and keeps the fastest; *chosen
+ * receives threads * 100 + tile bits. */
 int b200sv_batch_autotune(b200sv_batch_handle b, const double *params_device,
                           int *chosen);
 /* Number of kernels the last forward / vjp call launched. */
