@@ -236,6 +236,34 @@ def gate_sweep_30q(nq: int, hbm_peak: float):
     return per, sweep_ms, roof
 
 
+def matrix_sweep(nq: int, hbm_peak: float, kmax: int = 7, steps: int = 3):
+    """applyMatrix of random k-wire unitaries (k = 1..kmax, seeded wires) on an nq-qubit state,
+    complex128 and complex64: ms per launch, HBM GB/s (2 x bytes of the state) and the matrix
+    arithmetic in TFLOP/s (8 * 2^k real flops per amplitude).  Dense blocks cross from the
+    HBM roofline to the FP64 (complex128) or compensated-FP32 (complex64) one near k = 4."""
+    import torch
+    from lightning_b200 import capi
+    from lightning_b200.workloads import random_unitary
+    rng = np.random.default_rng(11)
+    st = torch.cuda.current_stream()
+    out = {}
+    for dt, label, S in ((np.complex128, "c128", 16), (np.complex64, "c64", 8)):
+        sv = capi.StateVector(nq, dt)
+        sv.set_stream(st.cuda_stream)
+        N = 1 << nq
+        rows = {}
+        for k in range(1, kmax + 1):
+            u = random_unitary(rng, k).astype(dt)
+            wires = [int(w) for w in rng.choice(nq, size=k, replace=False)]
+            ms = timed(lambda: sv.apply_matrix(u, wires), steps, 2, st)
+            rows[str(k)] = {"wires": wires, "ms": ms, "gbs": 2 * S * N / (ms * 1e6),
+                            "hbm_frac": 2 * S * N / (ms * 1e6) / hbm_peak,
+                            "tflops": 8 * (1 << k) * N / (ms * 1e9)}
+        sv.close()
+        out[label] = rows
+    return {"qubits": nq, "per_k": out}
+
+
 # DRAM bytes (read + write) of one k_dense<double,1> launch (RX) on a 26-qubit complex128
 # state, from an ncu capture; the kernel streams each amplitude once, so the traffic
 # grows in proportion to the state.
@@ -256,6 +284,20 @@ def run_case(args):
         gbs = 2 * 16 * (1 << args.qubits) / (ms * 1e6)
         print(json.dumps({"case": "gate", "kernel": "k_dense<double,1>", "qubits": args.qubits, "ms": ms,
                           "gbs": gbs}))
+        return
+    if args.case == "matrix":
+        # one random --k-wire unitary per step on a --qubits-qubit state (profiling)
+        from lightning_b200.workloads import random_unitary
+        dt = np.complex64 if args.dtype == "c64" else np.complex128
+        sv = capi.StateVector(args.qubits, dt)
+        st = torch.cuda.current_stream()
+        sv.set_stream(st.cuda_stream)
+        rng = np.random.default_rng(11)
+        u = random_unitary(rng, args.k).astype(dt)
+        wires = [int(w) for w in rng.choice(args.qubits, size=args.k, replace=False)]
+        ms = timed(lambda: sv.apply_matrix(u, wires), args.steps, args.warmup, st)
+        print(json.dumps({"case": "matrix", "qubits": args.qubits, "k": args.k, "dtype": args.dtype, "wires": wires,
+                          "ms": ms, "tflops": 8 * (1 << args.k) * (1 << args.qubits) / (ms * 1e9)}))
         return
     if args.case == "plain":
         print(json.dumps({"case": "plain", **plain_layered(not args.no_cpu)}))
@@ -490,11 +532,12 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--sweep-qubits", type=int, default=30)
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--case", default="full", choices=["full", "gate", "batch", "fused", "precision", "plain"],
+    ap.add_argument("--case", default="full", choices=["full", "gate", "batch", "fused", "precision", "plain", "matrix"],
                     help="gate / batch: one kernel family on a small case (profiling)")
     ap.add_argument("--qubits", type=int, default=28, help="--case gate: state width (complex128)")
     ap.add_argument("--ncirc", type=int, default=148, help="--case batch: number of circuits")
-    ap.add_argument("--dtype", default="c128", choices=["c64", "c128"], help="--case fused: state precision")
+    ap.add_argument("--dtype", default="c128", choices=["c64", "c128"], help="--case fused / matrix: state precision")
+    ap.add_argument("--k", type=int, default=5, help="--case matrix: wires of the unitary")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.case != "full":
@@ -613,6 +656,7 @@ def main():
 
     per, sweep_ms, roof = gate_sweep_30q(args.sweep_qubits, hbm_peak)
     roof["peak_kind"] = peak_kind
+    msweep = matrix_sweep(args.sweep_qubits, hbm_peak)
 
     cpu = None if args.no_cpu else reference_cpu(circuits, params_np, dy_np, 4)
     del eng
@@ -638,6 +682,7 @@ def main():
         "gate_sweep": {"qubits": args.sweep_qubits, "dtype": "c128", "per_gate": per,
                        "sweep_200_gates_ms": sweep_ms,
                        "fused_speedup": sweep_ms["unfused"] / sweep_ms["fused"]},
+        "matrix_sweep": msweep,
         "hea_batch_forward": hea,
         "hea_batch_forward_c128": hea128,
         "sampling": samp,
