@@ -57,8 +57,10 @@ struct DOp {
     int32_t gslot;       // gradient slot, -1 when not differentiated
     uint32_t cidx;       // constant coefficients (consts[cidx*16..])
     uint32_t gcidx;      // generator matrix (consts[gcidx*16..])
+    uint8_t back;        // run members: distance back to the run's head (0 for heads and single gates)
     double gscale;       // -2 * generator scale * (inverse ? -1 : 1)
 };
+static_assert(sizeof(DOp) == 96, "DOp layout: op records are staged in shared memory");
 
 struct DSeg {
     uint32_t op_begin, nops;
@@ -966,13 +968,11 @@ __device__ void exec_segment(const KArgs &A, C<R> *const (&tiles)[NS], int kt, c
         // find the step: a fused run (head op carries run >= 2) or a single gate
         int head = o, len = 1;
         if (REV) {
-            // walk back to the head of a run that ends at o
-            int h = o;
-            while (h > 0 && ops[h].run == 0) --h;
-            const DOp &hd = ops[h];
-            if (hd.run >= 2 && h + hd.run - 1 == o) {
+            // the sweep meets runs at their last member, which points back to the head
+            const int h = o - ops[o].back;
+            if (h != o) {
                 head = h;
-                len = hd.run;
+                len = ops[h].run;
             }
         } else {
             const DOp &hd = ops[o];
@@ -1597,7 +1597,10 @@ void mark_runs(DOp *ops, uint32_t n, const double2 *consts) {
                 ops[q].rbit = (uint8_t)b;
                 ops[q].mkind = member_kind(ops[q], consts);
             }
-            for (uint32_t q = i + 1; q < j; ++q) ops[q].run = 0;
+            for (uint32_t q = i + 1; q < j; ++q) {
+                ops[q].run = 0;
+                ops[q].back = (uint8_t)(q - i);
+            }
         }
         i = j;
     }
