@@ -236,6 +236,95 @@ def gate_sweep_30q(nq: int, hbm_peak: float):
     return per, sweep_ms, roof
 
 
+def rows_30q(nq: int, hbm_peak: float, cpu: bool, cpu_qubits: int = 26, steps: int = 3):
+    """The remaining single-state rows on an nq-qubit complex128 random state: state copy and
+    reset, the gates outside the sweep (MultiRZ, excitations, Ising, controlled rotations),
+    generators, probs, expval and var.  Per op: ms (CUDA events), algorithmic bytes (gates:
+    2 x 16 B x the amplitudes the op can change; reductions: 16 B per amplitude read; probs
+    adds 8 B per output), GB/s and the fraction of the measured copy peak; beside it, when the
+    reference module is built, the same op timed once with the reference's own lightning.qubit
+    on a cpu_qubits-qubit state on the host cores (GB/s of the same algorithmic bytes)."""
+    import torch
+    from lightning_b200 import capi
+    from lightning_b200.workloads import random_unitary
+    N = 1 << nq
+    S = 16
+    st = torch.cuda.current_stream()
+    sv = capi.StateVector(nq, np.complex128)
+    sv.set_stream(st.cuda_stream)
+    other = capi.StateVector(nq, np.complex128)
+    other.set_stream(st.cuda_stream)
+    rng = np.random.default_rng(5)
+    sv.apply_ops([("Hadamard", [q], False, []) for q in range(nq)] +
+                 [("RY", [q], False, [float(rng.uniform(0, 6.28))]) for q in range(nq)])
+    probs_out = torch.empty(N, dtype=torch.float64, device="cuda")
+    probs_small = torch.empty(1 << 10, dtype=torch.float64, device="cuda")
+    h2 = random_unitary(rng, 2)
+    h2 = (h2 + h2.conj().T) / 2
+    ham = [("ZZ", [q, (q + 1) % nq]) for q in range(nq)] + [("ZZ", [q, (q + 2) % nq]) for q in range(nq)] + \
+          [("X", [q]) for q in range(nq)]
+    # (label, call, algorithmic bytes, reference op or None)
+    rows = [
+        ("copy (A1)", lambda: other.copy_from(sv), 2 * S * N, None),
+        ("set_basis_state (A1)", lambda: other.set_basis_state(0), S * N, None),
+        ("MultiRZ 5 wires (A11)", lambda: sv.apply("MultiRZ", [0, 3, 7, 12, nq - 1], False, [0.3]), 2 * S * N,
+         ("MultiRZ", [0, 3, 7, 12, -1], [0.3])),
+        ("IsingXX (A11)", lambda: sv.apply("IsingXX", [4, nq - 3], False, [0.3]), 2 * S * N,
+         ("IsingXX", [4, -3], [0.3])),
+        ("CRX (A8)", lambda: sv.apply("CRX", [2, nq - 4], False, [0.3]), 2 * S * N // 2, ("CRX", [2, -4], [0.3])),
+        ("ControlledPhaseShift (A8)", lambda: sv.apply("ControlledPhaseShift", [6, 9], False, [0.3]),
+         2 * S * N // 4, ("ControlledPhaseShift", [6, 9], [0.3])),
+        ("SingleExcitation (A11)", lambda: sv.apply("SingleExcitation", [3, nq - 6], False, [0.3]), 2 * S * N // 2,
+         ("SingleExcitation", [3, -6], [0.3])),
+        ("DoubleExcitation (A11)", lambda: sv.apply("DoubleExcitation", [0, 5, 11, nq - 2], False, [0.3]),
+         2 * S * N // 8, ("DoubleExcitation", [0, 5, 11, -2], [0.3])),
+        ("generator RX (A12)", lambda: sv.apply_generator("RX", [8]), 2 * S * N, None),
+        ("generator CRY (A12)", lambda: sv.apply_generator("CRY", [1, 10]), 2 * S * N, None),
+        ("generator MultiRZ (A12)", lambda: sv.apply_generator("MultiRZ", [2, 4, 6]), 2 * S * N, None),
+        ("probs all wires, device output (A13)", lambda: sv.probs_device(probs_out.data_ptr()), S * N + 8 * N, None),
+        ("probs 10 wires (A13)", lambda: sv.probs_device(probs_small.data_ptr(), list(range(5, 15))), S * N, None),
+        ("expval Z0 X5 (A14)", lambda: sv.expval([(1.0, [("PauliZ", [0]), ("PauliX", [5])])]), S * N,
+         ("expval", [(1.0, [("PauliZ", [0]), ("PauliX", [5])])])),
+        ("expval Hermitian 2 wires (A14)", lambda: sv.expval([(1.0, [("Hermitian", [3, 17], h2)])]), S * N,
+         ("expval", [(1.0, [("Hermitian", [3, 17], h2)])])),
+        (f"expval_pauli {3 * nq}-term ZZ/X Hamiltonian (A14)", lambda: sv.expval_pauli(ham), S * N, None),
+        ("var Y7 (A15)", lambda: sv.var([(1.0, [("PauliY", [7])])]), S * N, ("var", [(1.0, [("PauliY", [7])])])),
+    ]
+    out = {}
+    for label, fn, nbytes, _ in rows:
+        ms = timed(fn, steps, 2, st)
+        out[label] = {"ms": ms, "algorithmic_bytes": nbytes, "gbs": nbytes / (ms * 1e6),
+                      "hbm_frac": nbytes / (ms * 1e6) / hbm_peak}
+    sv.close()
+    other.close()
+    del probs_out
+    if cpu:
+        import ref  # the reference module built from its sources: the CPU baseline only
+        m = ref.load()
+        if m is not None:
+            n2 = cpu_qubits
+            N2 = 1 << n2
+            st_np = (rng.normal(size=N2) + 1j * rng.normal(size=N2)).astype(np.complex128)
+            st_np /= np.linalg.norm(st_np)
+            svr = m.StateVectorC128(st_np)
+            scale = N2 / N
+            for label, _, nbytes, spec in rows:
+                if spec is None:
+                    continue
+                t0 = time.perf_counter()
+                if spec[0] in ("expval", "var"):
+                    getattr(ref, spec[0])(m, st_np, spec[1])
+                else:
+                    wires = [w if w >= 0 else n2 + w for w in spec[1]]
+                    getattr(svr, spec[0])(wires, False, list(spec[2]))
+                dt = time.perf_counter() - t0
+                out[label]["reference_cpu_gbs"] = nbytes * scale / (dt * 1e9)
+            out["reference_cpu"] = {"qubits": n2, "threads": os.environ.get("OMP_NUM_THREADS",
+                                                                            f"unset ({os.cpu_count()} cores)"),
+                                    "note": "one call per op, same algorithmic bytes scaled to the state size"}
+    return out
+
+
 def matrix_sweep(nq: int, hbm_peak: float, kmax: int = 7, steps: int = 3):
     """applyMatrix of random k-wire unitaries (k = 1..kmax, seeded wires) on an nq-qubit state,
     complex128 and complex64: ms per launch, HBM GB/s (2 x bytes of the state) and the matrix
@@ -301,6 +390,9 @@ def run_case(args):
         return
     if args.case == "plain":
         print(json.dumps({"case": "plain", **plain_layered(not args.no_cpu)}))
+        return
+    if args.case == "rows":
+        print(json.dumps({"case": "rows", **rows_30q(args.qubits, peaks()[0], not args.no_cpu)}))
         return
     if args.case == "precision":
         res = {"case": "precision",
@@ -532,7 +624,7 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--sweep-qubits", type=int, default=30)
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--case", default="full", choices=["full", "gate", "batch", "fused", "precision", "plain", "matrix"],
+    ap.add_argument("--case", default="full", choices=["full", "gate", "batch", "fused", "precision", "plain", "matrix", "rows"],
                     help="gate / batch: one kernel family on a small case (profiling)")
     ap.add_argument("--qubits", type=int, default=28, help="--case gate: state width (complex128)")
     ap.add_argument("--ncirc", type=int, default=148, help="--case batch: number of circuits")
@@ -657,6 +749,7 @@ def main():
     per, sweep_ms, roof = gate_sweep_30q(args.sweep_qubits, hbm_peak)
     roof["peak_kind"] = peak_kind
     msweep = matrix_sweep(args.sweep_qubits, hbm_peak)
+    rows = rows_30q(args.sweep_qubits, hbm_peak, not args.no_cpu)
 
     cpu = None if args.no_cpu else reference_cpu(circuits, params_np, dy_np, 4)
     del eng
@@ -683,6 +776,7 @@ def main():
                        "sweep_200_gates_ms": sweep_ms,
                        "fused_speedup": sweep_ms["unfused"] / sweep_ms["fused"]},
         "matrix_sweep": msweep,
+        "rows_single_state": rows,
         "hea_batch_forward": hea,
         "hea_batch_forward_c128": hea128,
         "sampling": samp,

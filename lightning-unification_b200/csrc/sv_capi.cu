@@ -269,36 +269,66 @@ void apply_observable(b200sv_state *h, const ObsRec &o, const void *psi, void *o
     }
 }
 
-// per-term Pauli values of an all-Pauli observable (host vector, term order)
+// per-term Pauli values of an all-Pauli observable (host vector, term order).  Words sorted by
+// X mask.  Words whose X mask stays below 4 MiB of amplitudes (and the diagonal ones) share
+// passes of reduce_pauli_multi, up to 32 per pass, their partner amplitudes coming from L2;
+// each wider X mask gets pair passes of reduce_pauli_group, where a thread reads both
+// amplitudes of a pair, so the state crosses HBM once per pass either way.
 std::vector<double> pauli_term_values(b200sv_state *h, const void *psi, const std::vector<PauliWord> &words) {
     const cudaStream_t st = h->stream();
     std::vector<double> vals(words.size(), 0.0);
-    // group by X mask, at most 32 per launch, results into d_small in order
     std::vector<size_t> order(words.size());
     for (size_t i = 0; i < order.size(); ++i) order[i] = i;
     std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) { return words[a].xmask < words[b].xmask; });
-    size_t done = 0;
-    std::vector<size_t> placed;
-    while (done < order.size()) {
+    const uint64_t near = (uint64_t(4) << 20) / h->amp_bytes();  // partner distance kept in L2
+    struct Pass {
+        size_t begin, count;
+        bool multi;
+    };
+    std::vector<Pass> passes;
+    size_t i = 0;
+    while (i < order.size() && words[order[i]].xmask < near) {
+        // up to 32 words and 8 distinct X masks per pass: each mask adds a partner read per
+        // amplitude, so wider passes cost as much as pair passes
+        size_t c = 0;
+        int masks = 0;
+        while (i + c < order.size() && c < 32 && words[order[i + c]].xmask < near) {
+            const bool fresh = c == 0 || words[order[i + c]].xmask != words[order[i + c - 1]].xmask;
+            if (fresh && words[order[i + c]].xmask != 0 && masks == 8) break;
+            if (fresh && words[order[i + c]].xmask != 0) ++masks;
+            ++c;
+        }
+        passes.push_back(Pass{i, c, true});
+        i += c;
+    }
+    while (i < order.size()) {
+        size_t c = 1;
+        while (i + c < order.size() && c < 32 && words[order[i + c]].xmask == words[order[i]].xmask) ++c;
+        passes.push_back(Pass{i, c, false});
+        i += c;
+    }
+    size_t pi = 0;
+    while (pi < passes.size()) {
         size_t batch = 0;
-        std::vector<std::pair<size_t, size_t>> slots;  // (term index, d_small slot)
-        while (done < order.size() && batch < kSmall) {
-            size_t j = done;
-            const uint64_t xm = words[order[j]].xmask;
+        const size_t first = passes[pi].begin;
+        while (pi < passes.size() && batch + passes[pi].count <= kSmall) {
+            const Pass &ps = passes[pi];
             std::vector<PauliWord> grp;
-            while (j < order.size() && words[order[j]].xmask == xm && grp.size() < 32) grp.push_back(words[order[j++]]);
-            if (batch + grp.size() > kSmall) break;
-            if (h->dtype == B200SV_C64)
-                reduce_pauli_group<float>(psi, h->nq, grp.data(), (int)grp.size(), h->d_partials, h->d_small + batch, st);
-            else
-                reduce_pauli_group<double>(psi, h->nq, grp.data(), (int)grp.size(), h->d_partials, h->d_small + batch, st);
-            for (size_t q = 0; q < grp.size(); ++q) slots.emplace_back(order[done + q], batch + q);
-            batch += grp.size();
-            done = j;
+            for (size_t q = 0; q < ps.count; ++q) grp.push_back(words[order[ps.begin + q]]);
+            const int cnt = (int)ps.count;
+            if (h->dtype == B200SV_C64) {
+                if (ps.multi) reduce_pauli_multi<float>(psi, h->nq, grp.data(), cnt, h->d_partials, h->d_small + batch, st);
+                else reduce_pauli_group<float>(psi, h->nq, grp.data(), cnt, h->d_partials, h->d_small + batch, st);
+            } else {
+                if (ps.multi) reduce_pauli_multi<double>(psi, h->nq, grp.data(), cnt, h->d_partials, h->d_small + batch, st);
+                else reduce_pauli_group<double>(psi, h->nq, grp.data(), cnt, h->d_partials, h->d_small + batch, st);
+            }
+            batch += ps.count;
+            ++pi;
         }
         B200SV_CUDA(cudaMemcpyAsync(h->h_small, h->d_small, batch * sizeof(double), cudaMemcpyDeviceToHost, st));
         B200SV_CUDA(cudaStreamSynchronize(st));
-        for (auto &s : slots) vals[s.first] = h->h_small[s.second];
+        for (size_t q = 0; q < batch; ++q) vals[order[first + q]] = h->h_small[q];
     }
     return vals;
 }
@@ -354,10 +384,15 @@ double expval_impl(b200sv_state *h, const ObsRec &o) {
 
 double var_impl(b200sv_state *h, const ObsRec &o) {
     if (o.terms.size() == 1 && o.terms[0].is_pauli) {
+        // <P^2> = <psi|psi> for a Pauli word: one pass gives <P> and the norm
         const double c = o.terms[0].coeff;
-        auto v = pauli_term_values(h, h->d_state, {o.terms[0].word});
-        const double n2 = norm2_of(h, h->d_state);
-        return c * c * n2 - (c * v[0]) * (c * v[0]);
+        if (h->dtype == B200SV_C64)
+            reduce_pauli_group<float>(h->d_state, h->nq, &o.terms[0].word, 1, h->d_partials, h->d_small, h->stream(), true);
+        else
+            reduce_pauli_group<double>(h->d_state, h->nq, &o.terms[0].word, 1, h->d_partials, h->d_small, h->stream(), true);
+        read_small(h, 1);
+        const double ev = h->h_small[0], n2 = h->h_small[1];
+        return c * c * n2 - (c * ev) * (c * ev);
     }
     void *out = scratch(h, 0);
     void *tmp = o.terms.size() > 1 ? scratch(h, 1) : nullptr;

@@ -55,13 +55,20 @@ void reduce_norm2(const void *a, uint32_t nq, double *partials, double *out_dev,
 template <typename R>
 void reduce_inner(const void *bra, const void *ket, uint32_t nq, double *partials, double *out_dev,
                   cudaStream_t st);
-// Pauli words sharing one X-mask.  out_dev[t] = <psi|P_t|psi> for t < nterms (<= 32).
+// A Pauli word: P|i> = i^ny (-1)^popcount(i & zmask) |i ^ xmask> (zmask covers Z and Y factors).
 struct PauliWord {
     uint64_t xmask = 0, zmask = 0;
     int ny = 0;  // number of Y factors (phase i^ny)
 };
+// out_dev[t] = <psi|P_t|psi> for up to 32 words sharing one X mask, in one pass over the
+// amplitude pairs; with_norm: out_dev[nterms] = <psi|psi> from the same pass.
 template <typename R>
 void reduce_pauli_group(const void *psi, uint32_t nq, const PauliWord *terms, int nterms,
+                        double *partials, double *out_dev, cudaStream_t st, bool with_norm = false);
+// out_dev[t] = <psi|P_t|psi> for up to 32 words of any X masks, sorted by X mask, in one pass
+// (each amplitude and its partners read; for partners within L2 reach).
+template <typename R>
+void reduce_pauli_multi(const void *psi, uint32_t nq, const PauliWord *terms, int nterms,
                         double *partials, double *out_dev, cudaStream_t st);
 // out_dev[0] = Re <psi| M |psi> for a dense Hermitian M on k <= 4 bits (matrix on device).
 template <typename R>

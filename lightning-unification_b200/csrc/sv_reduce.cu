@@ -72,57 +72,6 @@ __global__ void __launch_bounds__(kRT) k_inner(const C<R> *__restrict__ b, const
     }
 }
 
-// ---- Pauli words sharing an X mask -----------------------------------------
-// P|i> = i^ny (-1)^popcount(i & zmask) |i ^ xmask>  (zmask covers Z and Y factors)
-struct PauliGroupP {
-    uint64_t xmask, hb_low;  // hb_low: (1 << highest X bit) - 1, or 0 when xmask == 0
-    uint64_t npairs;
-    int nterms;
-    uint64_t zmask[32];
-    int ny[32];
-};
-template <typename R, int NT>
-__global__ void __launch_bounds__(kRT) k_pauli(const C<R> *__restrict__ a, PauliGroupP p, double *partials) {
-    __shared__ double sm[NT * 32];
-    double acc[NT];
-#pragma unroll
-    for (int t = 0; t < NT; ++t) acc[t] = 0.0;
-    for (uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < p.npairs;
-         g += (uint64_t)gridDim.x * blockDim.x) {
-        if (p.xmask == 0) {
-            const double2 z = widen<R>(a[g]);
-            const double pr = z.x * z.x + z.y * z.y;
-#pragma unroll
-            for (int t = 0; t < NT; ++t)
-                if (t < p.nterms) acc[t] += (__popcll(g & p.zmask[t]) & 1) ? -pr : pr;
-        } else {
-            const uint64_t lo = g & p.hb_low;
-            const uint64_t i = ((g ^ lo) << 1) | lo;  // highest X bit cleared
-            const uint64_t j = i ^ p.xmask;
-            const double2 vi = widen<R>(a[i]), vj = widen<R>(a[j]);
-            const double zr = vj.x * vi.x + vj.y * vi.y;  // conj(vj) vi
-            const double zi = vj.x * vi.y - vj.y * vi.x;
-#pragma unroll
-            for (int t = 0; t < NT; ++t) {
-                if (t < p.nterms) {
-                    double r;
-                    switch (p.ny[t] & 3) {
-                    case 0: r = zr; break;
-                    case 1: r = -zi; break;
-                    case 2: r = -zr; break;
-                    default: r = zi; break;
-                    }
-                    r *= 2.0;
-                    acc[t] += (__popcll(i & p.zmask[t]) & 1) ? -r : r;
-                }
-            }
-        }
-    }
-    block_reduce<NT>(acc, sm);
-    if (threadIdx.x == 0)
-        for (int t = 0; t < p.nterms; ++t) partials[(size_t)t * gridDim.x + blockIdx.x] = acc[t];
-}
-
 // ---- generator products ----------------------------------------------------
 // A generator acts on a group of 2^k rows (Dense k<=2, Diag k<=2, Pair k in {1,2,4})
 // or on single amplitudes by parity; w = G v is formed in registers.
@@ -140,63 +89,93 @@ template <typename R> struct GenP {
 template <typename R> struct Bras {
     const C<R> *p[16];
 };
-template <typename R>
-__device__ __forceinline__ int gen_apply(const GenP<R> &p, uint64_t g, const C<R> *__restrict__ ket,
-                                         uint64_t &base, double2 (&w)[16]) {
-    if (p.kind == (int)Kind::Parity) {
+// Row r of a group takes part in <bra|G|ket>: every row except, for the pair form with a zero
+// gamma (the excitation generators), the rows outside the 2x2 block.
+template <typename R, int KIND> __device__ __forceinline__ bool gen_row_used(const GenP<R> &p, int r) {
+    if constexpr (KIND == (int)Kind::Pair)
+        return r == p.pa || r == p.pb || p.gamma.x != 0 || p.gamma.y != 0;
+    return true;
+}
+
+// w = G v over one group, G's form (KIND) and width (K; the group has 2^K rows, one amplitude
+// for the parity form) fixed at compile time so the group stays in registers.
+template <typename R, int KIND, int K>
+__device__ __forceinline__ void gen_apply(const GenP<R> &p, uint64_t g, const C<R> *__restrict__ ket,
+                                          uint64_t &base, double2 (&w)[1 << K]) {
+    constexpr int D = 1 << K;
+    if constexpr (KIND == (int)Kind::Parity) {
         base = g;
         const double2 v = widen<R>(ket[g]);
         const C<R> f = p.pph[__popcll(g & p.pmask) & 1];
         w[0] = make_double2(f.x * v.x - f.y * v.y, f.x * v.y + f.y * v.x);
-        return 1;
-    }
-    base = p.ins(g);
-    const int D = 1 << p.k;
-    double2 v[16];
-    for (int r = 0; r < D; ++r) v[r] = widen<R>(ket[base + p.off[r]]);
-    if (p.kind == (int)Kind::Dense) {
-        for (int r = 0; r < D; ++r) {
-            double re = 0, im = 0;
-            for (int c = 0; c < D; ++c) {
-                const double mr = p.m[r * D + c].x, mi = p.m[r * D + c].y;
-                re += mr * v[c].x - mi * v[c].y;
-                im += mr * v[c].y + mi * v[c].x;
+        return;
+    } else {
+        base = p.ins(g);
+        double2 v[D];
+#pragma unroll
+        for (int r = 0; r < D; ++r)
+            v[r] = gen_row_used<R, KIND>(p, r) ? widen<R>(ket[base + p.off[r]]) : make_double2(0, 0);
+        if constexpr (KIND == (int)Kind::Dense) {
+#pragma unroll
+            for (int r = 0; r < D; ++r) {
+                double re = 0, im = 0;
+#pragma unroll
+                for (int c = 0; c < D; ++c) {
+                    const double mr = p.m[r * D + c].x, mi = p.m[r * D + c].y;
+                    re += mr * v[c].x - mi * v[c].y;
+                    im += mr * v[c].y + mi * v[c].x;
+                }
+                w[r] = make_double2(re, im);
             }
-            w[r] = make_double2(re, im);
-        }
-    } else if (p.kind == (int)Kind::Diag) {
-        for (int r = 0; r < D; ++r) {
-            const double mr = p.m[r].x, mi = p.m[r].y;
-            w[r] = make_double2(mr * v[r].x - mi * v[r].y, mr * v[r].y + mi * v[r].x);
-        }
-    } else {  // Pair
-        for (int r = 0; r < D; ++r) {
+        } else if constexpr (KIND == (int)Kind::Diag) {
+#pragma unroll
+            for (int r = 0; r < D; ++r) {
+                const double mr = p.m[r].x, mi = p.m[r].y;
+                w[r] = make_double2(mr * v[r].x - mi * v[r].y, mr * v[r].y + mi * v[r].x);
+            }
+        } else {  // Pair: 2x2 block on rows pa, pb, gamma on the others
+            // rows pa, pb picked by masked sums: a select the compiler could turn back into a
+            // run-time array index would put v in local memory
+            double2 va = make_double2(0, 0), vb = make_double2(0, 0);
+#pragma unroll
+            for (int r = 0; r < D; ++r) {
+                const double sa = r == p.pa ? 1.0 : 0.0, sb = r == p.pb ? 1.0 : 0.0;
+                va.x = fma(sa, v[r].x, va.x);
+                va.y = fma(sa, v[r].y, va.y);
+                vb.x = fma(sb, v[r].x, vb.x);
+                vb.y = fma(sb, v[r].y, vb.y);
+            }
+            const C<R> m0 = p.m2[0], m1 = p.m2[1], m2 = p.m2[2], m3 = p.m2[3];
+            const double2 wa = make_double2(m0.x * va.x - m0.y * va.y + m1.x * vb.x - m1.y * vb.y,
+                                            m0.x * va.y + m0.y * va.x + m1.x * vb.y + m1.y * vb.x);
+            const double2 wb = make_double2(m2.x * va.x - m2.y * va.y + m3.x * vb.x - m3.y * vb.y,
+                                            m2.x * va.y + m2.y * va.x + m3.x * vb.y + m3.y * vb.x);
             const double gr = p.gamma.x, gi = p.gamma.y;
-            w[r] = make_double2(gr * v[r].x - gi * v[r].y, gr * v[r].y + gi * v[r].x);
+#pragma unroll
+            for (int r = 0; r < D; ++r)
+                w[r] = r == p.pa ? wa
+                     : r == p.pb ? wb
+                                 : make_double2(gr * v[r].x - gi * v[r].y, gr * v[r].y + gi * v[r].x);
         }
-        const double2 va = v[p.pa], vb = v[p.pb];
-        const C<R> *m = p.m2;
-        w[p.pa] = make_double2(m[0].x * va.x - m[0].y * va.y + m[1].x * vb.x - m[1].y * vb.y,
-                               m[0].x * va.y + m[0].y * va.x + m[1].x * vb.y + m[1].y * vb.x);
-        w[p.pb] = make_double2(m[2].x * va.x - m[2].y * va.y + m[3].x * vb.x - m[3].y * vb.y,
-                               m[2].x * va.y + m[2].y * va.x + m[3].x * vb.y + m[3].y * vb.x);
     }
-    return D;
 }
 
 // Both components of <bra|G|ket> for one bra: partials[0..nb) = Re, [nb..2nb) = Im.
-template <typename R>
+template <typename R, int KIND, int K>
 __global__ void __launch_bounds__(kRT) k_gen_inner_c(const C<R> *__restrict__ bra, const C<R> *__restrict__ ket,
                                                      GenP<R> p, double *partials) {
     __shared__ double sm[2 * 32];
+    constexpr int D = 1 << K;
     double acc[2] = {0.0, 0.0};
     for (uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < p.ngroups;
          g += (uint64_t)gridDim.x * blockDim.x) {
         uint64_t base;
-        double2 w[16];
-        const int D = gen_apply<R>(p, g, ket, base, w);
+        double2 w[D];
+        gen_apply<R, KIND, K>(p, g, ket, base, w);
+#pragma unroll
         for (int r = 0; r < D; ++r) {
-            const uint64_t idx = (p.kind == (int)Kind::Parity) ? base : base + p.off[r];
+            if (!gen_row_used<R, KIND>(p, r)) continue;
+            const uint64_t idx = KIND == (int)Kind::Parity ? base : base + p.off[r];
             const double2 b = widen<R>(bra[idx]);
             acc[0] += b.x * w[r].x + b.y * w[r].y;  // Re conj(b) w
             acc[1] += b.x * w[r].y - b.y * w[r].x;  // Im conj(b) w
@@ -209,20 +188,23 @@ __global__ void __launch_bounds__(kRT) k_gen_inner_c(const C<R> *__restrict__ br
     }
 }
 
-template <typename R, int NB>
+template <typename R, int NB, int KIND, int K>
 __global__ void __launch_bounds__(kRT) k_gen_inner(Bras<R> bras, int nbra, const C<R> *__restrict__ ket,
                                                    GenP<R> p, double *partials) {
     __shared__ double sm[NB * 32];
+    constexpr int D = 1 << K;
     double acc[NB];
 #pragma unroll
     for (int o = 0; o < NB; ++o) acc[o] = 0.0;
     for (uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < p.ngroups;
          g += (uint64_t)gridDim.x * blockDim.x) {
         uint64_t base;
-        double2 w[16];
-        const int D = gen_apply<R>(p, g, ket, base, w);
+        double2 w[D];
+        gen_apply<R, KIND, K>(p, g, ket, base, w);
+#pragma unroll
         for (int r = 0; r < D; ++r) {
-            const uint64_t idx = (p.kind == (int)Kind::Parity) ? base : base + p.off[r];
+            if (!gen_row_used<R, KIND>(p, r)) continue;
+            const uint64_t idx = KIND == (int)Kind::Parity ? base : base + p.off[r];
 #pragma unroll
             for (int o = 0; o < NB; ++o) {
                 if (o < nbra) {
@@ -233,8 +215,58 @@ __global__ void __launch_bounds__(kRT) k_gen_inner(Bras<R> bras, int nbra, const
         }
     }
     block_reduce<NB>(acc, sm);
-    if (threadIdx.x == 0)
-        for (int o = 0; o < nbra; ++o) partials[(size_t)o * gridDim.x + blockIdx.x] = acc[o];
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int o = 0; o < NB; ++o)
+            if (o < nbra) partials[(size_t)o * gridDim.x + blockIdx.x] = acc[o];
+    }
+}
+
+// launchers of the two inner-product kernels for one generator form (with_gen_form)
+template <typename R> struct GoGenC {
+    int nb;
+    cudaStream_t st;
+    const C<R> *b, *k;
+    const GenP<R> &p;
+    double *partials;
+    template <int KIND, int K> void go() const { k_gen_inner_c<R, KIND, K><<<nb, kRT, 0, st>>>(b, k, p, partials); }
+};
+template <typename R> struct GoGen {
+    int nb, nbra;
+    cudaStream_t st;
+    const Bras<R> &B;
+    const C<R> *k;
+    const GenP<R> &p;
+    double *partials;
+    template <int KIND, int K> void go() const {
+        if (nbra == 1) k_gen_inner<R, 1, KIND, K><<<nb, kRT, 0, st>>>(B, nbra, k, p, partials);
+        else if (nbra <= 4) k_gen_inner<R, 4, KIND, K><<<nb, kRT, 0, st>>>(B, nbra, k, p, partials);
+        else k_gen_inner<R, 16, KIND, K><<<nb, kRT, 0, st>>>(B, nbra, k, p, partials);
+    }
+};
+
+// Call f.template go<KIND, K>() for the generator form of p (the forms and widths
+// compile_generator produces).
+template <typename R, typename F> void with_gen_form(const GenP<R> &p, const F &f) {
+    switch (p.kind) {
+    case (int)Kind::Parity: f.template go<(int)Kind::Parity, 0>(); return;
+    case (int)Kind::Dense:
+        if (p.k == 1) f.template go<(int)Kind::Dense, 1>();
+        else f.template go<(int)Kind::Dense, 2>();
+        return;
+    case (int)Kind::Diag:
+        if (p.k == 0) f.template go<(int)Kind::Diag, 0>();
+        else if (p.k == 1) f.template go<(int)Kind::Diag, 1>();
+        else f.template go<(int)Kind::Diag, 2>();
+        return;
+    case (int)Kind::Pair:
+        if (p.k == 1) f.template go<(int)Kind::Pair, 1>();
+        else if (p.k == 2) f.template go<(int)Kind::Pair, 2>();
+        else if (p.k == 4) f.template go<(int)Kind::Pair, 4>();
+        else throw Unsupported("generator pair form on 1, 2 or 4 wires");
+        return;
+    default: throw Unsupported("generator form not supported in the inner product");
+    }
 }
 
 // ---- Hermitian sandwich ------------------------------------------------------
@@ -244,21 +276,26 @@ template <typename R> struct DenseEvP {
     uint64_t off[16];
     int k;
 };
-template <typename R>
+// K is a template parameter so the group's amplitudes stay in registers (a run-time 2^k
+// indexed its array dynamically and put it in local memory)
+template <typename R, int K>
 __global__ void __launch_bounds__(kRT) k_dense_ev(const C<R> *__restrict__ a, DenseEvP<R> p,
                                                   const C<R> *__restrict__ m, double *partials) {
     __shared__ double sm[32];
+    constexpr int D = 1 << K;
     double acc[1] = {0.0};
-    const int D = 1 << p.k;
     for (uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < p.ngroups;
          g += (uint64_t)gridDim.x * blockDim.x) {
         const uint64_t base = p.ins(g);
-        double2 v[16];
+        double2 v[D];
+#pragma unroll
         for (int r = 0; r < D; ++r) v[r] = widen<R>(a[base + p.off[r]]);
+#pragma unroll
         for (int r = 0; r < D; ++r) {
             double re = 0, im = 0;
+#pragma unroll
             for (int c = 0; c < D; ++c) {
-                const C<R> x = m[r * D + c];
+                const C<R> x = __ldg(&m[r * D + c]);
                 re += (double)x.x * v[c].x - (double)x.y * v[c].y;
                 im += (double)x.x * v[c].y + (double)x.y * v[c].x;
             }
@@ -401,18 +438,142 @@ void reduce_inner(const void *bra, const void *ket, uint32_t nq, double *partial
     finalize(partials, nb, 2, out, 1, 1.0, st);
 }
 
+// ---- Pauli words sharing an X mask -----------------------------------------
+// P|i> = i^ny (-1)^popcount(i & zmask) |i ^ xmask>  (zmask covers Z and Y factors)
+struct PauliGroupP {
+    uint64_t xmask, hb_low;  // hb_low: (1 << highest X bit) - 1, or 0 when xmask == 0
+    uint64_t npairs;
+    int nterms;
+    int norm;               // also accumulate <psi|psi> (after the words)
+    uint64_t zmask[32];
+    double cr[32], ci[32];  // Re(i^ny z) = cr Re z + ci Im z
+};
+template <typename R, int NT>
+__global__ void __launch_bounds__(kRT) k_pauli(const C<R> *__restrict__ a, PauliGroupP p, double *partials) {
+    __shared__ double sm[(NT + 1) * 32];
+    double acc[NT + 1];
+#pragma unroll
+    for (int t = 0; t <= NT; ++t) acc[t] = 0.0;
+    for (uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < p.npairs;
+         g += (uint64_t)gridDim.x * blockDim.x) {
+        if (p.xmask == 0) {
+            const double2 z = widen<R>(a[g]);
+            const double pr = z.x * z.x + z.y * z.y;
+#pragma unroll
+            for (int t = 0; t < NT; ++t)
+                if (t < p.nterms) acc[t] += (__popcll(g & p.zmask[t]) & 1) ? -pr : pr;
+            acc[NT] += pr;
+        } else {
+            const uint64_t lo = g & p.hb_low;
+            const uint64_t i = ((g ^ lo) << 1) | lo;  // highest X bit cleared
+            const uint64_t j = i ^ p.xmask;
+            const double2 vi = widen<R>(a[i]), vj = widen<R>(a[j]);
+            const double zr = 2.0 * (vj.x * vi.x + vj.y * vi.y);  // 2 conj(vj) vi: both ends of the pair
+            const double zi = 2.0 * (vj.x * vi.y - vj.y * vi.x);
+#pragma unroll
+            for (int t = 0; t < NT; ++t) {
+                if (t < p.nterms) {
+                    const double r = fma(p.cr[t], zr, p.ci[t] * zi);
+                    acc[t] += (__popcll(i & p.zmask[t]) & 1) ? -r : r;
+                }
+            }
+            acc[NT] += vi.x * vi.x + vi.y * vi.y + vj.x * vj.x + vj.y * vj.y;
+        }
+    }
+    block_reduce<NT + 1>(acc, sm);
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int t = 0; t < NT; ++t)
+            if (t < p.nterms) partials[(size_t)t * gridDim.x + blockIdx.x] = acc[t];
+        if (p.norm) partials[(size_t)p.nterms * gridDim.x + blockIdx.x] = acc[NT];
+    }
+}
+
+// ---- Pauli words with different X masks, one pass -----------------------------
+// <psi|P|psi> = sum_i conj(psi_i) i^ny (-1)^popcount((i ^ x) & zmask) psi_(i ^ x), summed over
+// every i (each pair of amplitudes is visited from both ends).  Words come sorted by X mask;
+// a word whose mask differs from the previous word's loads its partner amplitude, the others
+// reuse it.  Per word the i^ny phase is a precomputed pair (cr, ci) applied to conj(v) u and
+// the sign a parity flip, so the inner step is branch-free; states of up to 32 qubits use
+// 32-bit index arithmetic.
+struct PauliMultiP {
+    uint64_t n;
+    int nterms;
+    uint64_t xmask[32];
+    uint64_t zmask[32];
+    double cr[32], ci[32];  // Re(i^ny z) = cr Re z + ci Im z
+    int newx[32];           // 1: this word's X mask differs from the previous word's
+};
+template <typename R, int NT, typename I>
+__global__ void __launch_bounds__(kRT) k_pauli_multi(const C<R> *__restrict__ a, PauliMultiP p, double *partials) {
+    // U amplitudes per thread and trip, so U loads (and U partner loads per X mask) are in
+    // flight together
+    constexpr int U = 4;
+    __shared__ double sm[NT * 32];
+    double acc[NT];
+#pragma unroll
+    for (int t = 0; t < NT; ++t) acc[t] = 0.0;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i0 = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i0 < p.n; i0 += U * stride) {
+        I i[U];
+        bool in[U];
+        double2 v[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            in[u] = i0 + u * stride < p.n;
+            i[u] = (I)(in[u] ? i0 + u * stride : i0);
+            v[u] = widen<R>(a[i[u]]);
+        }
+        double zr[U], zi[U];  // conj(v) * partner
+#pragma unroll
+        for (int u = 0; u < U; ++u) zr[u] = zi[u] = 0.0;
+#pragma unroll
+        for (int t = 0; t < NT; ++t) {
+            if (t < p.nterms) {
+                const I x = (I)p.xmask[t], z = (I)p.zmask[t];
+                if (p.newx[t]) {
+                    double2 w[U];
+#pragma unroll
+                    for (int u = 0; u < U; ++u) w[u] = x ? widen<R>(a[i[u] ^ x]) : v[u];
+#pragma unroll
+                    for (int u = 0; u < U; ++u) {
+                        zr[u] = v[u].x * w[u].x + v[u].y * w[u].y;
+                        zi[u] = v[u].x * w[u].y - v[u].y * w[u].x;
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const double r = fma(p.cr[t], zr[u], p.ci[t] * zi[u]);
+                    const I m = (i[u] ^ x) & z;
+                    const int odd = (sizeof(I) == 8 ? __popcll((uint64_t)m) : __popc((uint32_t)m)) & 1;
+                    acc[t] += in[u] ? (odd ? -r : r) : 0.0;
+                }
+            }
+        }
+    }
+    block_reduce<NT>(acc, sm);
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int t = 0; t < NT; ++t)
+            if (t < p.nterms) partials[(size_t)t * gridDim.x + blockIdx.x] = acc[t];
+    }
+}
+
 template <typename R>
 void reduce_pauli_group(const void *psi, uint32_t nq, const PauliWord *terms, int nterms, double *partials,
-                        double *out, cudaStream_t st) {
+                        double *out, cudaStream_t st, bool with_norm) {
     if (nterms <= 0) return;
     if (nterms > 32) throw ArgError("at most 32 Pauli words per group");
     PauliGroupP p{};
     p.xmask = terms[0].xmask;
     p.nterms = nterms;
+    p.norm = with_norm ? 1 : 0;
     for (int t = 0; t < nterms; ++t) {
         if (terms[t].xmask != p.xmask) throw ArgError("Pauli group with mixed X masks");
         p.zmask[t] = terms[t].zmask;
-        p.ny[t] = terms[t].ny;
+        const int ny = terms[t].ny & 3;  // Re(i^ny z): z.re, -z.im, -z.re, z.im
+        p.cr[t] = ny == 0 ? 1.0 : ny == 2 ? -1.0 : 0.0;
+        p.ci[t] = ny == 1 ? -1.0 : ny == 3 ? 1.0 : 0.0;
     }
     const uint64_t n = uint64_t(1) << nq;
     if (p.xmask) {
@@ -429,8 +590,38 @@ void reduce_pauli_group(const void *psi, uint32_t nq, const PauliWord *terms, in
     else if (nterms <= 8) k_pauli<R, 8><<<nb, kRT, 0, st>>>(a, p, partials);
     else k_pauli<R, 32><<<nb, kRT, 0, st>>>(a, p, partials);
     B200SV_CUDA(cudaGetLastError());
+    finalize(partials, nb, nterms + (with_norm ? 1 : 0), out, 1, 1.0, st);
+}
+
+template <typename R>
+void reduce_pauli_multi(const void *psi, uint32_t nq, const PauliWord *terms, int nterms, double *partials,
+                        double *out, cudaStream_t st) {
+    if (nterms <= 0) return;
+    if (nterms > 32) throw ArgError("at most 32 Pauli words per pass");
+    PauliMultiP p{};
+    p.n = uint64_t(1) << nq;
+    p.nterms = nterms;
+    for (int t = 0; t < nterms; ++t) {
+        p.xmask[t] = terms[t].xmask;
+        p.zmask[t] = terms[t].zmask;
+        const int ny = terms[t].ny & 3;  // Re(i^ny z): z.re, -z.im, -z.re, z.im
+        p.cr[t] = ny == 0 ? 1.0 : ny == 2 ? -1.0 : 0.0;
+        p.ci[t] = ny == 1 ? -1.0 : ny == 3 ? 1.0 : 0.0;
+        p.newx[t] = (t == 0 || terms[t].xmask != terms[t - 1].xmask) ? 1 : 0;
+    }
+    const int nb = red_blocks(p.n);
+    const C<R> *a = static_cast<const C<R> *>(psi);
+    if (nq <= 32) {
+        if (nterms <= 8) k_pauli_multi<R, 8, uint32_t><<<nb, kRT, 0, st>>>(a, p, partials);
+        else k_pauli_multi<R, 32, uint32_t><<<nb, kRT, 0, st>>>(a, p, partials);
+    } else {
+        if (nterms <= 8) k_pauli_multi<R, 8, uint64_t><<<nb, kRT, 0, st>>>(a, p, partials);
+        else k_pauli_multi<R, 32, uint64_t><<<nb, kRT, 0, st>>>(a, p, partials);
+    }
+    B200SV_CUDA(cudaGetLastError());
     finalize(partials, nb, nterms, out, 1, 1.0, st);
 }
+
 
 template <typename R>
 void reduce_dense_expval(const void *psi, uint32_t nq, const GateDesc &g, const void *dev_matrix, double *partials,
@@ -451,8 +642,13 @@ void reduce_dense_expval(const void *psi, uint32_t nq, const GateDesc &g, const 
     B200SV_CUDA(cudaMemcpyAsync(const_cast<void *>(dev_matrix), hm.data(), hm.size() * sizeof(C<R>),
                                 cudaMemcpyHostToDevice, st));
     const int nb = red_blocks(p.ngroups);
-    k_dense_ev<R><<<nb, kRT, 0, st>>>(static_cast<const C<R> *>(psi), p, static_cast<const C<R> *>(dev_matrix),
-                                      partials);
+    const C<R> *a = static_cast<const C<R> *>(psi), *m = static_cast<const C<R> *>(dev_matrix);
+    switch (g.k) {
+    case 1: k_dense_ev<R, 1><<<nb, kRT, 0, st>>>(a, p, m, partials); break;
+    case 2: k_dense_ev<R, 2><<<nb, kRT, 0, st>>>(a, p, m, partials); break;
+    case 3: k_dense_ev<R, 3><<<nb, kRT, 0, st>>>(a, p, m, partials); break;
+    default: k_dense_ev<R, 4><<<nb, kRT, 0, st>>>(a, p, m, partials); break;
+    }
     B200SV_CUDA(cudaGetLastError());
     finalize(partials, nb, 1, out, 1, 1.0, st);
 }
@@ -464,7 +660,7 @@ void reduce_generator_inner_complex(const void *bra, const void *ket, uint32_t n
                                     double *partials, double *out2, cudaStream_t st) {
     GenP<R> p = make_genp<R>(nq, g);
     const int nb = red_blocks(p.ngroups);
-    k_gen_inner_c<R><<<nb, kRT, 0, st>>>(static_cast<const C<R> *>(bra), static_cast<const C<R> *>(ket), p, partials);
+    with_gen_form<R>(p, GoGenC<R>{nb, st, static_cast<const C<R> *>(bra), static_cast<const C<R> *>(ket), p, partials});
     B200SV_CUDA(cudaGetLastError());
     finalize(partials, nb, 2, out2, 1, 1.0, st);
 }
@@ -509,9 +705,7 @@ void reduce_generator_inner(void *const *bras, int nbra, const void *ket, uint32
     for (int o = 0; o < nbra; ++o) B.p[o] = static_cast<const C<R> *>(bras[o]);
     const int nb = red_blocks(p.ngroups);
     const C<R> *k = static_cast<const C<R> *>(ket);
-    if (nbra == 1) k_gen_inner<R, 1><<<nb, kRT, 0, st>>>(B, nbra, k, p, partials);
-    else if (nbra <= 4) k_gen_inner<R, 4><<<nb, kRT, 0, st>>>(B, nbra, k, p, partials);
-    else k_gen_inner<R, 16><<<nb, kRT, 0, st>>>(B, nbra, k, p, partials);
+    with_gen_form<R>(p, GoGen<R>{nb, nbra, st, B, k, p, partials});
     B200SV_CUDA(cudaGetLastError());
     finalize(partials, nb, nbra, out, out_stride, alpha, st);
 }
@@ -574,6 +768,8 @@ template <typename R> void axpy(void *acc, const void *x, uint32_t nq, double c,
     template void reduce_norm2<R>(const void *, uint32_t, double *, double *, cudaStream_t);                    \
     template void reduce_inner<R>(const void *, const void *, uint32_t, double *, double *, cudaStream_t);      \
     template void reduce_pauli_group<R>(const void *, uint32_t, const PauliWord *, int, double *, double *,     \
+                                        cudaStream_t, bool);                                                    \
+    template void reduce_pauli_multi<R>(const void *, uint32_t, const PauliWord *, int, double *, double *,     \
                                         cudaStream_t);                                                          \
     template void reduce_dense_expval<R>(const void *, uint32_t, const GateDesc &, const void *, double *,      \
                                          double *, cudaStream_t);                                               \
