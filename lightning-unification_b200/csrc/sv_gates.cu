@@ -386,7 +386,7 @@ __global__ void __launch_bounds__(kThreads) k_parity(States s, ParityP<R> p) {
          i += (uint64_t)gridDim.x * blockDim.x) {
         const C<R> v = sv[i];
         CAcc<R> a;
-        a.add(p.ph[__popcll(i & p.mask) & 1], v);
+        a.add((__popcll(i & p.mask) & 1) ? p.ph[1] : p.ph[0], v);  // a select: an index would copy ph to local memory
         sv[i] = a.get();
     }
 }

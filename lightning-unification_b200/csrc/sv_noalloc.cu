@@ -91,8 +91,11 @@ __global__ void __launch_bounds__(kNoAllocThreads) k_words(const C<R> *__restric
         }
     }
     block_reduce<NT>(acc, sm);
-    if (threadIdx.x == 0)
-        for (int t = 0; t < p.nterms; ++t) partials[(size_t)t * gridDim.x + blockIdx.x] = acc[t];
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int t = 0; t < NT; ++t)  // constant indices keep acc in registers
+            if (t < p.nterms) partials[(size_t)t * gridDim.x + blockIdx.x] = acc[t];
+    }
 }
 
 // Second pass: out[t] = sum_b partials[t, b] in a fixed order.
