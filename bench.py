@@ -358,6 +358,12 @@ def matrix_sweep(nq: int, hbm_peak: float, kmax: int = 7, steps: int = 3):
 # grows in proportion to the state.
 RX_DRAM_BYTES_26Q = 1.0737e9 + 1.0137e9
 
+# DRAM bytes (read + write) of the forward and VJP launches of the batched kernel on 148
+# circuits of the batched-adjoint workload, from an ncu capture (profiles/k_batch_c64_148circ.md);
+# circuits are independent, so a step's traffic scales with the number of circuits.
+BATCH_DRAM_BYTES_148 = (0.0704e9 + 0.9838e9) + (3.1382e9 + 3.5036e9)
+BATCH_ISSUE_ACTIVE = 0.53  # scheduler cycles issuing, same capture (forward 51 %, VJP 53 %)
+
 
 def run_case(args):
     """Small single-kernel cases for profiling: `gate` applies RX to a complex128 state of
@@ -782,6 +788,14 @@ def main():
         "sampling": samp,
         "plain_20q_layered": plain20,
         "roofline": roof,
+        "roofline_batch": {
+            "kernel": "k_batch<float,0|1,false> (forward + VJP launch of the headline step)",
+            "bound": "issue", "hbm_traffic_per_step": BATCH_DRAM_BYTES_148 * ncirc / 148,
+            "hbm_achieved_gbs": BATCH_DRAM_BYTES_148 * ncirc / 148 / (ms * 1e6),
+            "hbm_frac": BATCH_DRAM_BYTES_148 * ncirc / 148 / (ms * 1e6) / hbm_peak, "peak_kind": peak_kind,
+            "issue_active_frac": BATCH_ISSUE_ACTIVE,
+            "note": "per-circuit states stay in shared memory within a segment; the kernel is bound by "
+                    "instruction issue and latency (ncu: FMA pipe 20-23 %, shared memory 42-49 %), not by HBM"},
         "cpu_baseline": cpu,
         "e2e": {"value": aggregate_rate(world, ncirc, e2e_ms), "unit": "circuits/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
