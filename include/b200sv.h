@@ -188,6 +188,10 @@ int b200sv_probs(b200sv_handle h, const uint32_t *wires, uint32_t nwires,
 /* Device-side variant: writes 2^nwires doubles to a device buffer. */
 int b200sv_probs_device(b200sv_handle h, const uint32_t *wires,
                         uint32_t nwires, double *out_device);
+/* psi <- O psi in place (Observable::applyInPlace, CS/observables/Observables.hpp:63-73;
+ * Hamiltonian::applyInPlace, LQ/observables/ObservablesLQubit.hpp:156-305: the sum of
+ * coeff * term applied to copies of psi).  O need not be unitary, so psi is not renormalised. */
+int b200sv_apply_observable(b200sv_handle h, const b200sv_observable *obs);
 /* <psi|O|psi> for an observable (expval(Observable), :248-265). */
 int b200sv_expval(b200sv_handle h, const b200sv_observable *obs, double *out);
 /* <O^2> - <O>^2 as ||O psi||^2 - <psi|O psi>^2 (var(Observable), :273-372). */

@@ -35,6 +35,9 @@ template <class StateVectorT> class Observable {
     // Terms of this observable (a Hamiltonian has several, the others one).
     [[nodiscard]] virtual std::vector<TermData<PrecisionT>> terms() const = 0;
     [[nodiscard]] bool operator==(const Observable &o) const { return getObsName() == o.getObsName() && same(o); }
+    // sv <- O sv (Observables.hpp:63-73; a Hamiltonian sums coeff * term over copies of sv,
+    // ObservablesLQubit.hpp:156-305), on the device
+    void applyInPlace(StateVectorT &sv) const;
 
   protected:
     [[nodiscard]] virtual bool same(const Observable &o) const = 0;
@@ -213,5 +216,10 @@ template <class PrecisionT> class ObsRecord {
     }
     ObsRecord(const ObsRecord &) = delete;
 };
+
+template <class StateVectorT> void Observable<StateVectorT>::applyInPlace(StateVectorT &sv) const {
+    ObsRecord<PrecisionT> r(terms());
+    check(b200sv_apply_observable(sv.handle(), &r.rec));
+}
 
 }  // namespace Pennylane::LightningB200

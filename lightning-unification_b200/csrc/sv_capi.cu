@@ -674,6 +674,19 @@ int b200sv_probs(b200sv_handle h, const uint32_t *wires, uint32_t nwires, double
     });
 }
 
+int b200sv_apply_observable(b200sv_handle h, const b200sv_observable *obs) {
+    return guard([&] {
+        check_handle(h);
+        need(obs != nullptr, "NULL observable");
+        DeviceGuard dg(h->device);
+        const ObsRec o = read_obs(*obs, h->nq, h->dtype);
+        void *out = scratch(h, 0);
+        void *tmp = o.terms.size() > 1 ? scratch(h, 1) : nullptr;
+        apply_observable(h, o, h->d_state, out, tmp);
+        B200SV_CUDA(cudaMemcpyAsync(h->d_state, out, h->state_bytes(), cudaMemcpyDeviceToDevice, h->stream()));
+    });
+}
+
 int b200sv_expval(b200sv_handle h, const b200sv_observable *obs, double *out) {
     return guard([&] {
         check_handle(h);

@@ -119,6 +119,7 @@ _SIGS = {
                                 C.POINTER(C.c_double)], C.c_int),
     "b200sv_probs": ([C.c_void_p, C.POINTER(C.c_uint32), C.c_uint32, C.POINTER(C.c_double)], C.c_int),
     "b200sv_probs_device": ([C.c_void_p, C.POINTER(C.c_uint32), C.c_uint32, C.c_void_p], C.c_int),
+    "b200sv_apply_observable": ([C.c_void_p, C.POINTER(Observable)], C.c_int),
     "b200sv_expval": ([C.c_void_p, C.POINTER(Observable), C.POINTER(C.c_double)], C.c_int),
     "b200sv_var": ([C.c_void_p, C.POINTER(Observable), C.POINTER(C.c_double)], C.c_int),
     "b200sv_expval_pauli": ([C.c_void_p, C.c_uint32, C.POINTER(C.c_double), C.POINTER(C.c_uint32),
@@ -378,6 +379,11 @@ class StateVector:
         w, wp = _u32(wires)
         check(lib().b200sv_probs(self.h, wp, len(w), out.ctypes.data_as(C.POINTER(C.c_double))))
         return out
+
+    def apply_observable(self, terms):
+        """psi <- O psi (Observable::applyInPlace); terms as for expval."""
+        ob = ObservableBuilder(terms, self.np_dtype)
+        check(lib().b200sv_apply_observable(self.h, C.byref(ob.obs)))
 
     def expval(self, terms) -> float:
         ob = ObservableBuilder(terms, self.np_dtype)

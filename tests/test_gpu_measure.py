@@ -89,6 +89,58 @@ def test_pauli_sums_and_hamiltonians(capi, dtype):
         assert abs(sv.var(terms) - O.var(st64, terms)) < tol * 100
 
 
+@pytest.mark.parametrize("dtype", [np.complex128, np.complex64])
+def test_pauli_passes_near_and_far(capi, dtype):
+    """Pauli sums at 20 qubits, where X masks on the two highest wires (state bits 19, 18) lie
+    beyond the shared passes' 4 MiB reach and get pair passes: 70 words (several passes of
+    each kind, more than 8 X masks), and single-word variances on an unnormalised state
+    (the norm comes from the same pass)."""
+    import lq_oracle as O
+    rng = np.random.default_rng(21)
+    n = 20
+    st = (random_state(rng, n, dtype) * 1.3).astype(dtype)
+    sv = capi.StateVector(n, dtype)
+    sv.upload(st)
+    st64 = st.astype(np.complex128)
+    letters = "XYZ"
+    words = [("ZZ", [q, (q + 1) % n]) for q in range(n)] + [("X", [q]) for q in range(n)]
+    for _ in range(30):
+        k = int(rng.integers(1, 4))
+        ws = [int(w) for w in rng.choice(n, k, replace=False)]
+        words.append(("".join(letters[int(rng.integers(3))] for _ in ws), ws))
+    coeffs = rng.normal(size=len(words))
+    per, tot = sv.expval_pauli(words, coeffs)
+    want = [O.pauli_expval(st64, wd, ws) for wd, ws in words]
+    tol = 1e-11 if dtype == np.complex128 else 1e-5
+    assert np.abs(per - want).max() < tol
+    assert abs(tot - float(np.dot(coeffs, want))) < tol * 10
+    names = {"X": "PauliX", "Y": "PauliY", "Z": "PauliZ"}
+    for wd, ws in (("X", [0]), ("Y", [1]), ("Z", [5]), ("XY", [0, 19]), ("Y", [19])):
+        terms = [(0.7, [(names[c], [w]) for c, w in zip(wd, ws)])]
+        assert abs(sv.var(terms) - O.var(st64, terms)) < tol * 10
+
+
+@pytest.mark.parametrize("dtype", [np.complex128, np.complex64])
+def test_apply_observable_in_place(capi, dtype):
+    """psi <- O psi (Observable::applyInPlace): named, tensor, Hermitian and Hamiltonian."""
+    import lq_oracle as O
+    rng = np.random.default_rng(8)
+    n = 9
+    st = random_state(rng, n, dtype)
+    herm = rng.normal(size=(4, 4)) + 1j * rng.normal(size=(4, 4))
+    herm = herm + herm.conj().T
+    tol = 1e-12 if dtype == np.complex128 else 2e-5
+    for terms in ([(1.0, [("PauliY", [4])])], [(1.0, [("PauliX", [0]), ("PauliZ", [8])])],
+                  [(1.0, [("Hermitian", [2, 6], herm)])],
+                  [(0.5, [("PauliZ", [1]), ("PauliZ", [2])]), (-1.5, [("PauliX", [3])]),
+                   (2.0, [("Hermitian", [2, 6], herm)])]):
+        sv = capi.StateVector(n, dtype)
+        sv.upload(st)
+        sv.apply_observable(terms)
+        want = O.apply_observable(st.astype(np.complex128), terms)
+        assert np.abs(sv.download() - want).max() < tol * (1 + np.abs(want).max())
+
+
 def test_inner_product_norm(capi):
     rng = np.random.default_rng(6)
     n = 12
