@@ -270,9 +270,10 @@ void apply_observable(b200sv_state *h, const ObsRec &o, const void *psi, void *o
 }
 
 // per-term Pauli values of an all-Pauli observable (host vector, term order).  Words sorted by
-// X mask.  Words whose X mask stays below 4 MiB of amplitudes (and the diagonal ones) share
-// passes of reduce_pauli_multi, up to 32 per pass, their partner amplitudes coming from L2;
-// each wider X mask gets pair passes of reduce_pauli_group, where a thread reads both
+// X mask.  Diagonal words (two or more, 10+ qubits) share Walsh-Hadamard passes of
+// reduce_pauli_diag, up to 256 per pass.  Words whose X mask stays below 4 MiB of amplitudes
+// share passes of reduce_pauli_multi, up to 32 per pass, their partner amplitudes coming from
+// L2; each wider X mask gets pair passes of reduce_pauli_group, where a thread reads both
 // amplitudes of a pair, so the state crosses HBM once per pass either way.
 std::vector<double> pauli_term_values(b200sv_state *h, const void *psi, const std::vector<PauliWord> &words) {
     const cudaStream_t st = h->stream();
@@ -284,9 +285,18 @@ std::vector<double> pauli_term_values(b200sv_state *h, const void *psi, const st
     struct Pass {
         size_t begin, count;
         bool multi;
+        bool diag = false;
     };
     std::vector<Pass> passes;
     size_t i = 0;
+    // diagonal words (sorted first): Walsh-Hadamard passes, any number of words per read
+    size_t ndiag = 0;
+    while (ndiag < order.size() && words[order[ndiag]].xmask == 0) ++ndiag;
+    const bool diag_pass = h->nq >= 10 && ndiag >= 2;
+    if (diag_pass) {
+        for (size_t d = 0; d < ndiag; d += 256) passes.push_back(Pass{d, std::min<size_t>(256, ndiag - d), true, true});
+        i = ndiag;
+    }
     while (i < order.size() && words[order[i]].xmask < near) {
         // up to 32 words and 8 distinct X masks per pass: each mask adds a partner read per
         // amplitude, so wider passes cost as much as pair passes
@@ -316,6 +326,22 @@ std::vector<double> pauli_term_values(b200sv_state *h, const void *psi, const st
             std::vector<PauliWord> grp;
             for (size_t q = 0; q < ps.count; ++q) grp.push_back(words[order[ps.begin + q]]);
             const int cnt = (int)ps.count;
+            if (ps.diag) {
+                // the Z masks ride at the end of the partials buffer, past what the pass uses
+                std::vector<uint64_t> zm(ps.count);
+                for (size_t q = 0; q < ps.count; ++q) zm[q] = grp[q].zmask;
+                uint64_t *dz = reinterpret_cast<uint64_t *>(h->d_partials + kPartialsCapacity - 256);
+                B200SV_CUDA(cudaMemcpyAsync(dz, zm.data(), zm.size() * sizeof(uint64_t), cudaMemcpyHostToDevice, st));
+                if (h->dtype == B200SV_C64)
+                    reduce_pauli_diag<float>(psi, h->nq, dz, cnt, h->d_partials, kPartialsCapacity - 256,
+                                             h->d_small + batch, st);
+                else
+                    reduce_pauli_diag<double>(psi, h->nq, dz, cnt, h->d_partials, kPartialsCapacity - 256,
+                                              h->d_small + batch, st);
+                batch += ps.count;
+                ++pi;
+                continue;
+            }
             if (h->dtype == B200SV_C64) {
                 if (ps.multi) reduce_pauli_multi<float>(psi, h->nq, grp.data(), cnt, h->d_partials, h->d_small + batch, st);
                 else reduce_pauli_group<float>(psi, h->nq, grp.data(), cnt, h->d_partials, h->d_small + batch, st);

@@ -626,7 +626,14 @@ int fused_tile_bits(int dtype, uint32_t nq) {
     return (int)std::min<uint32_t>(kt, nq);
 }
 
-bool fused_worthwhile(int dtype, uint32_t nq) { return nq >= (uint32_t)fused_tile_bits(dtype, nq) + 8; }
+// Below 21 qubits (2^8 / 2^9 tiles) a segment has too few tiles to fill 148 SMs and one
+// launch per gate is faster: on a 200-gate random sweep at 20 qubits complex128, 1.5 ms per
+// gate launch against 3.9 ms fused; from 21 qubits on (L2-resident or not) the fused path
+// wins on deep circuits (a 10-layer RX RY RZ + CNOT circuit: 4.2 vs 7.8 ms at 21 qubits,
+// 89 vs 334 ms at 26).
+bool fused_worthwhile(int dtype, uint32_t nq) {
+    return nq >= (uint32_t)fused_tile_bits(dtype, nq) + (dtype == B200SV_C64 ? 8 : 9);
+}
 
 void apply_fused(void *state, uint32_t nq, int dtype, const std::vector<GateDesc> &descs,
                  const std::function<void(const GateDesc &)> &apply_single, cudaStream_t st) {

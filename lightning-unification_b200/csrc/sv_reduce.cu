@@ -593,6 +593,98 @@ void reduce_pauli_group(const void *psi, uint32_t nq, const PauliWord *terms, in
     finalize(partials, nb, nterms + (with_norm ? 1 : 0), out, 1, 1.0, st);
 }
 
+// ---- diagonal Pauli words (Z and I factors only), any number in one pass -----------------
+// Per tile of 1024 consecutive amplitudes (state bits 0-9), the Walsh-Hadamard transform of
+// the probabilities, W[k] = sum_m (-1)^popcount(m & k) p_(base + m), holds every diagonal
+// word's restriction to the tile: <Z_z> gains (-1)^popcount(tile & (z >> 10)) W[z & 1023].
+// The transform costs ten FP64 additions per amplitude whatever the number of words (bits
+// 0-1 in registers, 2-6 across lanes with shuffles, 7-9 across warps in shared memory, in a
+// fixed order); thread t then accumulates word t.  256 threads, four amplitudes each.
+constexpr int kDiagThreads = 256;
+constexpr int kDiagMaxWords = 256;
+struct PauliDiagP {
+    uint64_t ntiles;
+    int nwords;
+};
+template <typename R>
+__global__ void __launch_bounds__(kDiagThreads) k_pauli_diag(const C<R> *__restrict__ a, PauliDiagP p,
+                                                             const uint64_t *__restrict__ zmask, double *partials) {
+    __shared__ double w[1024];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const bool has_word = tid < p.nwords;
+    const uint64_t z = has_word ? zmask[tid] : 0;
+    const uint32_t zlo = (uint32_t)(z & 1023u);
+    const uint64_t zhi = z >> 10;
+    double acc = 0.0;
+    for (uint64_t t = blockIdx.x; t < p.ntiles; t += gridDim.x) {
+        const C<R> *src = a + (t << 10) + 4 * tid;
+        double v[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const double2 x = widen<R>(src[j]);
+            v[j] = x.x * x.x + x.y * x.y;
+        }
+        // bits 0, 1: in registers
+        {
+            const double a0 = v[0] + v[1], a1 = v[0] - v[1], a2 = v[2] + v[3], a3 = v[2] - v[3];
+            v[0] = a0 + a2;
+            v[1] = a1 + a3;
+            v[2] = a0 - a2;
+            v[3] = a1 - a3;
+        }
+        // bits 2-6: lane bits 0-4
+#pragma unroll
+        for (int s = 0; s < 5; ++s) {
+            const bool hi = (lane >> s) & 1;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const double o = __shfl_xor_sync(0xffffffffu, v[j], 1 << s);
+                v[j] = hi ? o - v[j] : v[j] + o;
+            }
+        }
+        // bits 7-9: warp bits 0-2, through shared memory
+        __syncthreads();  // the previous tile's words have read w
+#pragma unroll
+        for (int s = 0; s < 3; ++s) {
+#pragma unroll
+            for (int j = 0; j < 4; ++j) w[4 * tid + j] = v[j];
+            __syncthreads();
+            const bool hi = (warp >> s) & 1;
+            const int partner = 4 * (tid ^ (32 << s));
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const double o = w[partner + j];
+                v[j] = hi ? o - v[j] : v[j] + o;
+            }
+            __syncthreads();
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j) w[4 * tid + j] = v[j];
+        __syncthreads();
+        if (has_word) {
+            const double x = w[zlo];
+            acc += (__popcll(t & zhi) & 1) ? -x : x;
+        }
+    }
+    if (has_word) partials[(size_t)tid * gridDim.x + blockIdx.x] = acc;
+}
+
+template <typename R>
+void reduce_pauli_diag(const void *psi, uint32_t nq, const uint64_t *zmask_dev, int nwords, double *partials,
+                       size_t partials_cap, double *out, cudaStream_t st) {
+    if (nwords <= 0) return;
+    if (nwords > kDiagMaxWords) throw ArgError("at most 256 diagonal Pauli words per pass");
+    if (nq < 10) throw Unsupported("diagonal Pauli pass needs at least 10 qubits");
+    PauliDiagP p{};
+    p.ntiles = uint64_t(1) << (nq - 10);
+    p.nwords = nwords;
+    const uint64_t cap = std::min<uint64_t>(kMaxRedBlocks, partials_cap / (size_t)nwords);
+    const int nb = (int)std::max<uint64_t>(1, std::min<uint64_t>(p.ntiles, cap));
+    k_pauli_diag<R><<<nb, kDiagThreads, 0, st>>>(static_cast<const C<R> *>(psi), p, zmask_dev, partials);
+    B200SV_CUDA(cudaGetLastError());
+    finalize(partials, nb, nwords, out, 1, 1.0, st);
+}
+
 template <typename R>
 void reduce_pauli_multi(const void *psi, uint32_t nq, const PauliWord *terms, int nterms, double *partials,
                         double *out, cudaStream_t st) {
@@ -769,6 +861,8 @@ template <typename R> void axpy(void *acc, const void *x, uint32_t nq, double c,
     template void reduce_inner<R>(const void *, const void *, uint32_t, double *, double *, cudaStream_t);      \
     template void reduce_pauli_group<R>(const void *, uint32_t, const PauliWord *, int, double *, double *,     \
                                         cudaStream_t, bool);                                                    \
+    template void reduce_pauli_diag<R>(const void *, uint32_t, const uint64_t *, int, double *, size_t,         \
+                                       double *, cudaStream_t);                                                 \
     template void reduce_pauli_multi<R>(const void *, uint32_t, const PauliWord *, int, double *, double *,     \
                                         cudaStream_t);                                                          \
     template void reduce_dense_expval<R>(const void *, uint32_t, const GateDesc &, const void *, double *,      \

@@ -303,13 +303,15 @@ class LightningQubit:
                 raise DeviceError(f"Operation {op.name} cannot be used after other "
                                   f"Operations have already been applied on a {self.short_name} device.")
         ops = [op for op in operations if op.name != "Identity"]
+        # the fused apply: one pass over the state per run of gates that fit a shared-memory
+        # tile on wide states, one launch per gate on narrow ones (same results to rounding)
         if ops:
-            self._sv.apply_ops(self._serialize_ops(ops))
+            self._sv.apply_ops_fused(self._serialize_ops(ops))
         if rotations:
             if self._rot is None:
                 self._rot = capi.StateVector(self.num_wires, self.C_DTYPE)
             self._rot.copy_from(self._sv)
-            self._rot.apply_ops(self._serialize_ops(rotations))
+            self._rot.apply_ops_fused(self._serialize_ops(rotations))
         else:
             if self._rot is not None:
                 self._rot.close()
