@@ -325,7 +325,7 @@ def rows_30q(nq: int, hbm_peak: float, cpu: bool, cpu_qubits: int = 26, steps: i
     return out
 
 
-def matrix_sweep(nq: int, hbm_peak: float, kmax: int = 7, steps: int = 3):
+def matrix_sweep(nq: int, hbm_peak: float, kmax: int = 8, steps: int = 3):
     """applyMatrix of random k-wire unitaries (k = 1..kmax, seeded wires) on an nq-qubit state,
     complex128 and complex64: ms per launch, HBM GB/s (2 x bytes of the state) and the matrix
     arithmetic in TFLOP/s (8 * 2^k real flops per amplitude).  Dense blocks cross from the

@@ -162,7 +162,7 @@ __global__ void __launch_bounds__(kThreads) k_dense_dev(States s, DenseDevP<R, K
     }
 }
 
-// Dense blocks on K = 5..7 target bits (compute-bound from K = 5 in FP64): a register-tiled
+// Dense blocks on K = 5..10 target bits (compute-bound from K = 5 in FP64): a register-tiled
 // complex matrix product.  Each CTA takes tiles of 4096 amplitudes — TG = 4096 / 2^K
 // consecutive groups times all 2^K rows — staged in shared memory with coalesced loads
 // (consecutive threads take consecutive groups), and each thread accumulates a 4 x 4 block
@@ -263,7 +263,7 @@ __global__ void __launch_bounds__(kTiledThreads, 2) k_dense_tiled(States s, Tile
     }
 }
 
-// Large dense blocks (k = 8..11, and 7 on states under 12 qubits): one CTA per group, the
+// Large dense blocks (k = 11, and 7..10 on states under 12 qubits): one CTA per group, the
 // group staged in shared memory.
 struct BigDenseP {
     Insert ins;
@@ -499,7 +499,18 @@ void launch_gate(void *const *states, int nstates, uint32_t nq, const GateDesc &
         case 5: launch_dense_k<R, 5>(S, nstates, nq, g, scratch, st); break;
         case 6: launch_dense_k<R, 6>(S, nstates, nq, g, scratch, st); break;
         case 7:
-            if (launch_dense_k<R, 7>(S, nstates, nq, g, scratch, st)) break;
+        case 8:
+        case 9:
+        case 10: {
+            bool done = false;
+            switch (g.k) {
+            case 7: done = launch_dense_k<R, 7>(S, nstates, nq, g, scratch, st); break;
+            case 8: done = launch_dense_k<R, 8>(S, nstates, nq, g, scratch, st); break;
+            case 9: done = launch_dense_k<R, 9>(S, nstates, nq, g, scratch, st); break;
+            default: done = launch_dense_k<R, 10>(S, nstates, nq, g, scratch, st); break;
+            }
+            if (done) break;
+        }
             [[fallthrough]];
         default: {
             if (g.k > 11 || !g.cbits.empty()) throw Unsupported("dense matrices act on at most 11 wires");

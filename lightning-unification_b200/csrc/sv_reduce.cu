@@ -3,8 +3,9 @@
 // The reference computes every expectation value by copying the state, applying
 // the observable and taking innerProdC (LQ/measurements/MeasurementsLQubit.hpp:145-180,
 // :248-265; LQ/utils/LinearAlgebra.hpp:151-213): three full passes per term.
-// Here a Pauli word is evaluated in one read-only pass (all words sharing an
-// X-mask together), a Hermitian matrix as v^dagger M v per group, and the
+// Here Pauli words are evaluated in read-only passes (diagonal words together through a
+// Walsh-Hadamard transform per tile, words with nearby X masks together, each distant X mask
+// in a pass over its amplitude pairs), a Hermitian matrix as v^dagger M v per group, and the
 // adjoint method's -2 Im<H lambda| G |mu> (LQ/algorithms/AdjointJacobianLQubit.hpp:68-77,
 // :301-323) without materialising G|mu>.  All accumulators are FP64 (complex64
 // amplitudes are widened on load) and every reduction is two-pass with a fixed

@@ -104,9 +104,9 @@ def test_apply_matrix(capi, k, dtype):
 
 
 @pytest.mark.parametrize("dtype", [np.complex128, np.complex64])
-@pytest.mark.parametrize("k", [4, 5, 6, 7])
+@pytest.mark.parametrize("k", [4, 5, 6, 7, 8, 10])
 def test_apply_matrix_tiled(capi, k, dtype):
-    """Matrices on 4..7 wires of a state wide enough for the tiled kernel (tiles of 4096
+    """Matrices on 4..10 wires of a state wide enough for the tiled kernel (tiles of 4096
     amplitudes), wires in the lowest, highest and scattered positions."""
     import lq_oracle as O
     from lightning_b200.workloads import random_unitary
