@@ -139,7 +139,8 @@ int b200sv_num_qubits(b200sv_handle h, uint32_t *out);
 int b200sv_dtype(b200sv_handle h, int *out);
 /* Run the handle's work on `cuda_stream` from now on (e.g. torch's current
  * stream).  NULL selects the legacy default stream, which torch uses unless told
- * otherwise.  Until the first call the handle runs on a private stream. */
+ * otherwise.  Until the first call the handle runs on a private stream.  When the
+ * stream changes, the call waits for the work already issued on the previous one. */
 int b200sv_set_stream(b200sv_handle h, void *cuda_stream);
 int b200sv_synchronize(b200sv_handle h);
 /* Device address of the amplitudes (complex<T>[2^n]) for zero-copy interop. */

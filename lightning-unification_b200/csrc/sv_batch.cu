@@ -2034,6 +2034,9 @@ int b200sv_batch_destroy(b200sv_batch_handle b) {
 int b200sv_batch_set_stream(b200sv_batch_handle b, void *s) {
     return run_guarded([&] {
         if (!b) throw ArgError("NULL batch");
+        // on a change of stream, the work issued on the previous one completes first
+        if (!b->b->has_ext || b->b->ext != static_cast<cudaStream_t>(s))
+            B200SV_CUDA(cudaStreamSynchronize(b->b->stream()));
         b->b->ext = static_cast<cudaStream_t>(s);
         b->b->has_ext = true;  // instantiated graphs launch on any stream
     });

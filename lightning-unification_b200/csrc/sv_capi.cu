@@ -23,7 +23,8 @@ struct b200sv_state {
     cudaStream_t ext = nullptr;
     bool has_ext = false;          // set_stream called: ext (NULL = legacy default stream)
     void *d_state = nullptr;
-    double *d_partials = nullptr;  // kPartialsCapacity doubles
+    double *d_partials = nullptr;  // kPartialsCapacity doubles, then the arrival counter
+    unsigned int *arrival() const { return reinterpret_cast<unsigned int *>(d_partials + kPartialsCapacity); }
     double *d_small = nullptr;     // small results (kSmall doubles)
     double *h_small = nullptr;     // pinned mirror of d_small
     void *d_matrix = nullptr;      // dense matrix staging
@@ -470,7 +471,8 @@ int b200sv_create(uint32_t num_qubits, int dtype, b200sv_handle *out) {
         try {
             B200SV_CUDA(cudaStreamCreateWithFlags(&h->own, cudaStreamNonBlocking));
             B200SV_CUDA(cudaMalloc(&h->d_state, h->state_bytes()));
-            B200SV_CUDA(cudaMalloc(&h->d_partials, kPartialsCapacity * sizeof(double)));
+            B200SV_CUDA(cudaMalloc(&h->d_partials, (kPartialsCapacity + 1) * sizeof(double)));
+            B200SV_CUDA(cudaMemsetAsync(h->arrival(), 0, sizeof(double), h->own));
             B200SV_CUDA(cudaMalloc(&h->d_small, kSmall * sizeof(double)));
             B200SV_CUDA(cudaMallocHost(&h->h_small, kSmall * sizeof(double)));
             if (dtype == B200SV_C64) set_basis<float>(h->d_state, num_qubits, 0, h->own);
@@ -521,6 +523,10 @@ int b200sv_dtype(b200sv_handle h, int *out) {
 int b200sv_set_stream(b200sv_handle h, void *s) {
     return guard([&] {
         check_handle(h);
+        DeviceGuard dg(h->device);
+        // on a change of stream, work issued on the previous one (the handle's initialisation
+        // among it) completes before anything issued on the new one
+        if (!h->has_ext || h->ext != static_cast<cudaStream_t>(s)) B200SV_CUDA(cudaStreamSynchronize(h->stream()));
         h->ext = static_cast<cudaStream_t>(s);
         h->has_ext = true;
     });
@@ -1003,10 +1009,10 @@ int b200sv_adjoint_jacobian(b200sv_handle psi, const b200sv_op *ops, uint32_t no
                         double *dst = d_jac + (size_t)trainable_number * nobs + o0;
                         if (h->dtype == B200SV_C64)
                             reduce_generator_inner<float>(bras.data() + o0, cnt, lambda, h->nq, G, -2.0 * scaling,
-                                                          h->d_partials, dst, 1, st);
+                                                          h->d_partials, dst, 1, st, h->arrival());
                         else
                             reduce_generator_inner<double>(bras.data() + o0, cnt, lambda, h->nq, G, -2.0 * scaling,
-                                                           h->d_partials, dst, 1, st);
+                                                           h->d_partials, dst, 1, st, h->arrival());
                     }
                     --trainable_number;
                     --tp_pos;

@@ -79,11 +79,13 @@ void reduce_pauli_multi(const void *psi, uint32_t nq, const PauliWord *terms, in
 template <typename R>
 void reduce_dense_expval(const void *psi, uint32_t nq, const GateDesc &g, const void *dev_matrix,
                          double *partials, double *out_dev, cudaStream_t st);
-// out_dev[o * out_stride] = alpha * Im <bra_o| G |ket>, o < nbra (<= 16).
+// out_dev[o * out_stride] = alpha * Im <bra_o| G |ket>, o < nbra (<= 16).  With `arrival`
+// (a device counter that is zero, and is left zero) the kernel's last block forms the results
+// and no finalize launch follows.
 template <typename R>
 void reduce_generator_inner(void *const *bras, int nbra, const void *ket, uint32_t nq,
                             const GateDesc &g, double alpha, double *partials, double *out_dev,
-                            int out_stride, cudaStream_t st);
+                            int out_stride, cudaStream_t st, unsigned int *arrival = nullptr);
 // out2_dev[0..1] = (Re, Im) <bra| G |ket>.
 template <typename R>
 void reduce_generator_inner_complex(const void *bra, const void *ket, uint32_t nq, const GateDesc &g,

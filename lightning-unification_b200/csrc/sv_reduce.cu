@@ -189,9 +189,18 @@ __global__ void __launch_bounds__(kRT) k_gen_inner_c(const C<R> *__restrict__ br
     }
 }
 
+// With `fin` set, the last block to finish also forms the results (out[o * stride] = alpha *
+// the sum of partials[o][*], per bra a warp summing in a fixed order) and rearms fin->count,
+// which saves the separate finalize launch in the adjoint sweep's per-parameter loop.
+struct GenFinal {
+    unsigned int *count;  // zero before the launch; zero again after it
+    double *out;
+    int stride;
+    double alpha;
+};
 template <typename R, int NB, int KIND, int K>
 __global__ void __launch_bounds__(kRT) k_gen_inner(Bras<R> bras, int nbra, const C<R> *__restrict__ ket,
-                                                   GenP<R> p, double *partials) {
+                                                   GenP<R> p, double *partials, GenFinal fin) {
     __shared__ double sm[NB * 32];
     constexpr int D = 1 << K;
     double acc[NB];
@@ -221,6 +230,24 @@ __global__ void __launch_bounds__(kRT) k_gen_inner(Bras<R> bras, int nbra, const
         for (int o = 0; o < NB; ++o)
             if (o < nbra) partials[(size_t)o * gridDim.x + blockIdx.x] = acc[o];
     }
+    if (fin.count == nullptr) return;
+    __shared__ bool last;
+    if (threadIdx.x == 0) {
+        __threadfence();  // this block's partials before its arrival
+        last = atomicAdd(fin.count, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int o = warp; o < nbra; o += (int)(blockDim.x >> 5)) {
+        double v = 0.0;
+        for (int b = lane; b < (int)gridDim.x; b += 32) v += __ldcg(&partials[(size_t)o * gridDim.x + b]);
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+        if (lane == 0) fin.out[(size_t)o * fin.stride] = fin.alpha * v;
+    }
+    if (threadIdx.x == 0) *fin.count = 0u;
 }
 
 // launchers of the two inner-product kernels for one generator form (with_gen_form)
@@ -239,10 +266,11 @@ template <typename R> struct GoGen {
     const C<R> *k;
     const GenP<R> &p;
     double *partials;
+    GenFinal fin;
     template <int KIND, int K> void go() const {
-        if (nbra == 1) k_gen_inner<R, 1, KIND, K><<<nb, kRT, 0, st>>>(B, nbra, k, p, partials);
-        else if (nbra <= 4) k_gen_inner<R, 4, KIND, K><<<nb, kRT, 0, st>>>(B, nbra, k, p, partials);
-        else k_gen_inner<R, 16, KIND, K><<<nb, kRT, 0, st>>>(B, nbra, k, p, partials);
+        if (nbra == 1) k_gen_inner<R, 1, KIND, K><<<nb, kRT, 0, st>>>(B, nbra, k, p, partials, fin);
+        else if (nbra <= 4) k_gen_inner<R, 4, KIND, K><<<nb, kRT, 0, st>>>(B, nbra, k, p, partials, fin);
+        else k_gen_inner<R, 16, KIND, K><<<nb, kRT, 0, st>>>(B, nbra, k, p, partials, fin);
     }
 };
 
@@ -790,7 +818,8 @@ template <typename R> GenP<R> make_genp(uint32_t nq, const GateDesc &g) {
 
 template <typename R>
 void reduce_generator_inner(void *const *bras, int nbra, const void *ket, uint32_t nq, const GateDesc &g,
-                            double alpha, double *partials, double *out, int out_stride, cudaStream_t st) {
+                            double alpha, double *partials, double *out, int out_stride, cudaStream_t st,
+                            unsigned int *arrival) {
     if (nbra <= 0) return;
     if (nbra > 16) throw ArgError("at most 16 bras per generator product");
     GenP<R> p = make_genp<R>(nq, g);
@@ -798,9 +827,10 @@ void reduce_generator_inner(void *const *bras, int nbra, const void *ket, uint32
     for (int o = 0; o < nbra; ++o) B.p[o] = static_cast<const C<R> *>(bras[o]);
     const int nb = red_blocks(p.ngroups);
     const C<R> *k = static_cast<const C<R> *>(ket);
-    with_gen_form<R>(p, GoGen<R>{nb, nbra, st, B, k, p, partials});
+    const GenFinal fin{arrival, out, out_stride, alpha};
+    with_gen_form<R>(p, GoGen<R>{nb, nbra, st, B, k, p, partials, fin});
     B200SV_CUDA(cudaGetLastError());
-    finalize(partials, nb, nbra, out, out_stride, alpha, st);
+    if (arrival == nullptr) finalize(partials, nb, nbra, out, out_stride, alpha, st);
 }
 
 template <typename R>
@@ -869,7 +899,7 @@ template <typename R> void axpy(void *acc, const void *x, uint32_t nq, double c,
     template void reduce_dense_expval<R>(const void *, uint32_t, const GateDesc &, const void *, double *,      \
                                          double *, cudaStream_t);                                               \
     template void reduce_generator_inner<R>(void *const *, int, const void *, uint32_t, const GateDesc &,       \
-                                            double, double *, double *, int, cudaStream_t);                     \
+                                            double, double *, double *, int, cudaStream_t, unsigned int *);     \
     template void reduce_generator_inner_complex<R>(const void *, const void *, uint32_t, const GateDesc &,     \
                                                     double *, double *, cudaStream_t);                          \
     template void reduce_probs<R>(const void *, uint32_t, const std::vector<uint32_t> &, double *, size_t,      \
