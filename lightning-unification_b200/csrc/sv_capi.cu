@@ -927,6 +927,26 @@ int b200sv_sample_mcmc(b200sv_handle h, int proposal, uint64_t num_burnin, uint6
     });
 }
 
+// The 2x2 matrix of a one-wire descriptor without controls; false for other forms.
+static bool as_one_wire(const GateDesc &g, cd (&m)[4]) {
+    if (g.tbits.size() != 1 || !g.cbits.empty() || g.k != 1) return false;
+    switch (g.kind) {
+    case Kind::Dense:
+        for (int i = 0; i < 4; ++i) m[i] = g.m[i];
+        return true;
+    case Kind::Diag:
+        m[0] = g.m[0];
+        m[1] = m[2] = cd(0.0, 0.0);
+        m[3] = g.m[1];
+        return true;
+    case Kind::Swap:
+        m[0] = m[3] = cd(0.0, 0.0);
+        m[1] = m[2] = cd(1.0, 0.0);
+        return g.sa != g.sb;
+    default: return false;
+    }
+}
+
 // ---- adjoint Jacobian: LQ/algorithms/AdjointJacobianLQubit.hpp:212-335 --------
 int b200sv_adjoint_jacobian(b200sv_handle psi, const b200sv_op *ops, uint32_t nops, const b200sv_observable *obs,
                             uint32_t nobs, const uint64_t *trainable, uint32_t ntp, int apply_operations,
@@ -1004,6 +1024,23 @@ int b200sv_adjoint_jacobian(b200sv_handle psi, const b200sv_op *ops, uint32_t no
                     double sc = 0.0;
                     GateDesc G = compile_generator((uint32_t)gen, op.wires.data(), (uint32_t)op.wires.size(), h->nq, &sc);
                     const double scaling = sc * (op.inverse ? -1.0 : 1.0);
+                    // one-wire gates: the products and the inverse gate in one pass over the pairs
+                    GateDesc adj1 = compile_op(op, !op.inverse, h->nq);
+                    cd g2[4], u2[4];
+                    if (nobs >= 1 && nobs <= 16 && as_one_wire(G, g2) && as_one_wire(adj1, u2) &&
+                        G.tbits[0] == adj1.tbits[0]) {
+                        double *dst = d_jac + (size_t)trainable_number * nobs;
+                        if (h->dtype == B200SV_C64)
+                            adjoint_rot_step<float>(lambda, bras.data(), (int)nobs, h->nq, G.tbits[0], g2, u2,
+                                                    -2.0 * scaling, h->d_partials, dst, 1, h->arrival(), st);
+                        else
+                            adjoint_rot_step<double>(lambda, bras.data(), (int)nobs, h->nq, G.tbits[0], g2, u2,
+                                                     -2.0 * scaling, h->d_partials, dst, 1, h->arrival(), st);
+                        --trainable_number;
+                        --tp_pos;
+                        --current_param_idx;
+                        continue;
+                    }
                     for (uint32_t o0 = 0; o0 < nobs; o0 += 16) {
                         const int cnt = (int)std::min<uint32_t>(16, nobs - o0);
                         double *dst = d_jac + (size_t)trainable_number * nobs + o0;

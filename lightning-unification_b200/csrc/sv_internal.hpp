@@ -79,6 +79,13 @@ void reduce_pauli_multi(const void *psi, uint32_t nq, const PauliWord *terms, in
 template <typename R>
 void reduce_dense_expval(const void *psi, uint32_t nq, const GateDesc &g, const void *dev_matrix,
                          double *partials, double *out_dev, cudaStream_t st);
+// One adjoint step of a one-wire gate on state bit `bit`: out_dev[o * out_stride] = alpha *
+// Im <bra_o| G |lambda> (G the 2x2 generator), then lambda and every bra <- U lambda, U bra
+// (U the 2x2 inverse gate), in one pass; `arrival` as for reduce_generator_inner.
+template <typename R>
+void adjoint_rot_step(void *lambda, void *const *bras, int nbra, uint32_t nq, uint32_t bit, const cd (&g)[4],
+                      const cd (&u)[4], double alpha, double *partials, double *out_dev, int out_stride,
+                      unsigned int *arrival, cudaStream_t st);
 // out_dev[o * out_stride] = alpha * Im <bra_o| G |ket>, o < nbra (<= 16).  With `arrival`
 // (a device counter that is zero, and is left zero) the kernel's last block forms the results
 // and no finalize launch follows.

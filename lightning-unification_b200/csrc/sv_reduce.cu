@@ -833,6 +833,112 @@ void reduce_generator_inner(void *const *bras, int nbra, const void *ket, uint32
     if (arrival == nullptr) finalize(partials, nb, nbra, out, out_stride, alpha, st);
 }
 
+// ---- one adjoint step of a one-wire rotation, fused -------------------------------------
+// At a differentiated one-wire gate the sweep needs -2 scale Im<bra_o|G|lambda> for every
+// bra and then U^dagger applied to lambda and to every bra.  Both act on the same amplitude
+// pairs, so one pass reads each pair once: the products come from the pair's values before
+// the update, then the pair is updated in place (CAcc, as the gate kernels).  The results
+// are formed by the last block (GenFinal).
+struct AdjRotP {
+    uint64_t npairs, low;  // (1 << bit) - 1
+    uint64_t bit;
+    double2 g[4];          // generator, row-major
+    int nbra;
+};
+template <typename R> struct AdjRotMat {
+    C<R> u[4];  // the inverse gate, row-major
+};
+template <typename R, int NB>
+__global__ void __launch_bounds__(kRT) k_adj_rot(C<R> *__restrict__ lambda, Bras<R> bras, AdjRotP p, AdjRotMat<R> um,
+                                                 double *partials, GenFinal fin) {
+    __shared__ double sm[NB * 32];
+    double acc[NB];
+#pragma unroll
+    for (int o = 0; o < NB; ++o) acc[o] = 0.0;
+    for (uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < p.npairs;
+         g += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t lo = g & p.low;
+        const uint64_t i0 = ((g ^ lo) << 1) | lo, i1 = i0 | p.bit;
+        const C<R> l0 = lambda[i0], l1 = lambda[i1];
+        const double2 a0 = widen<R>(l0), a1 = widen<R>(l1);
+        // w = G (a0, a1)
+        const double2 w0 = make_double2(p.g[0].x * a0.x - p.g[0].y * a0.y + p.g[1].x * a1.x - p.g[1].y * a1.y,
+                                        p.g[0].x * a0.y + p.g[0].y * a0.x + p.g[1].x * a1.y + p.g[1].y * a1.x);
+        const double2 w1 = make_double2(p.g[2].x * a0.x - p.g[2].y * a0.y + p.g[3].x * a1.x - p.g[3].y * a1.y,
+                                        p.g[2].x * a0.y + p.g[2].y * a0.x + p.g[3].x * a1.y + p.g[3].y * a1.x);
+#pragma unroll
+        for (int o = 0; o < NB; ++o) {
+            if (o < p.nbra) {
+                C<R> *b = const_cast<C<R> *>(bras.p[o]);
+                const C<R> c0 = b[i0], c1 = b[i1];
+                const double2 b0 = widen<R>(c0), b1 = widen<R>(c1);
+                acc[o] += (b0.x * w0.y - b0.y * w0.x) + (b1.x * w1.y - b1.y * w1.x);  // Im conj(b) w
+                CAcc<R> x, y;
+                x.add(um.u[0], c0);
+                x.add(um.u[1], c1);
+                y.add(um.u[2], c0);
+                y.add(um.u[3], c1);
+                b[i0] = x.get();
+                b[i1] = y.get();
+            }
+        }
+        CAcc<R> x, y;
+        x.add(um.u[0], l0);
+        x.add(um.u[1], l1);
+        y.add(um.u[2], l0);
+        y.add(um.u[3], l1);
+        lambda[i0] = x.get();
+        lambda[i1] = y.get();
+    }
+    block_reduce<NB>(acc, sm);
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int o = 0; o < NB; ++o)
+            if (o < p.nbra) partials[(size_t)o * gridDim.x + blockIdx.x] = acc[o];
+    }
+    __shared__ bool last;
+    if (threadIdx.x == 0) {
+        __threadfence();
+        last = atomicAdd(fin.count, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int o = warp; o < p.nbra; o += (int)(blockDim.x >> 5)) {
+        double v = 0.0;
+        for (int b = lane; b < (int)gridDim.x; b += 32) v += __ldcg(&partials[(size_t)o * gridDim.x + b]);
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+        if (lane == 0) fin.out[(size_t)o * fin.stride] = fin.alpha * v;
+    }
+    if (threadIdx.x == 0) *fin.count = 0u;
+}
+
+template <typename R>
+void adjoint_rot_step(void *lambda, void *const *bras, int nbra, uint32_t nq, uint32_t bit, const cd (&g)[4],
+                      const cd (&u)[4], double alpha, double *partials, double *out, int out_stride,
+                      unsigned int *arrival, cudaStream_t st) {
+    if (nbra <= 0 || nbra > 16) throw ArgError("one-wire adjoint step takes 1..16 bras");
+    AdjRotP p{};
+    p.npairs = uint64_t(1) << (nq - 1);
+    p.bit = uint64_t(1) << bit;
+    p.low = p.bit - 1;
+    for (int i = 0; i < 4; ++i) p.g[i] = make_double2(g[i].real(), g[i].imag());
+    p.nbra = nbra;
+    AdjRotMat<R> um{};
+    for (int i = 0; i < 4; ++i) um.u[i] = cvt<R>(u[i]);
+    Bras<R> B{};
+    for (int o = 0; o < nbra; ++o) B.p[o] = static_cast<const C<R> *>(bras[o]);
+    const int nb = red_blocks(p.npairs);
+    const GenFinal fin{arrival, out, out_stride, alpha};
+    C<R> *lam = static_cast<C<R> *>(lambda);
+    if (nbra == 1) k_adj_rot<R, 1><<<nb, kRT, 0, st>>>(lam, B, p, um, partials, fin);
+    else if (nbra <= 4) k_adj_rot<R, 4><<<nb, kRT, 0, st>>>(lam, B, p, um, partials, fin);
+    else k_adj_rot<R, 16><<<nb, kRT, 0, st>>>(lam, B, p, um, partials, fin);
+    B200SV_CUDA(cudaGetLastError());
+}
+
 template <typename R>
 void reduce_probs(const void *psi, uint32_t nq, const std::vector<uint32_t> &bits, double *partials,
                   size_t partials_cap, double *out, cudaStream_t st) {
@@ -902,6 +1008,9 @@ template <typename R> void axpy(void *acc, const void *x, uint32_t nq, double c,
                                             double, double *, double *, int, cudaStream_t, unsigned int *);     \
     template void reduce_generator_inner_complex<R>(const void *, const void *, uint32_t, const GateDesc &,     \
                                                     double *, double *, cudaStream_t);                          \
+    template void adjoint_rot_step<R>(void *, void *const *, int, uint32_t, uint32_t, const cd(&)[4],          \
+                                      const cd(&)[4], double, double *, double *, int, unsigned int *,         \
+                                      cudaStream_t);                                                           \
     template void reduce_probs<R>(const void *, uint32_t, const std::vector<uint32_t> &, double *, size_t,      \
                                   double *, cudaStream_t);                                                      \
     template void set_basis<R>(void *, uint32_t, uint64_t, cudaStream_t);                                       \
