@@ -651,53 +651,56 @@ __device__ void exec_run(C<R> *const (&s)[NS], int kt, int wl, bool wloc, const 
         }
         return;
     }
-    // adjoint sweep: register copies in reverse order
-    C<R> m[kMaxRun][4];
-    double ip[kMaxRun];
-    int gc[kMaxRun], mk_[kMaxRun];
+    if constexpr (REV) {
+        // adjoint sweep: register copies in reverse order
+        C<R> m[kMaxRun][4];
+        double ip[kMaxRun];
+        int gc[kMaxRun], mk_[kMaxRun];
 #pragma unroll
-    for (int kk = 0; kk < kMaxRun; ++kk) {
-        ip[kk] = 0.0;
-        gc[kk] = 0;
-        mk_[kk] = MK_GENERAL;
-        if (kk < len) {
-            const DOp &op = ops[len - 1 - kk];
-            member_from<R>(op, cf[len - 1 - kk], m[kk]);
-            mk_[kk] = op.mkind;
-            if (op.gslot >= 0) gc[kk] = op.gcode;
-        }
-    }
-    switch (run_sig(len, mk_[0], gc[0], mk_[1], gc[1], mk_[2], gc[2])) {
-    case run_sig(3, MK_DIAG, 3, MK_REAL, 2, MK_DIAG, 3):  // Rot = RZ RY RZ, every angle trained
-        run_rev_fixed<R, NS, 3, MK_DIAG, 3, MK_REAL, 2, MK_DIAG, 3>(s, rg, low, bit, m, ip);
-        break;
-    case run_sig(2, MK_DIAG, 3, MK_REAL, 2):  // RY then RZ
-        run_rev_fixed<R, NS, 2, MK_DIAG, 3, MK_REAL, 2, MK_GENERAL, 0>(s, rg, low, bit, m, ip);
-        break;
-    case run_sig(2, MK_REAL, 2, MK_DIAG, 3):  // RZ then RY
-        run_rev_fixed<R, NS, 2, MK_REAL, 2, MK_DIAG, 3, MK_GENERAL, 0>(s, rg, low, bit, m, ip);
-        break;
-    default:
-        for (uint32_t g = rg.g0; g < rg.g1; g += rg.gs) {
-            const uint32_t i0 = ((g & ~low) << 1) | (g & low), i1 = i0 | bit;
-            C<R> a0 = s[0][i0], a1 = s[0][i1], b0 = s[NS - 1][i0], b1 = s[NS - 1][i1];
-#pragma unroll
-            for (int kk = 0; kk < kMaxRun; ++kk) {
-                if (kk < len) {
-                    if (gc[kk]) ip[kk] += pair_gen_im<R>(gc[kk], a0, a1, b0, b1);
-                    apply_pair<R>(mk_[kk], m[kk], a0, a1);
-                    apply_pair<R>(mk_[kk], m[kk], b0, b1);
-                }
+        for (int kk = 0; kk < kMaxRun; ++kk) {
+            ip[kk] = 0.0;
+            gc[kk] = 0;
+            mk_[kk] = MK_GENERAL;
+            if (kk < len) {
+                const DOp &op = ops[len - 1 - kk];
+                member_from<R>(op, cf[len - 1 - kk], m[kk]);
+                mk_[kk] = op.mkind;
+                if (op.gslot >= 0) gc[kk] = op.gcode;
             }
-            s[0][i0] = a0;
-            s[0][i1] = a1;
-            s[NS - 1][i0] = b0;
-            s[NS - 1][i1] = b1;
         }
-    }
+        switch (run_sig(len, mk_[0], gc[0], mk_[1], gc[1], mk_[2], gc[2])) {
+        case run_sig(3, MK_DIAG, 3, MK_REAL, 2, MK_DIAG, 3):  // Rot = RZ RY RZ, every angle trained
+            run_rev_fixed<R, NS, 3, MK_DIAG, 3, MK_REAL, 2, MK_DIAG, 3>(s, rg, low, bit, m, ip);
+            break;
+        case run_sig(2, MK_DIAG, 3, MK_REAL, 2):  // RY then RZ
+            run_rev_fixed<R, NS, 2, MK_DIAG, 3, MK_REAL, 2, MK_GENERAL, 0>(s, rg, low, bit, m, ip);
+            break;
+        case run_sig(2, MK_REAL, 2, MK_DIAG, 3):  // RZ then RY
+            run_rev_fixed<R, NS, 2, MK_REAL, 2, MK_DIAG, 3, MK_GENERAL, 0>(s, rg, low, bit, m, ip);
+            break;
+        default:
+            for (uint32_t g = rg.g0; g < rg.g1; g += rg.gs) {
+                const uint32_t i0 = ((g & ~low) << 1) | (g & low), i1 = i0 | bit;
+                C<R> a0 = s[0][i0], a1 = s[0][i1], b0 = s[NS - 1][i0], b1 = s[NS - 1][i1];
 #pragma unroll
-    for (int kk = 0; kk < kMaxRun; ++kk)
-        if (kk < len && gc[kk]) add_grad(gradw, ops[len - 1 - kk].gslot, ip[kk], first_tile);
+                for (int kk = 0; kk < kMaxRun; ++kk) {
+                    if (kk < len) {
+                        if (gc[kk]) ip[kk] += pair_gen_im<R>(gc[kk], a0, a1, b0, b1);
+                        apply_pair<R>(mk_[kk], m[kk], a0, a1);
+                        apply_pair<R>(mk_[kk], m[kk], b0, b1);
+                    }
+                }
+                s[0][i0] = a0;
+                s[0][i1] = a1;
+                s[NS - 1][i0] = b0;
+                s[NS - 1][i1] = b1;
+            }
+        }
+#pragma unroll
+        for (int kk = 0; kk < kMaxRun; ++kk)
+            if (kk < len && gc[kk]) add_grad(gradw, ops[len - 1 - kk].gslot, ip[kk], first_tile);
+
+    }
 }
 
 // ---- two runs on different bits in one pass over amplitude quadruples -------------------
@@ -1104,6 +1107,9 @@ __device__ void run_forward(const KArgs &A, const DCirc &c, C<R> *sm, C<R> *pa, 
 // MODE 0: forward expectation values; MODE 1: forward (unless reused) and the VJP sweep.
 // FULL: compiled with the two-wire dense step and generator paths (only batches that
 // hold such gates launch it; the others get a kernel without them, in fewer registers).
+// Compiled for 512 threads (128 registers a thread).  Instantiations for 256 threads with up to
+// 255 registers (no spills in the complex128 steps) were tried: the autotuner kept 512 threads
+// for every workload of the bench (complex128 HEA batch 1027 ms either way).
 template <typename R, int MODE, bool FULL>
 __global__ void __launch_bounds__(512) k_batch(KArgs A) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -1879,8 +1885,8 @@ void launch_main(Batch &B, int mode, const double *dy, double *out, const int *r
     A.max_kt = mk;
     B200SV_CUDA(cudaMemsetAsync(B.d_counter, 0, sizeof(uint32_t), st));
     void *args[] = {&A};
-    B200SV_CUDA(cudaLaunchKernel(batch_kernel(B.dtype, mode, B.full), dim3(B.grid), dim3(B.cfg.threads), args,
-                                 B.smem_bytes, st));
+    const void *k = batch_kernel(B.dtype, mode, B.full);
+    B200SV_CUDA(cudaLaunchKernel(k, dim3(B.grid), dim3(B.cfg.threads), args, B.smem_bytes, st));
 }
 
 // Forward: expectation values; the final states of circuits wider than a tile stay
