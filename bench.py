@@ -325,6 +325,90 @@ def rows_30q(nq: int, hbm_peak: float, cpu: bool, cpu_qubits: int = 26, steps: i
     return out
 
 
+def next_rows(cpu: bool, reps: int = 3):
+    """The rows beside the core path, complex128: the state-return VJP (20 qubits, 2 layers of
+    RX RY RZ + CNOT ladder, 120 parameters), a sparse Hamiltonian expectation value (22 qubits,
+    the periodic tridiagonal CSR matrix of the reference's tests, 3 entries per row) and
+    Metropolis sampling (20 qubits, local proposal, 4096 chains).  GPU calls through the C ABI
+    (median of `reps`, host clock around the call, results back on the host); beside them the
+    reference module compiled from its sources, once, on the host cores."""
+    from lightning_b200 import capi
+    from lightning_b200.workloads import layered_rotations
+    rng = np.random.default_rng(17)
+    out = {}
+
+    def med(fn):
+        fn()
+        ts = []
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            fn()
+            ts.append((time.perf_counter() - t0) * 1e3)
+        return float(np.median(ts))
+
+    # state-return VJP
+    n = 20
+    ops, _, _ = layered_rotations(n=n, layers=2, seed=3)
+    tp = list(range(sum(1 for op in ops if op[3])))
+    sv = capi.StateVector(n, np.complex128)
+    sv.apply_ops(ops)
+    psi = sv.download()
+    dy = rng.normal(size=1 << n) + 1j * rng.normal(size=1 << n)
+    dy /= np.linalg.norm(dy)
+    vjp = sv.vjp_state(ops, dy, tp)
+    out["vjp_state"] = {"qubits": n, "params": len(tp), "ms": med(lambda: sv.vjp_state(ops, dy, tp))}
+    sv.close()
+    # sparse Hamiltonian
+    ns = 22
+    N = 1 << ns
+    r = np.arange(N, dtype=np.uint64)
+    indptr = np.arange(N + 1, dtype=np.uint64) * 3
+    cols = np.stack([(r + N - 1) % N, r, (r + 1) % N], axis=1)
+    vals = np.tile(np.array([-1.0, 1.0, -1.0], dtype=np.complex128), (N, 1))
+    order = np.argsort(cols, axis=1, kind="stable")  # columns ascending within a row
+    indices = np.take_along_axis(cols, order, axis=1).reshape(-1).astype(np.uint64)
+    data = np.take_along_axis(vals, order, axis=1).reshape(-1)
+    st = (rng.normal(size=N) + 1j * rng.normal(size=N)).astype(np.complex128)
+    st /= np.linalg.norm(st)
+    sv = capi.StateVector(ns, np.complex128)
+    sv.upload(st)
+    ev = sv.expval_sparse(indptr, indices, data)
+    out["sparse_expval"] = {"qubits": ns, "nnz": int(3 * N), "ms": med(lambda: sv.expval_sparse(indptr, indices, data))}
+    sv.close()
+    # Metropolis sampling
+    nm = 20
+    sm = (rng.normal(size=1 << nm) + 1j * rng.normal(size=1 << nm)).astype(np.complex128)
+    sm /= np.linalg.norm(sm)
+    sv = capi.StateVector(nm, np.complex128)
+    sv.upload(sm)
+    shots = 1_000_000
+    ms = med(lambda: sv.sample_mcmc(capi.MCMC_LOCAL, 100, shots, 4096, seed=1))
+    out["mcmc_local"] = {"qubits": nm, "shots": shots, "burnin": 100, "chains": 4096, "ms": ms,
+                         "shots_per_s": shots / (ms / 1e3)}
+    sv.close()
+    if cpu:
+        import ref  # the reference module built from its sources: the CPU baseline only
+        m = ref.load()
+        if m is not None:
+            t0 = time.perf_counter()
+            want = ref.vjp_state(m, psi.copy(), ops, dy, tp)
+            out["vjp_state"]["reference_cpu_ms"] = (time.perf_counter() - t0) * 1e3
+            out["vjp_state"]["max_abs_diff"] = float(np.abs(vjp - want).max())
+            t0 = time.perf_counter()
+            ev_ref = ref.sparse_expval(m, st.copy(), indptr, indices, data)
+            out["sparse_expval"]["reference_cpu_ms"] = (time.perf_counter() - t0) * 1e3
+            out["sparse_expval"]["abs_diff"] = abs(ev - ev_ref)
+            svr = m.StateVectorC128(sm.copy())
+            rshots = 100_000
+            t0 = time.perf_counter()
+            m.MeasurementsC128(svr).generate_mcmc_samples(nm, "Local", 100, rshots)
+            dt = time.perf_counter() - t0
+            out["mcmc_local"]["reference_cpu_shots_per_s"] = rshots / dt
+            out["reference_cpu"] = {"threads": os.environ.get("OMP_NUM_THREADS", f"unset ({os.cpu_count()} cores)"),
+                                    "note": "one call each; the reference's Metropolis run takes 1e5 shots"}
+    return out
+
+
 def matrix_sweep(nq: int, hbm_peak: float, kmax: int = 8, steps: int = 3):
     """applyMatrix of random k-wire unitaries (k = 1..kmax, seeded wires) on an nq-qubit state,
     complex128 and complex64: ms per launch, HBM GB/s (2 x bytes of the state) and the matrix
@@ -396,6 +480,9 @@ def run_case(args):
         return
     if args.case == "plain":
         print(json.dumps({"case": "plain", **plain_layered(not args.no_cpu)}))
+        return
+    if args.case == "next":
+        print(json.dumps({"case": "next", **next_rows(not args.no_cpu)}))
         return
     if args.case == "rows":
         print(json.dumps({"case": "rows", **rows_30q(args.qubits, peaks()[0], not args.no_cpu)}))
@@ -630,7 +717,7 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--sweep-qubits", type=int, default=30)
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--case", default="full", choices=["full", "gate", "batch", "fused", "precision", "plain", "matrix", "rows"],
+    ap.add_argument("--case", default="full", choices=["full", "gate", "batch", "fused", "precision", "plain", "matrix", "rows", "next"],
                     help="gate / batch: one kernel family on a small case (profiling)")
     ap.add_argument("--qubits", type=int, default=28, help="--case gate: state width (complex128)")
     ap.add_argument("--ncirc", type=int, default=148, help="--case batch: number of circuits")
@@ -756,6 +843,7 @@ def main():
     roof["peak_kind"] = peak_kind
     msweep = matrix_sweep(args.sweep_qubits, hbm_peak)
     rows = rows_30q(args.sweep_qubits, hbm_peak, not args.no_cpu)
+    nxt = next_rows(not args.no_cpu)
 
     cpu = None if args.no_cpu else reference_cpu(circuits, params_np, dy_np, 4)
     del eng
@@ -783,6 +871,7 @@ def main():
                        "fused_speedup": sweep_ms["unfused"] / sweep_ms["fused"]},
         "matrix_sweep": msweep,
         "rows_single_state": rows,
+        "rows_next": nxt,
         "hea_batch_forward": hea,
         "hea_batch_forward_c128": hea128,
         "sampling": samp,

@@ -802,11 +802,11 @@ static void sparse_impl(b200sv_state *h, const uint64_t *row_map, uint64_t row_m
     need(row_map != nullptr || row_map_size == 0, "NULL row_map");
     need(row_map_size >= 1 && row_map_size - 1 == N, "Statevector and Hamiltonian have incompatible sizes.");
     const uint64_t base = row_map[0];
-    for (uint64_t i = 0; i < N; ++i) need(row_map[i] <= row_map[i + 1], "row_map must be non-decreasing");
+    need(row_map[N] >= base, "row_map must be non-decreasing");
     const uint64_t used = row_map[N] - base;
     need(used <= nnz, "row_map addresses more non-zeros than the value array holds");
     need(used == 0 || (entries != nullptr && values != nullptr), "NULL entries or values");
-    for (uint64_t k = 0; k < used; ++k) need(entries[k] < N, "sparse column index out of range");
+    // the per-row bounds and column indices are checked on the device as the kernel reads them
     const cudaStream_t st = h->stream();
     const size_t S = h->dtype == B200SV_C64 ? 8 : 16;
     uint64_t *d_rows = nullptr, *d_cols = nullptr;
@@ -828,11 +828,17 @@ static void sparse_impl(b200sv_state *h, const uint64_t *row_map, uint64_t row_m
         B200SV_CUDA(cudaMemcpyAsync(d_cols, entries, used * sizeof(uint64_t), cudaMemcpyHostToDevice, st));
         B200SV_CUDA(cudaMemcpyAsync(d_vals, values, used * S, cudaMemcpyHostToDevice, st));
     }
+    unsigned int *bad = reinterpret_cast<unsigned int *>(h->d_small + 2);
+    B200SV_CUDA(cudaMemsetAsync(bad, 0, sizeof(double), st));
     if (h->dtype == B200SV_C64)
-        reduce_sparse<float>(h->d_state, h->nq, d_rows, d_cols, d_vals, used, h->d_partials, h->d_small, st);
+        reduce_sparse<float>(h->d_state, h->nq, d_rows, d_cols, d_vals, used, h->d_partials, h->d_small, bad, st);
     else
-        reduce_sparse<double>(h->d_state, h->nq, d_rows, d_cols, d_vals, used, h->d_partials, h->d_small, st);
-    read_small(h, 1);
+        reduce_sparse<double>(h->d_state, h->nq, d_rows, d_cols, d_vals, used, h->d_partials, h->d_small, bad, st);
+    read_small(h, 2);
+    unsigned int flags = 0;
+    std::memcpy(&flags, &h->h_small[2], sizeof(flags));
+    need(!(flags & 1u), "row_map must be non-decreasing");
+    need(!(flags & 2u), "sparse column index out of range");
     out[0] = h->h_small[0];
     out[1] = h->h_small[1];
 }

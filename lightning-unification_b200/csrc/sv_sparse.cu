@@ -20,10 +20,15 @@ namespace {
 
 constexpr int kST = 256;
 
+// The CSR arrays are checked here, on the device, as they are read: a row whose bounds are
+// decreasing or leave [row_map[0], row_map[0] + used] sets bit 0 of *bad and counts as empty,
+// a column index outside the state sets bit 1 and its term is skipped, so no access leaves
+// the arrays; the host turns the bits into the reference's error messages.
 template <typename R, int W>
 __global__ void __launch_bounds__(kST) k_sparse_ev(const C<R> *__restrict__ psi, const uint64_t *__restrict__ row_map,
                                                    const uint64_t *__restrict__ cols, const C<R> *__restrict__ vals,
-                                                   uint64_t nrows, double *partials) {
+                                                   uint64_t nrows, uint64_t used, double *partials,
+                                                   unsigned int *bad) {
     __shared__ double sm[2 * 32];
     double acc[2] = {0.0, 0.0};
     const int lane = threadIdx.x % W;
@@ -37,10 +42,20 @@ __global__ void __launch_bounds__(kST) k_sparse_ev(const C<R> *__restrict__ psi,
         const bool live = r < nrows;
         double yr = 0.0, yi = 0.0;
         if (live) {
-            const uint64_t b = row_map[r] - base, e = row_map[r + 1] - base;
+            const uint64_t lo = row_map[r], hi = row_map[r + 1];
+            uint64_t b = lo - base, e = hi - base;
+            if (hi < lo || lo < base || e > used) {
+                if (lane == 0) atomicOr(bad, 1u);
+                e = b = 0;
+            }
             for (uint64_t k = b + lane; k < e; k += W) {
+                const uint64_t c = cols[k];
+                if (c >= nrows) {
+                    atomicOr(bad, 2u);
+                    continue;
+                }
                 const double2 v = widen<R>(vals[k]);
-                const double2 x = widen<R>(psi[cols[k]]);
+                const double2 x = widen<R>(psi[c]);
                 yr = fma(v.x, x.x, fma(-v.y, x.y, yr));
                 yi = fma(v.x, x.y, fma(v.y, x.x, yi));
             }
@@ -79,9 +94,9 @@ __global__ void k_sparse_finalize(const double *__restrict__ partials, int nb, d
 
 template <typename R, int W>
 void launch_w(const void *psi, const uint64_t *row_map, const uint64_t *cols, const void *vals, uint64_t nrows,
-              double *partials, int nb, cudaStream_t st) {
+              uint64_t used, double *partials, unsigned int *bad, int nb, cudaStream_t st) {
     k_sparse_ev<R, W><<<nb, kST, 0, st>>>(static_cast<const C<R> *>(psi), row_map, cols,
-                                          static_cast<const C<R> *>(vals), nrows, partials);
+                                          static_cast<const C<R> *>(vals), nrows, used, partials, bad);
 }
 
 }  // namespace
@@ -96,18 +111,20 @@ int sparse_lanes(uint64_t nrows, uint64_t nnz) {
 
 template <typename R>
 void reduce_sparse(const void *psi, uint32_t nq, const uint64_t *row_map_dev, const uint64_t *cols_dev,
-                   const void *vals_dev, uint64_t nnz, double *partials, double *out_dev, cudaStream_t st) {
+                   const void *vals_dev, uint64_t nnz, double *partials, double *out_dev, unsigned int *bad_dev,
+                   cudaStream_t st) {
     const uint64_t nrows = uint64_t(1) << nq;
     const int w = sparse_lanes(nrows, nnz);
     const uint64_t threads = nrows * (uint64_t)w;
     const int nb = (int)std::max<uint64_t>(1, std::min<uint64_t>((threads + kST - 1) / kST, kMaxRedBlocks));
+    const uint64_t *rm = row_map_dev, *cl = cols_dev;
     switch (w) {
-    case 1: launch_w<R, 1>(psi, row_map_dev, cols_dev, vals_dev, nrows, partials, nb, st); break;
-    case 2: launch_w<R, 2>(psi, row_map_dev, cols_dev, vals_dev, nrows, partials, nb, st); break;
-    case 4: launch_w<R, 4>(psi, row_map_dev, cols_dev, vals_dev, nrows, partials, nb, st); break;
-    case 8: launch_w<R, 8>(psi, row_map_dev, cols_dev, vals_dev, nrows, partials, nb, st); break;
-    case 16: launch_w<R, 16>(psi, row_map_dev, cols_dev, vals_dev, nrows, partials, nb, st); break;
-    default: launch_w<R, 32>(psi, row_map_dev, cols_dev, vals_dev, nrows, partials, nb, st); break;
+    case 1: launch_w<R, 1>(psi, rm, cl, vals_dev, nrows, nnz, partials, bad_dev, nb, st); break;
+    case 2: launch_w<R, 2>(psi, rm, cl, vals_dev, nrows, nnz, partials, bad_dev, nb, st); break;
+    case 4: launch_w<R, 4>(psi, rm, cl, vals_dev, nrows, nnz, partials, bad_dev, nb, st); break;
+    case 8: launch_w<R, 8>(psi, rm, cl, vals_dev, nrows, nnz, partials, bad_dev, nb, st); break;
+    case 16: launch_w<R, 16>(psi, rm, cl, vals_dev, nrows, nnz, partials, bad_dev, nb, st); break;
+    default: launch_w<R, 32>(psi, rm, cl, vals_dev, nrows, nnz, partials, bad_dev, nb, st); break;
     }
     B200SV_CUDA(cudaGetLastError());
     k_sparse_finalize<<<1, 128, 0, st>>>(partials, nb, out_dev);
@@ -115,8 +132,8 @@ void reduce_sparse(const void *psi, uint32_t nq, const uint64_t *row_map_dev, co
 }
 
 template void reduce_sparse<float>(const void *, uint32_t, const uint64_t *, const uint64_t *, const void *,
-                                   uint64_t, double *, double *, cudaStream_t);
+                                   uint64_t, double *, double *, unsigned int *, cudaStream_t);
 template void reduce_sparse<double>(const void *, uint32_t, const uint64_t *, const uint64_t *, const void *,
-                                    uint64_t, double *, double *, cudaStream_t);
+                                    uint64_t, double *, double *, unsigned int *, cudaStream_t);
 
 }  // namespace b200sv
