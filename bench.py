@@ -374,6 +374,13 @@ def next_rows(cpu: bool, reps: int = 3):
     sv.upload(st)
     ev = sv.expval_sparse(indptr, indices, data)
     out["sparse_expval"] = {"qubits": ns, "nnz": int(3 * N), "ms": med(lambda: sv.expval_sparse(indptr, indices, data))}
+    import torch
+    dp = torch.tensor(indptr.astype(np.int64), device="cuda")
+    di = torch.tensor(indices.astype(np.int64), device="cuda")
+    dv = torch.tensor(data, device="cuda")
+    out["sparse_expval"]["device_arrays_ms"] = med(
+        lambda: sv.expval_sparse_device(dp.data_ptr(), di.data_ptr(), dv.data_ptr(), int(3 * N)))
+    del dp, di, dv
     sv.close()
     # Metropolis sampling
     nm = 20

@@ -224,6 +224,18 @@ int b200sv_expval_sparse(b200sv_handle h, const uint64_t *row_map,
 int b200sv_var_sparse(b200sv_handle h, const uint64_t *row_map,
                       uint64_t row_map_size, const uint64_t *entries,
                       const void *values, uint64_t nnz, double *out);
+/* The same with the CSR arrays already in device memory (a Hamiltonian kept resident
+ * across calls): row_map holds 2^n + 1 entries, entries and values nnz each; nothing
+ * crosses from the host.  Row bounds and column indices are checked on the device, with
+ * the messages of the host-array forms. */
+int b200sv_expval_sparse_device(b200sv_handle h, const uint64_t *row_map_device,
+                                const uint64_t *entries_device,
+                                const void *values_device, uint64_t nnz,
+                                double *out);
+int b200sv_var_sparse_device(b200sv_handle h, const uint64_t *row_map_device,
+                             const uint64_t *entries_device,
+                             const void *values_device, uint64_t nnz,
+                             double *out);
 
 /* Sampling by inverse CDF (the lightning.kokkos rule,
  * LK/measurements/MeasuresFunctors.hpp:70-103 over an exclusive scan,

@@ -796,6 +796,9 @@ int b200sv_norm2(b200sv_handle h, double *out) {
 // ---- sparse Hamiltonian: LQ/measurements/MeasurementsLQubit.hpp:197-214, :451-472 ----
 // out[0] = Re<psi|H psi>, out[1] = <H psi|H psi>.  The CSR arrays are checked on the host
 // (the reference reads them unchecked) so no launch reads outside them or the state.
+static void sparse_device(b200sv_state *h, const uint64_t *d_rows, const uint64_t *d_cols, const void *d_vals,
+                          uint64_t nnz, double out[2]);
+
 static void sparse_impl(b200sv_state *h, const uint64_t *row_map, uint64_t row_map_size, const uint64_t *entries,
                         const void *values, uint64_t nnz, double out[2]) {
     const uint64_t N = uint64_t(1) << h->nq;
@@ -828,19 +831,54 @@ static void sparse_impl(b200sv_state *h, const uint64_t *row_map, uint64_t row_m
         B200SV_CUDA(cudaMemcpyAsync(d_cols, entries, used * sizeof(uint64_t), cudaMemcpyHostToDevice, st));
         B200SV_CUDA(cudaMemcpyAsync(d_vals, values, used * S, cudaMemcpyHostToDevice, st));
     }
+    sparse_device(h, d_rows, d_cols, d_vals, used, out);
+}
+
+// CSR arrays in device memory: the kernel checks every row's bounds against [row_map[0],
+// row_map[0] + nnz] and every column index, so nothing is read from the host.
+static void sparse_device(b200sv_state *h, const uint64_t *d_rows, const uint64_t *d_cols, const void *d_vals,
+                          uint64_t nnz, double out[2]) {
+    const cudaStream_t st = h->stream();
     unsigned int *bad = reinterpret_cast<unsigned int *>(h->d_small + 2);
     B200SV_CUDA(cudaMemsetAsync(bad, 0, sizeof(double), st));
     if (h->dtype == B200SV_C64)
-        reduce_sparse<float>(h->d_state, h->nq, d_rows, d_cols, d_vals, used, h->d_partials, h->d_small, bad, st);
+        reduce_sparse<float>(h->d_state, h->nq, d_rows, d_cols, d_vals, nnz, h->d_partials, h->d_small, bad, st);
     else
-        reduce_sparse<double>(h->d_state, h->nq, d_rows, d_cols, d_vals, used, h->d_partials, h->d_small, bad, st);
+        reduce_sparse<double>(h->d_state, h->nq, d_rows, d_cols, d_vals, nnz, h->d_partials, h->d_small, bad, st);
     read_small(h, 2);
     unsigned int flags = 0;
     std::memcpy(&flags, &h->h_small[2], sizeof(flags));
     need(!(flags & 1u), "row_map must be non-decreasing");
+    need(!(flags & 4u), "row_map addresses more non-zeros than the value array holds");
     need(!(flags & 2u), "sparse column index out of range");
     out[0] = h->h_small[0];
     out[1] = h->h_small[1];
+}
+
+int b200sv_expval_sparse_device(b200sv_handle h, const uint64_t *row_map, const uint64_t *entries,
+                                const void *values, uint64_t nnz, double *out) {
+    return guard([&] {
+        check_handle(h);
+        need(out != nullptr && row_map != nullptr, "NULL row_map or output");
+        need(nnz == 0 || (entries != nullptr && values != nullptr), "NULL entries or values");
+        DeviceGuard dg(h->device);
+        double r[2];
+        sparse_device(h, row_map, entries, values, nnz, r);
+        *out = r[0];
+    });
+}
+
+int b200sv_var_sparse_device(b200sv_handle h, const uint64_t *row_map, const uint64_t *entries,
+                             const void *values, uint64_t nnz, double *out) {
+    return guard([&] {
+        check_handle(h);
+        need(out != nullptr && row_map != nullptr, "NULL row_map or output");
+        need(nnz == 0 || (entries != nullptr && values != nullptr), "NULL entries or values");
+        DeviceGuard dg(h->device);
+        double r[2];
+        sparse_device(h, row_map, entries, values, nnz, r);
+        *out = r[1] - r[0] * r[0];
+    });
 }
 
 int b200sv_expval_sparse(b200sv_handle h, const uint64_t *row_map, uint64_t row_map_size, const uint64_t *entries,

@@ -99,8 +99,8 @@ void reduce_generator_inner_complex(const void *bra, const void *ket, uint32_t n
                                     double *partials, double *out2_dev, cudaStream_t st);
 // out_dev[0] = Re<psi|H psi>, out_dev[1] = |H psi|^2 for H in CSR form (device arrays,
 // row i owning [row_map[i] - row_map[0], row_map[i+1] - row_map[0]), nnz the entries row_map
-// addresses); sv_sparse.cu.  *bad_dev (zero before the call) gets bit 0 for decreasing or
-// out-of-range row bounds and bit 1 for a column index outside the state.
+// addresses); sv_sparse.cu.  *bad_dev (zero before the call) gets bit 0 for decreasing row
+// bounds, bit 2 for a row ending past nnz and bit 1 for a column index outside the state.
 template <typename R>
 void reduce_sparse(const void *psi, uint32_t nq, const uint64_t *row_map_dev, const uint64_t *cols_dev,
                    const void *vals_dev, uint64_t nnz, double *partials, double *out_dev, unsigned int *bad_dev,

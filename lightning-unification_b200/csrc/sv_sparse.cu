@@ -21,9 +21,10 @@ namespace {
 constexpr int kST = 256;
 
 // The CSR arrays are checked here, on the device, as they are read: a row whose bounds are
-// decreasing or leave [row_map[0], row_map[0] + used] sets bit 0 of *bad and counts as empty,
-// a column index outside the state sets bit 1 and its term is skipped, so no access leaves
-// the arrays; the host turns the bits into the reference's error messages.
+// decreasing (or below row_map[0]) sets bit 0 of *bad, one ending past the `used` entries
+// sets bit 2, and either counts as empty; a column index outside the state sets bit 1 and
+// its term is skipped, so no access leaves the arrays.  The host turns the bits into the
+// error messages of the host-array checks.
 template <typename R, int W>
 __global__ void __launch_bounds__(kST) k_sparse_ev(const C<R> *__restrict__ psi, const uint64_t *__restrict__ row_map,
                                                    const uint64_t *__restrict__ cols, const C<R> *__restrict__ vals,
@@ -45,7 +46,7 @@ __global__ void __launch_bounds__(kST) k_sparse_ev(const C<R> *__restrict__ psi,
             const uint64_t lo = row_map[r], hi = row_map[r + 1];
             uint64_t b = lo - base, e = hi - base;
             if (hi < lo || lo < base || e > used) {
-                if (lane == 0) atomicOr(bad, 1u);
+                if (lane == 0) atomicOr(bad, e > used && hi >= lo && lo >= base ? 4u : 1u);
                 e = b = 0;
             }
             for (uint64_t k = b + lane; k < e; k += W) {

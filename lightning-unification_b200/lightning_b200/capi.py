@@ -129,6 +129,10 @@ _SIGS = {
     "b200sv_norm2": ([C.c_void_p, C.POINTER(C.c_double)], C.c_int),
     "b200sv_sample_mcmc": ([C.c_void_p, C.c_int, C.c_uint64, C.c_uint64, C.c_uint32, C.c_uint64,
                             C.POINTER(C.c_uint64)], C.c_int),
+    "b200sv_expval_sparse_device": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64,
+                                     C.POINTER(C.c_double)], C.c_int),
+    "b200sv_var_sparse_device": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64,
+                                  C.POINTER(C.c_double)], C.c_int),
     "b200sv_expval_sparse": ([C.c_void_p, C.POINTER(C.c_uint64), C.c_uint64, C.POINTER(C.c_uint64), C.c_void_p,
                               C.c_uint64, C.POINTER(C.c_double)], C.c_int),
     "b200sv_var_sparse": ([C.c_void_p, C.POINTER(C.c_uint64), C.c_uint64, C.POINTER(C.c_uint64), C.c_void_p,
@@ -413,6 +417,19 @@ class StateVector:
 
     def var_sparse(self, indptr, indices, data) -> float:
         return self._sparse(lib().b200sv_var_sparse, indptr, indices, data)
+
+    def expval_sparse_device(self, indptr_ptr: int, indices_ptr: int, data_ptr: int, nnz: int) -> float:
+        """expval_sparse with the CSR arrays in device memory (uint64, uint64, the state's dtype)."""
+        r = C.c_double()
+        check(lib().b200sv_expval_sparse_device(self.h, C.c_void_p(indptr_ptr), C.c_void_p(indices_ptr),
+                                                C.c_void_p(data_ptr), int(nnz), C.byref(r)))
+        return r.value
+
+    def var_sparse_device(self, indptr_ptr: int, indices_ptr: int, data_ptr: int, nnz: int) -> float:
+        r = C.c_double()
+        check(lib().b200sv_var_sparse_device(self.h, C.c_void_p(indptr_ptr), C.c_void_p(indices_ptr),
+                                             C.c_void_p(data_ptr), int(nnz), C.byref(r)))
+        return r.value
 
     def expval_pauli(self, words, coeffs=None):
         """words: list of (pauli_string, wires); returns (per-term values, weighted sum)."""

@@ -233,6 +233,41 @@ def test_sparse_vs_oracle(capi, n, density, dtype):
     assert abs(sv.var_sparse(indptr, indices, data) - want_v) < tol * scale
 
 
+@pytest.mark.parametrize("dtype", [np.complex128, np.complex64])
+def test_sparse_device_arrays(capi, dtype):
+    """The CSR arrays in device memory give the host-array results; bad arrays are rejected
+    with the same messages (checked on the device)."""
+    import torch
+    import lq_oracle as O
+    rng = np.random.default_rng(31)
+    n = 9
+    st = random_state(rng, n, dtype)
+    sv = capi.StateVector(n, dtype)
+    sv.upload(st)
+    indptr, indices, data = O.tridiagonal_periodic_csr(1 << n)
+    data = (data * rng.normal(size=data.size)).astype(dtype)
+    tdt = torch.complex64 if dtype == np.complex64 else torch.complex128
+    dp = torch.tensor(indptr.astype(np.int64), device="cuda")
+    di = torch.tensor(indices.astype(np.int64), device="cuda")
+    dv = torch.tensor(data, dtype=tdt, device="cuda")
+    got = sv.expval_sparse_device(dp.data_ptr(), di.data_ptr(), dv.data_ptr(), data.size)
+    assert got == sv.expval_sparse(indptr, indices, data)
+    gv = sv.var_sparse_device(dp.data_ptr(), di.data_ptr(), dv.data_ptr(), data.size)
+    assert gv == sv.var_sparse(indptr, indices, data)
+    tol = 1e-12 if dtype == np.complex128 else 1e-5
+    assert abs(got - O.sparse_expval(st.astype(np.complex128), indptr, indices, data.astype(np.complex128))) < tol
+    bad = di.clone()
+    bad[7] = 1 << n
+    with pytest.raises(capi.B200Error, match="column index out of range"):
+        sv.expval_sparse_device(dp.data_ptr(), bad.data_ptr(), dv.data_ptr(), data.size)
+    with pytest.raises(capi.B200Error, match="more non-zeros"):
+        sv.expval_sparse_device(dp.data_ptr(), di.data_ptr(), dv.data_ptr(), data.size - 3)
+    rows = dp.clone()
+    rows[5], rows[6] = dp[6], dp[5]
+    with pytest.raises(capi.B200Error, match="non-decreasing"):
+        sv.expval_sparse_device(rows.data_ptr(), di.data_ptr(), dv.data_ptr(), data.size)
+
+
 def test_sparse_rejects_bad_csr(capi):
     sv = capi.StateVector(2)
     rows = np.array([0, 1, 2, 3, 4], dtype=np.uint64)
