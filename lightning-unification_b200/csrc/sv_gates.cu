@@ -138,6 +138,32 @@ __global__ void __launch_bounds__(kThreads) k_dense(States s, DenseP<R, K> p) {
     }
 }
 
+// A one-wire matrix on state bit 0: the pair of a group is two adjacent amplitudes, which the
+// group-per-thread kernel reads and writes with two half-used 32-byte sectors per access.
+// Here each thread owns one amplitude (fully coalesced loads and stores), takes its partner
+// from the neighbouring lane and forms its own output row with the same FMA order.
+template <typename R> struct Dense1LowP {
+    uint64_t n;
+    C<R> m[4];
+};
+template <typename R>
+__global__ void __launch_bounds__(kThreads) k_dense1_low(States s, Dense1LowP<R> p) {
+    C<R> *__restrict__ sv = static_cast<C<R> *>(s.p[blockIdx.y]);
+    // n and the stride are multiples of 32, so every lane of a warp makes the same trips
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < p.n;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const C<R> v = sv[i];
+        C<R> o;
+        o.x = __shfl_xor_sync(0xffffffffu, v.x, 1);
+        o.y = __shfl_xor_sync(0xffffffffu, v.y, 1);
+        const bool hi = i & 1;
+        CAcc<R> a;
+        a.add(hi ? p.m[2] : p.m[0], hi ? o : v);
+        a.add(hi ? p.m[3] : p.m[1], hi ? v : o);
+        sv[i] = a.get();
+    }
+}
+
 template <typename R, int K>
 __global__ void __launch_bounds__(kThreads) k_dense_dev(States s, DenseDevP<R, K> p) {
     C<R> *__restrict__ sv = static_cast<C<R> *>(s.p[blockIdx.y]);
@@ -426,6 +452,15 @@ bool launch_dense_k(const States &S, int ns, uint32_t nq, const GateDesc &g, voi
             return true;
         }
         if constexpr (K > 6) return false;
+    }
+    if constexpr (K == 1) {
+        if (g.cbits.empty() && g.tbits[0] == 0 && nq >= 5) {
+            Dense1LowP<R> p{};
+            p.n = uint64_t(1) << nq;
+            for (int i = 0; i < 4; ++i) p.m[i] = cvt<R>(g.m[i]);
+            k_dense1_low<R><<<grid_for(p.n, ns), kThreads, 0, st>>>(S, p);
+            return true;
+        }
     }
     if constexpr (K <= 3) {
         DenseP<R, K> p{};
