@@ -671,27 +671,28 @@ __global__ void __launch_bounds__(kDiagThreads) k_pauli_diag(const C<R> *__restr
                 v[j] = hi ? o - v[j] : v[j] + o;
             }
         }
-        // bits 7-9: warp bits 0-2, through shared memory
+        // bits 7-9: warp bits 0-2, through shared memory laid out value-major (w[j * 256 +
+        // thread]) so a warp's accesses fall in distinct banks
         __syncthreads();  // the previous tile's words have read w
 #pragma unroll
         for (int s = 0; s < 3; ++s) {
 #pragma unroll
-            for (int j = 0; j < 4; ++j) w[4 * tid + j] = v[j];
+            for (int j = 0; j < 4; ++j) w[j * kDiagThreads + tid] = v[j];
             __syncthreads();
             const bool hi = (warp >> s) & 1;
-            const int partner = 4 * (tid ^ (32 << s));
+            const int partner = tid ^ (32 << s);
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
-                const double o = w[partner + j];
+                const double o = w[j * kDiagThreads + partner];
                 v[j] = hi ? o - v[j] : v[j] + o;
             }
             __syncthreads();
         }
 #pragma unroll
-        for (int j = 0; j < 4; ++j) w[4 * tid + j] = v[j];
+        for (int j = 0; j < 4; ++j) w[j * kDiagThreads + tid] = v[j];
         __syncthreads();
         if (has_word) {
-            const double x = w[zlo];
+            const double x = w[(zlo & 3u) * kDiagThreads + (zlo >> 2)];  // W[k], k = 4 * thread + j
             acc += (__popcll(t & zhi) & 1) ? -x : x;
         }
     }
