@@ -271,7 +271,7 @@ void apply_observable(b200sv_state *h, const ObsRec &o, const void *psi, void *o
 }
 
 // per-term Pauli values of an all-Pauli observable (host vector, term order).  Words sorted by
-// X mask.  Diagonal words (two or more, 10+ qubits) share Walsh-Hadamard passes of
+// X mask.  Diagonal words (two or more, 12+ qubits) share Walsh-Hadamard passes of
 // reduce_pauli_diag, up to 256 per pass.  Words whose X mask stays below 4 MiB of amplitudes
 // share passes of reduce_pauli_multi, up to 32 per pass, their partner amplitudes coming from
 // L2; each wider X mask gets pair passes of reduce_pauli_group, where a thread reads both
@@ -293,7 +293,7 @@ std::vector<double> pauli_term_values(b200sv_state *h, const void *psi, const st
     // diagonal words (sorted first): Walsh-Hadamard passes, any number of words per read
     size_t ndiag = 0;
     while (ndiag < order.size() && words[order[ndiag]].xmask == 0) ++ndiag;
-    const bool diag_pass = h->nq >= 10 && ndiag >= 2;
+    const bool diag_pass = h->nq >= 12 && ndiag >= 2;
     if (diag_pass) {
         for (size_t d = 0; d < ndiag; d += 256) passes.push_back(Pass{d, std::min<size_t>(256, ndiag - d), true, true});
         i = ndiag;

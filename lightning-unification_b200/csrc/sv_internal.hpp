@@ -66,7 +66,7 @@ template <typename R>
 void reduce_pauli_group(const void *psi, uint32_t nq, const PauliWord *terms, int nterms,
                         double *partials, double *out_dev, cudaStream_t st, bool with_norm = false);
 // out_dev[t] = <psi|Z_(zmask_dev[t])|psi> for up to 256 diagonal words (device masks), one
-// pass over a state of at least 10 qubits.
+// pass over a state of at least 12 qubits.
 template <typename R>
 void reduce_pauli_diag(const void *psi, uint32_t nq, const uint64_t *zmask_dev, int nwords, double *partials,
                        size_t partials_cap, double *out_dev, cudaStream_t st);

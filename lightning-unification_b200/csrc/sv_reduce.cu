@@ -623,80 +623,79 @@ void reduce_pauli_group(const void *psi, uint32_t nq, const PauliWord *terms, in
 }
 
 // ---- diagonal Pauli words (Z and I factors only), any number in one pass -----------------
-// Per tile of 1024 consecutive amplitudes (state bits 0-9), the Walsh-Hadamard transform of
+// Per tile of 4096 consecutive amplitudes (state bits 0-11), the Walsh-Hadamard transform of
 // the probabilities, W[k] = sum_m (-1)^popcount(m & k) p_(base + m), holds every diagonal
-// word's restriction to the tile: <Z_z> gains (-1)^popcount(tile & (z >> 10)) W[z & 1023].
-// The transform costs ten FP64 additions per amplitude whatever the number of words (bits
-// 0-1 in registers, 2-6 across lanes with shuffles, 7-9 across warps in shared memory, in a
-// fixed order); thread t then accumulates word t.  256 threads, four amplitudes each.
+// word's restriction to the tile: <Z_z> gains (-1)^popcount(tile & (z >> 12)) W[z & 4095].
+// The transform costs twelve FP64 additions per amplitude whatever the number of words: each
+// thread holds 16 values and transforms four bits in registers, three times, with the tile
+// passed through shared memory between (bits 8-11, then 4-7, then 0-3; the stages commute),
+// under an XOR swizzle that keeps every phase's accesses free of bank conflicts.  Thread t
+// then accumulates word t.  256 threads.
 constexpr int kDiagThreads = 256;
 constexpr int kDiagMaxWords = 256;
+constexpr int kDiagTileBits = 12;
 struct PauliDiagP {
     uint64_t ntiles;
     int nwords;
 };
+__device__ __forceinline__ int diag_pos(int m) { return m ^ ((m >> 4) & 15); }
+__device__ __forceinline__ void fwht16(double (&v)[16]) {
+#pragma unroll
+    for (int h = 1; h < 16; h <<= 1) {
+#pragma unroll
+        for (int i = 0; i < 16; ++i) {
+            if (!(i & h)) {
+                const double a = v[i], b = v[i + h];
+                v[i] = a + b;
+                v[i + h] = a - b;
+            }
+        }
+    }
+}
 template <typename R>
 __global__ void __launch_bounds__(kDiagThreads) k_pauli_diag(const C<R> *__restrict__ a, PauliDiagP p,
                                                              const uint64_t *__restrict__ zmask, double *partials) {
-    __shared__ double w[1024];
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const bool has_word = tid < p.nwords;
-    const uint64_t z = has_word ? zmask[tid] : 0;
-    const uint32_t zlo = (uint32_t)(z & 1023u);
-    const uint64_t zhi = z >> 10;
+    __shared__ double w[1 << kDiagTileBits];
+    const int t = threadIdx.x;
+    const bool has_word = t < p.nwords;
+    const uint64_t z = has_word ? zmask[t] : 0;
+    const int zlo = (int)(z & ((1u << kDiagTileBits) - 1));
+    const uint64_t zhi = z >> kDiagTileBits;
     double acc = 0.0;
-    for (uint64_t t = blockIdx.x; t < p.ntiles; t += gridDim.x) {
-        const C<R> *src = a + (t << 10) + 4 * tid;
-        double v[4];
+    for (uint64_t tile = blockIdx.x; tile < p.ntiles; tile += gridDim.x) {
+        const C<R> *src = a + (tile << kDiagTileBits);
+        double v[16];
+        // bits 8-11 in registers: element m = t + 256 r (coalesced loads)
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            const double2 x = widen<R>(src[j]);
-            v[j] = x.x * x.x + x.y * x.y;
+        for (int r = 0; r < 16; ++r) {
+            const double2 x = widen<R>(src[t + 256 * r]);
+            v[r] = x.x * x.x + x.y * x.y;
         }
-        // bits 0, 1: in registers
-        {
-            const double a0 = v[0] + v[1], a1 = v[0] - v[1], a2 = v[2] + v[3], a3 = v[2] - v[3];
-            v[0] = a0 + a2;
-            v[1] = a1 + a3;
-            v[2] = a0 - a2;
-            v[3] = a1 - a3;
-        }
-        // bits 2-6: lane bits 0-4
-#pragma unroll
-        for (int s = 0; s < 5; ++s) {
-            const bool hi = (lane >> s) & 1;
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                const double o = __shfl_xor_sync(0xffffffffu, v[j], 1 << s);
-                v[j] = hi ? o - v[j] : v[j] + o;
-            }
-        }
-        // bits 7-9: warp bits 0-2, through shared memory laid out value-major (w[j * 256 +
-        // thread]) so a warp's accesses fall in distinct banks
+        fwht16(v);
         __syncthreads();  // the previous tile's words have read w
 #pragma unroll
-        for (int s = 0; s < 3; ++s) {
+        for (int r = 0; r < 16; ++r) w[diag_pos(t + 256 * r)] = v[r];
+        __syncthreads();
+        // bits 4-7: m = (t & 15) | r << 4 | (t >> 4) << 8
 #pragma unroll
-            for (int j = 0; j < 4; ++j) w[j * kDiagThreads + tid] = v[j];
-            __syncthreads();
-            const bool hi = (warp >> s) & 1;
-            const int partner = tid ^ (32 << s);
+        for (int r = 0; r < 16; ++r) v[r] = w[diag_pos((t & 15) | (r << 4) | ((t >> 4) << 8))];
+        fwht16(v);
 #pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                const double o = w[j * kDiagThreads + partner];
-                v[j] = hi ? o - v[j] : v[j] + o;
-            }
-            __syncthreads();
-        }
+        for (int r = 0; r < 16; ++r) w[diag_pos((t & 15) | (r << 4) | ((t >> 4) << 8))] = v[r];
+        __syncthreads();
+        // bits 0-3: m = r | t << 4
 #pragma unroll
-        for (int j = 0; j < 4; ++j) w[j * kDiagThreads + tid] = v[j];
+        for (int r = 0; r < 16; ++r) v[r] = w[diag_pos(r | (t << 4))];
+        fwht16(v);
+#pragma unroll
+        for (int r = 0; r < 16; ++r) w[diag_pos(r | (t << 4))] = v[r];
         __syncthreads();
         if (has_word) {
-            const double x = w[(zlo & 3u) * kDiagThreads + (zlo >> 2)];  // W[k], k = 4 * thread + j
-            acc += (__popcll(t & zhi) & 1) ? -x : x;
+            const double x = w[diag_pos(zlo)];
+            acc += (__popcll(tile & zhi) & 1) ? -x : x;
         }
     }
-    if (has_word) partials[(size_t)tid * gridDim.x + blockIdx.x] = acc;
+    if (has_word) partials[(size_t)t * gridDim.x + blockIdx.x] = acc;
 }
 
 template <typename R>
@@ -704,9 +703,9 @@ void reduce_pauli_diag(const void *psi, uint32_t nq, const uint64_t *zmask_dev, 
                        size_t partials_cap, double *out, cudaStream_t st) {
     if (nwords <= 0) return;
     if (nwords > kDiagMaxWords) throw ArgError("at most 256 diagonal Pauli words per pass");
-    if (nq < 10) throw Unsupported("diagonal Pauli pass needs at least 10 qubits");
+    if (nq < (uint32_t)kDiagTileBits) throw Unsupported("diagonal Pauli pass needs at least 12 qubits");
     PauliDiagP p{};
-    p.ntiles = uint64_t(1) << (nq - 10);
+    p.ntiles = uint64_t(1) << (nq - kDiagTileBits);
     p.nwords = nwords;
     const uint64_t cap = std::min<uint64_t>(kMaxRedBlocks, partials_cap / (size_t)nwords);
     const int nb = (int)std::max<uint64_t>(1, std::min<uint64_t>(p.ntiles, cap));

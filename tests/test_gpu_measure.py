@@ -120,6 +120,25 @@ def test_pauli_passes_near_and_far(capi, dtype):
         assert abs(sv.var(terms) - O.var(st64, terms)) < tol * 10
 
 
+@pytest.mark.parametrize("n", [12, 13, 15])
+def test_diagonal_pauli_words_one_pass(capi, n):
+    """Many diagonal words (Z and I factors, masks on low, high and both halves of the
+    4096-amplitude tiles) in the Walsh-Hadamard pass, from one tile (12 qubits) up."""
+    import lq_oracle as O
+    rng = np.random.default_rng(40 + n)
+    st = random_state(rng, n)
+    sv = capi.StateVector(n)
+    sv.upload(st)
+    words = []
+    for _ in range(300):
+        k = int(rng.integers(1, 5))
+        ws = [int(w) for w in rng.choice(n, k, replace=False)]
+        words.append(("".join("Z" if rng.random() < 0.8 else "I" for _ in ws), ws))
+    per, _ = sv.expval_pauli(words)
+    want = [O.pauli_expval(st, wd, ws) for wd, ws in words]
+    assert np.abs(per - want).max() < 1e-12
+
+
 @pytest.mark.parametrize("dtype", [np.complex128, np.complex64])
 def test_apply_observable_in_place(capi, dtype):
     """psi <- O psi (Observable::applyInPlace): named, tensor, Hermitian and Hamiltonian."""
