@@ -77,7 +77,7 @@ void reduce_pauli_multi(const void *psi, uint32_t nq, const PauliWord *terms, in
                         double *partials, double *out_dev, cudaStream_t st);
 // out_dev[0] = Re <psi| M |psi> for a dense Hermitian M on k <= 4 bits (matrix on device).
 template <typename R>
-void reduce_dense_expval(const void *psi, uint32_t nq, const GateDesc &g, const void *dev_matrix,
+void reduce_dense_expval(const void *psi, uint32_t nq, const GateDesc &g, void *dev_matrix,
                          double *partials, double *out_dev, cudaStream_t st);
 // One adjoint step of a one-wire gate on state bit `bit`: out_dev[o * out_stride] = alpha *
 // Im <bra_o| G |lambda> (G the 2x2 generator), then lambda and every bra <- U lambda, U bra

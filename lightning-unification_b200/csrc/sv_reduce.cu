@@ -745,7 +745,7 @@ void reduce_pauli_multi(const void *psi, uint32_t nq, const PauliWord *terms, in
 
 
 template <typename R>
-void reduce_dense_expval(const void *psi, uint32_t nq, const GateDesc &g, const void *dev_matrix, double *partials,
+void reduce_dense_expval(const void *psi, uint32_t nq, const GateDesc &g, void *dev_matrix, double *partials,
                          double *out, cudaStream_t st) {
     if (g.kind != Kind::Dense || g.k > 4 || !g.cbits.empty()) throw Unsupported("dense expval needs k <= 4");
     DenseEvP<R> p{};
@@ -760,7 +760,7 @@ void reduce_dense_expval(const void *psi, uint32_t nq, const GateDesc &g, const 
     }
     std::vector<C<R>> hm(g.m.size());
     for (size_t i = 0; i < g.m.size(); ++i) hm[i] = cvt<R>(g.m[i]);
-    B200SV_CUDA(cudaMemcpyAsync(const_cast<void *>(dev_matrix), hm.data(), hm.size() * sizeof(C<R>),
+    B200SV_CUDA(cudaMemcpyAsync(dev_matrix, hm.data(), hm.size() * sizeof(C<R>),
                                 cudaMemcpyHostToDevice, st));
     const int nb = red_blocks(p.ngroups);
     const C<R> *a = static_cast<const C<R> *>(psi), *m = static_cast<const C<R> *>(dev_matrix);
@@ -848,9 +848,12 @@ struct AdjRotP {
 template <typename R> struct AdjRotMat {
     C<R> u[4];  // the inverse gate, row-major
 };
+template <typename R> struct MutBras {
+    C<R> *p[16];  // the bras, updated in place
+};
 template <typename R, int NB>
-__global__ void __launch_bounds__(kRT) k_adj_rot(C<R> *__restrict__ lambda, Bras<R> bras, AdjRotP p, AdjRotMat<R> um,
-                                                 double *partials, GenFinal fin) {
+__global__ void __launch_bounds__(kRT) k_adj_rot(C<R> *__restrict__ lambda, MutBras<R> bras, AdjRotP p,
+                                                 AdjRotMat<R> um, double *partials, GenFinal fin) {
     __shared__ double sm[NB * 32];
     double acc[NB];
 #pragma unroll
@@ -869,7 +872,7 @@ __global__ void __launch_bounds__(kRT) k_adj_rot(C<R> *__restrict__ lambda, Bras
 #pragma unroll
         for (int o = 0; o < NB; ++o) {
             if (o < p.nbra) {
-                C<R> *b = const_cast<C<R> *>(bras.p[o]);
+                C<R> *b = bras.p[o];
                 const C<R> c0 = b[i0], c1 = b[i1];
                 const double2 b0 = widen<R>(c0), b1 = widen<R>(c1);
                 acc[o] += (b0.x * w0.y - b0.y * w0.x) + (b1.x * w1.y - b1.y * w1.x);  // Im conj(b) w
@@ -928,8 +931,8 @@ void adjoint_rot_step(void *lambda, void *const *bras, int nbra, uint32_t nq, ui
     p.nbra = nbra;
     AdjRotMat<R> um{};
     for (int i = 0; i < 4; ++i) um.u[i] = cvt<R>(u[i]);
-    Bras<R> B{};
-    for (int o = 0; o < nbra; ++o) B.p[o] = static_cast<const C<R> *>(bras[o]);
+    MutBras<R> B{};
+    for (int o = 0; o < nbra; ++o) B.p[o] = static_cast<C<R> *>(bras[o]);
     const int nb = red_blocks(p.npairs);
     const GenFinal fin{arrival, out, out_stride, alpha};
     C<R> *lam = static_cast<C<R> *>(lambda);
@@ -1002,7 +1005,7 @@ template <typename R> void axpy(void *acc, const void *x, uint32_t nq, double c,
                                        double *, cudaStream_t);                                                 \
     template void reduce_pauli_multi<R>(const void *, uint32_t, const PauliWord *, int, double *, double *,     \
                                         cudaStream_t);                                                          \
-    template void reduce_dense_expval<R>(const void *, uint32_t, const GateDesc &, const void *, double *,      \
+    template void reduce_dense_expval<R>(const void *, uint32_t, const GateDesc &, void *, double *,      \
                                          double *, cudaStream_t);                                               \
     template void reduce_generator_inner<R>(void *const *, int, const void *, uint32_t, const GateDesc &,       \
                                             double, double *, double *, int, cudaStream_t, unsigned int *);     \
