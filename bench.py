@@ -181,59 +181,123 @@ def timed(fn, steps, warmup, stream=None):
     return e0.elapsed_time(e1) / steps  # ms
 
 
-def gate_sweep_30q(nq: int, hbm_peak: float):
-    """Per-gate HBM throughput at nq qubits (complex128); roofline of the dense 1-qubit gate kernel."""
+SWEEP_TOUCHED = {"Hadamard": 1.0, "RX": 1.0, "RY": 1.0, "RZ": 1.0, "CNOT": 0.5, "CZ": 0.25, "SWAP": 0.5,
+                 "Toffoli": 0.25, "U2": 1.0, "U3": 1.0}  # fraction of the amplitudes each gate can change
+
+
+def _sweep_call(target, kind, wires, mat):
+    """One gate of the sweep set on `target` (this engine's StateVector or the reference's StateVectorC128)."""
+    if kind in ("U2", "U3"):
+        if hasattr(target, "apply_matrix"):
+            return lambda: target.apply_matrix(mat, wires)
+        flat = np.ascontiguousarray(mat.reshape(-1))
+        return lambda: target.applyMatrix(flat, wires, False)
+    params = [0.3] if kind in ("RX", "RY", "RZ") else []
+    if hasattr(target, "apply"):
+        return lambda: target.apply(kind, wires, False, params)
+    return lambda: getattr(target, kind)(wires, False, params)
+
+
+def gate_sweep(nq: int, hbm_peak: float, cpu: bool, draws: int = 6):
+    """The gate-throughput configuration at nq qubits, complex128: for each gate kind of the sweep
+    set, `draws` launches on uniformly drawn distinct wires (seeded), each timed alone with CUDA
+    events (the state is larger than L2 from 26 qubits); GB/s of the amplitudes the gate can
+    change (2 x 16 B each) and of the whole state.  Then the 200-gate random sequence per gate
+    and fused.  Beside each gate, when the reference module is built and the host has the
+    memory, the reference's own lightning.qubit on the same wires (fewer draws: its gate
+    kernels are single-threaded), host clock around each call."""
     import torch
     from lightning_b200 import capi
-    from lightning_b200.workloads import gate_sweep, random_unitary
+    from lightning_b200.workloads import gate_sweep as sweep_ops, random_unitary
     sv = capi.StateVector(nq, np.complex128)
     stream = torch.cuda.current_stream()
     sv.set_stream(stream.cuda_stream)
     N = 1 << nq
     state_bytes = 16 * N
-    rng = np.random.default_rng(0)
-    u2, u3 = random_unitary(rng, 2), random_unitary(rng, 3)
-    kinds = {
-        "Hadamard": lambda: sv.apply("Hadamard", [nq // 2]),
-        "RX": lambda: sv.apply("RX", [3], False, [0.3]),
-        "RY(wire n-1)": lambda: sv.apply("RY", [nq - 1], False, [0.3]),
-        "RZ": lambda: sv.apply("RZ", [7], False, [0.3]),
-        "CNOT": lambda: sv.apply("CNOT", [2, nq - 3]),
-        "CZ": lambda: sv.apply("CZ", [5, 9]),
-        "SWAP": lambda: sv.apply("SWAP", [1, nq - 2]),
-        "Toffoli": lambda: sv.apply("Toffoli", [0, 4, nq - 1]),
-        "U2": lambda: sv.apply_matrix(u2, [6, nq - 5]),
-        "U3": lambda: sv.apply_matrix(u3, [2, 11, nq - 7]),
-    }
-    # amplitudes each gate can change (algorithmic bytes = 2 x 16 B x that count)
-    touched = {"Hadamard": N, "RX": N, "RY(wire n-1)": N, "RZ": N, "CNOT": N // 2, "CZ": N // 4, "SWAP": N // 2,
-               "Toffoli": N // 4, "U2": N, "U3": N}
+    rng = np.random.default_rng(100 + nq)
+    plan = {}
+    for kind in SWEEP_TOUCHED:
+        k = {"CNOT": 2, "CZ": 2, "SWAP": 2, "Toffoli": 3, "U2": 2, "U3": 3}.get(kind, 1)
+        plan[kind] = [([int(w) for w in rng.choice(nq, k, replace=False)],
+                       random_unitary(rng, k) if kind in ("U2", "U3") else None) for _ in range(draws)]
     per = {}
-    for k, f in kinds.items():
-        ms = timed(f, 5, 2, stream)
-        per[k] = {"ms": ms, "gbs_touched": 2 * 16 * touched[k] / (ms * 1e6), "gbs_state": 2 * state_bytes / (ms * 1e6)}
-    ops = gate_sweep(nq, 200, seed=7)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for kind, draws_k in plan.items():
+        for wires, mat in draws_k[:1]:
+            f = _sweep_call(sv, kind, wires, mat)
+            f(); f()
+        ms = []
+        for wires, mat in draws_k:
+            f = _sweep_call(sv, kind, wires, mat)
+            torch.cuda.synchronize()
+            e0.record(stream)
+            f()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        touched = 2 * 16 * N * SWEEP_TOUCHED[kind]
+        g = [touched / (m * 1e6) for m in ms]
+        per[kind] = {"ms_mean": float(np.mean(ms)), "gbs_touched_mean": float(np.mean(g)),
+                     "gbs_touched_min": float(min(g)), "gbs_touched_max": float(max(g)),
+                     "hbm_frac_mean": float(np.mean(g)) / hbm_peak,
+                     "gbs_state_mean": float(np.mean([2 * state_bytes / (m * 1e6) for m in ms])),
+                     "wires": [w for w, _ in draws_k]}
+    ops = sweep_ops(nq, 200, seed=7)
     sweep = {}
+    ol = capi.OpList(ops, np.complex128)
     for label, fn in (("unfused", sv.apply_ops), ("fused", sv.apply_ops_fused)):
-        fn(ops[:10])  # warm
+        fn(capi.OpList(ops[:10], np.complex128))  # warm
         sv.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        fn(ops)
+        fn(ol)
         e1.record(stream)
         torch.cuda.synchronize()
         sweep[label] = e0.elapsed_time(e1)
-    sweep_ms = sweep
-    dense = per["RX"]
-    roof = {"bound": "hbm", "kernel": f"k_dense<double,1> (RX, {nq} qubits complex128)",
-            "achieved": dense["gbs_touched"], "peak": hbm_peak, "unit": "GB/s",
-            "frac": dense["gbs_touched"] / hbm_peak,
-            "traffic": RX_DRAM_BYTES_26Q * float(1 << (nq - 26)),
-            "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one 26-qubit launch "
-                              "(profiles/k_dense_rx_c128_26q.md), scaled by the state size",
-            "algorithmic_bytes_per_launch": 2 * state_bytes}
     sv.close()
-    return per, sweep_ms, roof
+    out = {"qubits": nq, "dtype": "c128", "per_gate": per, "sweep_200_gates_ms": sweep,
+           "fused_speedup": sweep["unfused"] / sweep["fused"]}
+    if cpu and nq <= 30:
+        import psutil
+        import ref  # the reference module built from its sources: the CPU baseline only
+        m = ref.load()
+        if m is None:
+            out["reference_cpu"] = "not timed: reference module not built"
+        elif psutil.virtual_memory().available < 3 * state_bytes:
+            out["reference_cpu"] = f"not timed: the host has less than {3 * state_bytes / 2**30:.0f} GiB free"
+        else:
+            host = np.full(N, 1 / np.sqrt(N), dtype=np.complex128)
+            svr = m.StateVectorC128(host)
+            nref = {26: 3, 28: 2}.get(nq, 1)
+            for kind, draws_k in plan.items():
+                ts = []
+                for wires, mat in draws_k[:nref]:
+                    f = _sweep_call(svr, kind, wires, mat)
+                    t0 = time.perf_counter()
+                    f()
+                    ts.append(time.perf_counter() - t0)
+                per[kind]["reference_cpu_gbs"] = float(np.mean([2 * 16 * N * SWEEP_TOUCHED[kind] / (t * 1e9)
+                                                                for t in ts]))
+            out["reference_cpu"] = {"draws_per_gate": nref, "threads": os.environ.get(
+                "OMP_NUM_THREADS", f"unset ({os.cpu_count()} cores; the gate kernels are single-threaded)")}
+            del svr, host
+    elif cpu:
+        out["reference_cpu"] = f"not timed: {nq} qubits ({state_bytes / 2**30:.0f} GiB) is beyond the host-timed sizes"
+    return out
+
+
+def sweep_roofline(sw30: dict, hbm_peak: float):
+    """Roofline of the dense one-wire kernel (RX, k_dense<double,1> or k_dense1_low on bit 0)
+    from the 30-qubit sweep's RX draws; traffic from one ncu capture of an RX launch on a
+    26-qubit complex128 state, scaled by the state size."""
+    nq = sw30["qubits"]
+    rx = sw30["per_gate"]["RX"]
+    return {"bound": "hbm", "kernel": f"k_dense<double,1> (RX on random wires, {nq} qubits complex128)",
+            "achieved": rx["gbs_touched_mean"], "peak": hbm_peak, "unit": "GB/s",
+            "frac": rx["gbs_touched_mean"] / hbm_peak,
+            "traffic": RX_DRAM_BYTES_26Q * float(1 << (nq - 26)),
+            "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one RX launch on a "
+                              "26-qubit complex128 state, scaled by the state size",
+            "algorithmic_bytes_per_launch": 2 * 16 * (1 << nq)}
 
 
 def rows_30q(nq: int, hbm_peak: float, cpu: bool, cpu_qubits: int = 26, steps: int = 3):
@@ -450,7 +514,7 @@ def matrix_sweep(nq: int, hbm_peak: float, kmax: int = 8, steps: int = 3):
 RX_DRAM_BYTES_26Q = 1.0737e9 + 1.0137e9
 
 # DRAM bytes (read + write) of the forward and VJP launches of the batched kernel on 148
-# circuits of the batched-adjoint workload, from an ncu capture (profiles/k_batch_c64_148circ.md);
+# circuits of the batched-adjoint workload, from an ncu capture of `bench.py --case batch`;
 # circuits are independent, so a step's traffic scales with the number of circuits.
 BATCH_DRAM_BYTES_148 = (0.0704e9 + 0.9838e9) + (3.1382e9 + 3.5036e9)
 BATCH_ISSUE_ACTIVE = 0.53  # scheduler cycles issuing, same capture (forward 51 %, VJP 53 %)
@@ -530,10 +594,13 @@ def run_case(args):
     print(json.dumps({"case": "batch", "ncirc": args.ncirc, "ms": ms, "circuits_per_s": args.ncirc / (ms / 1e3)}))
 
 
-def hea_forward(steps: int, warmup: int, ncirc: int = 4096, dtype=np.complex64):
+def hea_forward(steps: int, warmup: int, ncirc: int = 4096, dtype=np.complex64, cpu: bool = False):
     """Batched hardware-efficient-ansatz forward (n ~ U[10, 20], depth ~ U[4, 16], 3n-term
     Hamiltonian) in `dtype`, one persistent launch replayed as a CUDA graph, vs a per-circuit
-    loop through the plain C ABI on a sample (after one untimed circuit per width)."""
+    loop through the plain C ABI on a sample (after one untimed circuit per width).  With
+    `cpu`, the reference's own lightning.qubit on the host cores over a seeded subset (the
+    first 16 circuits: forward, then the Hamiltonian's expectation value as one observable),
+    extrapolated to the whole batch and labelled as such."""
     import torch
     from lightning_b200 import capi
     from lightning_b200.batch import BatchedCircuits
@@ -564,10 +631,29 @@ def hea_forward(steps: int, warmup: int, ncirc: int = 4096, dtype=np.complex64):
     for sv in handles.values():
         sv.close()
     err = float(np.abs(np.array(plain) - out[:nsample]).max())
-    return {"circuits": ncirc, "dtype": "c64" if np.dtype(dtype) == np.complex64 else "c128",
-            "value": ncirc / (ms / 1e3), "unit": "circuits/s",
-            "ms_per_step": ms, "per_circuit_loop": nsample / plain_s, "ratio": (ncirc / (ms / 1e3)) / (nsample / plain_s),
-            "max_abs_diff_vs_loop": err}
+    res = {"circuits": ncirc, "dtype": "c64" if np.dtype(dtype) == np.complex64 else "c128",
+           "value": ncirc / (ms / 1e3), "unit": "circuits/s",
+           "ms_per_step": ms, "per_circuit_loop": nsample / plain_s, "ratio": (ncirc / (ms / 1e3)) / (nsample / plain_s),
+           "max_abs_diff_vs_loop": err}
+    if cpu:
+        import ref  # the reference module built from its sources: the CPU baseline only
+        from lightning_b200.workloads import obs_terms
+        m = ref.load()
+        if m is not None:
+            rdt = np.complex64 if np.dtype(dtype) == np.complex64 else np.complex128
+            t0 = time.perf_counter()
+            vals = []
+            for c in circuits[:nsample]:
+                st_ = ref.run_circuit(m, c["num_qubits"], bind(c, params_np), rdt)
+                vals.append(ref.expval(m, st_, obs_terms(c["observables"][0])))
+            dt = time.perf_counter() - t0
+            res["reference_cpu"] = {"sample_circuits": nsample, "circuits_per_s": nsample / dt,
+                                    "extrapolated_batch_s": dt / nsample * ncirc,
+                                    "max_abs_diff_vs_batch": float(np.abs(np.array(vals) - out[:nsample]).max()),
+                                    "note": "seeded subset, extrapolated to the whole batch by circuit count",
+                                    "threads": os.environ.get("OMP_NUM_THREADS", f"unset ({os.cpu_count()} cores)")}
+            res["ratio_vs_reference_cpu"] = res["value"] / (nsample / dt)
+    return res
 
 
 def plain_layered(cpu: bool, reps: int = 3):
@@ -652,11 +738,21 @@ def sampling_case(nq: int, shots: int = 10_000_000):
             "chi2_per_dof": chi2 / max(dof, 1)}
 
 
+def product_marginal(thetas, wires):
+    """probs(wires) of the product state RY(theta_q)|0> on every wire, in FP64 (closed form)."""
+    out = np.ones(1)
+    for w in wires:
+        out = np.kron(out, [np.cos(thetas[w] / 2) ** 2, np.sin(thetas[w] / 2) ** 2])
+    return out
+
+
 def precision_case(nq: int, dtype, shots: int = 10_000_000):
     """Full-size precision and sampling run: RY layer + QFT ladder (fused) on an nq-qubit
     state, probs over every wire into device memory (2^nq doubles), then `shots` samples by
     the fixed-order inverse CDF.  Size-independent checks: |norm^2 - 1|, |sum(probs) - 1|,
-    chi-squared of the sampled top-10-wire marginal."""
+    chi-squared of the sampled top-10-wire marginal.  Then the inverse QFT (fused) returns
+    the RY product state, whose <Z_q> = cos(theta_q) and marginals are known in FP64: the
+    errors of the engine's expectation values and marginals against that FP64 answer."""
     import torch
     from lightning_b200 import capi
     from lightning_b200.workloads import qft_circuit
@@ -692,12 +788,58 @@ def precision_case(nq: int, dtype, shots: int = 10_000_000):
     chi2 = float(((hist[mask] - expct[mask]) ** 2 / expct[mask]).sum())
     dof = int(mask.sum()) - 1
     amp = np.dtype(dtype).itemsize
+    # known answer: the inverse QFT brings back the RY product state
+    thetas = [op[3][0] for op in ops[:nq]]
+    undo = [(name, wires, not inv, params) for name, wires, inv, params in reversed(ops[nq:])]
+    e0.record(st)
+    sv.apply_ops_fused(undo)
+    e1.record(st)
+    torch.cuda.synchronize()
+    t_undo = e0.elapsed_time(e1) / 1e3
+    z, _ = sv.expval_pauli([("Z", [q]) for q in range(nq)])
+    marg_err = 0.0
+    for wires in (list(range(10)), list(range(nq - 10, nq)), [0, 15, 16, 30, nq - 1]):
+        marg_err = max(marg_err, float(np.abs(sv.probs(wires) - product_marginal(thetas, wires)).max()))
+    known = {"circuit": "RY layer + QFT + inverse QFT = RY product state", "inverse_qft_s": t_undo,
+             "max_abs_err_expval_z": float(np.abs(z - np.cos(thetas)).max()),
+             "max_abs_err_marginals": marg_err, "norm2_err": abs(sv.norm2() - 1.0),
+             "marginals": "wires 0-9, the last 10, and (0, 15, 16, 30, n-1)"}
     sv.close()
     return {"qubits": nq, "dtype": "c64" if np.dtype(dtype) == np.complex64 else "c128",
             "state_gib": (amp << nq) / 2**30, "gates": len(ops), "gates_fused_s": t_gates,
             "norm2_err": norm_err, "probs_s": t_probs, "probs_gbs": ((amp + 8) << nq) / t_probs / 1e9,
             "probs_sum_err": psum_err, "shots": shots, "sample_s": t_sample, "shots_per_s": shots / t_sample,
-            "chi2_per_dof": chi2 / max(dof, 1), "chi2_dof": dof}
+            "chi2_per_dof": chi2 / max(dof, 1), "chi2_dof": dof, "vs_fp64_closed_form": known}
+
+
+def precision_vs_reference(nq: int = 24):
+    """The same circuit family at nq qubits against the reference's own complex128 lightning.qubit
+    on the host (FP64): max |probs difference| over every basis state, a 10-wire marginal and a
+    four-term Pauli Hamiltonian, for the complex128 and complex64 engines."""
+    import ref  # the reference module built from its sources: the FP64 answer only
+    from lightning_b200 import capi
+    from lightning_b200.workloads import qft_circuit
+    m = ref.load()
+    if m is None:
+        return {"unavailable": "reference module not built"}
+    ops = qft_circuit(nq, seed=9)
+    t0 = time.perf_counter()
+    psi = ref.run_circuit(m, nq, ops)
+    t_ref = time.perf_counter() - t0
+    ham = [(0.7, [("PauliZ", [0]), ("PauliX", [5])]), (-1.3, [("PauliY", [nq - 1])]),
+           (0.4, [("PauliX", [11]), ("PauliX", [12])]), (2.1, [("PauliZ", [17])])]
+    ev_ref = ref.expval(m, psi.copy(), ham)
+    marg_ref = ref.probs(m, psi.copy(), list(range(10)))
+    p_ref = np.abs(psi) ** 2
+    out = {"qubits": nq, "gates": len(ops), "reference_cpu_s": t_ref}
+    for dt, label in ((np.complex128, "c128"), (np.complex64, "c64")):
+        sv = capi.StateVector(nq, dt)
+        sv.apply_ops_fused(ops)
+        out[label] = {"max_abs_err_probs": float(np.abs(sv.probs() - p_ref).max()),
+                      "max_abs_err_marginal_10": float(np.abs(sv.probs(list(range(10))) - marg_ref).max()),
+                      "abs_err_expval": abs(sv.expval(ham) - ev_ref)}
+        sv.close()
+    return out
 
 
 def precision_compare(nq: int = 32, k: int = 16):
@@ -846,7 +988,8 @@ def main():
         err = max(err, float(np.abs(g_np[slots] - grads_plain[ci]).max()))
     sv.close()
 
-    per, sweep_ms, roof = gate_sweep_30q(args.sweep_qubits, hbm_peak)
+    sweeps = {str(q): gate_sweep(q, hbm_peak, not args.no_cpu) for q in (26, 28, 30, 32)}
+    roof = sweep_roofline(sweeps["30"], hbm_peak)
     roof["peak_kind"] = peak_kind
     msweep = matrix_sweep(args.sweep_qubits, hbm_peak)
     rows = rows_30q(args.sweep_qubits, hbm_peak, not args.no_cpu)
@@ -855,10 +998,14 @@ def main():
     cpu = None if args.no_cpu else reference_cpu(circuits, params_np, dy_np, 4)
     del eng
     torch.cuda.empty_cache()
-    hea = hea_forward(3, 3)
-    hea128 = hea_forward(3, 3, dtype=np.complex128)
+    hea = hea_forward(3, 3, cpu=not args.no_cpu)
+    hea128 = hea_forward(3, 3, dtype=np.complex128, cpu=not args.no_cpu)
     samp = sampling_case(28)
     plain20 = plain_layered(not args.no_cpu)
+    precision = {"c64_33q": precision_case(33, np.complex64), "c128_32q": precision_case(32, np.complex128),
+                 "c64_vs_c128_32q": precision_compare(32)}
+    if not args.no_cpu:
+        precision["vs_reference_24q"] = precision_vs_reference(24)
     line = {
         "metric": METRIC, "value": value, "unit": "circuits/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
@@ -873,9 +1020,7 @@ def main():
                   "path": "C ABI, one gate per launch: apply_ops + 16 Pauli expvals + adjoint VJP"},
         "ratio_vs_plain": value / world / plain_value,
         "max_grad_err_vs_fp64": err,
-        "gate_sweep": {"qubits": args.sweep_qubits, "dtype": "c128", "per_gate": per,
-                       "sweep_200_gates_ms": sweep_ms,
-                       "fused_speedup": sweep_ms["unfused"] / sweep_ms["fused"]},
+        "gate_sweep": sweeps,
         "matrix_sweep": msweep,
         "rows_single_state": rows,
         "rows_next": nxt,
@@ -883,6 +1028,7 @@ def main():
         "hea_batch_forward_c128": hea128,
         "sampling": samp,
         "plain_20q_layered": plain20,
+        "precision_sampling": precision,
         "roofline": roof,
         "roofline_batch": {
             "kernel": "k_batch<float,0|1,false> (forward + VJP launch of the headline step)",

@@ -281,8 +281,10 @@ int b200sv_sample_mcmc(b200sv_handle h, int proposal, uint64_t num_burnin,
  * state_device: 2^num_qubits amplitudes of `dtype` owned by the caller;
  * out_device: nterms doubles owned by the caller, receiving <psi|P_t|psi>;
  * words as in b200sv_expval_pauli.  At most B200SV_NOALLOC_MAX_TERMS words per
- * call (more is rejected with an error).  Work is queued on cuda_stream (NULL =
- * legacy default stream) and not synchronised.  Scratch is one static device
+ * call (more is rejected with an error).  state_device, out_device and
+ * cuda_stream must belong to the current CUDA device (pointers of another device
+ * are rejected with an error).  Work is queued on cuda_stream (NULL = legacy
+ * default stream) and not synchronised.  Scratch is one static device
  * array shared by all calls: calls that overlap on the GPU race, so serialise
  * them; the first call on a device sets up the array's address and should come
  * before any stream capture. */

@@ -52,6 +52,22 @@ double *scratch_address() {
     return g_addr[dev];
 }
 
+// The state and the output must be device memory of the current device, where the
+// scratch array's cached address is valid.  cudaPointerGetAttributes allocates nothing.
+void check_on_current_device(const void *ptr, const char *what) {
+    int dev = 0;
+    B200SV_CUDA(cudaGetDevice(&dev));
+    cudaPointerAttributes attr{};
+    const cudaError_t e = cudaPointerGetAttributes(&attr, ptr);
+    if (e != cudaSuccess) {
+        (void)cudaGetLastError();
+        throw ArgError(std::string("b200sv_expval_pauli_noalloc: ") + what + " is not a device pointer");
+    }
+    if ((attr.type != cudaMemoryTypeDevice && attr.type != cudaMemoryTypeManaged) || attr.device != dev)
+        throw ArgError(std::string("b200sv_expval_pauli_noalloc: ") + what +
+                       " must be device memory of the current device (" + std::to_string(dev) + ")");
+}
+
 struct WordsP {
     uint64_t xmask, hb_low, npairs;
     int nterms;
@@ -146,6 +162,8 @@ extern "C" int b200sv_expval_pauli_noalloc(const void *state_device, uint32_t nu
         if (nterms > B200SV_NOALLOC_MAX_TERMS)
             throw ArgError("b200sv_expval_pauli_noalloc: at most " + std::to_string(B200SV_NOALLOC_MAX_TERMS) +
                            " Pauli words per call (got " + std::to_string(nterms) + ")");
+        check_on_current_device(state_device, "state_device");
+        check_on_current_device(out_device, "out_device");
         if (nterms == 0) return;
         if (!offsets) throw ArgError("b200sv_expval_pauli_noalloc: NULL offsets");
         // Words, validated on the host (no device memory involved).

@@ -36,7 +36,7 @@ def test_apply_and_measure(D, dtype):
     ops = circuit(D)
     dev.apply(ops)
     want = O.run_circuit(4, oracle_ops(D, dev, ops))
-    tol = TOL[dtype] * 10
+    tol = TOL[dtype]
     assert np.abs(dev.state - want).max() < tol
     obs = {
         "named": D.named("PauliX", ["b"]),
@@ -55,8 +55,9 @@ def test_apply_and_measure(D, dtype):
     H = sp.random(16, 16, density=0.3, random_state=1) + 1j * sp.random(16, 16, density=0.3, random_state=2)
     H = H + H.conj().T
     so = D.sparse_hamiltonian(H)
-    assert abs(dev.expval(so) - O.sparse_expval(want, *so.csr)) < tol * 10
-    assert abs(dev.var(so) - O.sparse_var(want, *so.csr)) < tol * 10
+    stol = tol if dtype == np.complex128 else tol * 10  # complex64: H entries up to ~2, values up to ~10
+    assert abs(dev.expval(so) - O.sparse_expval(want, *so.csr)) < stol
+    assert abs(dev.var(so) - O.sparse_var(want, *so.csr)) < stol
 
 
 def test_state_preparation(D):

@@ -36,7 +36,7 @@ def capi():
 @pytest.mark.parametrize("name", list(GATES))
 def test_gate_random_state(capi, name, inverse, dtype):
     import lq_oracle as O
-    rng = np.random.default_rng(abs(hash((name, inverse))) % 2**32)
+    rng = np.random.default_rng(1000 + 2 * list(GATES).index(name) + int(inverse))
     n = 9
     k, p = GATES[name]
     for _ in range(3):
@@ -48,7 +48,7 @@ def test_gate_random_state(capi, name, inverse, dtype):
         sv.apply(name, wires, inverse, params)
         got = sv.download()
         want = O.apply_op(st.astype(np.complex128), name, wires, inverse, params)
-        assert np.abs(got - want).max() < TOL[dtype] * 10, (name, wires)
+        assert np.abs(got - want).max() < TOL[dtype], (name, wires)
 
 
 @pytest.mark.parametrize("name", ["CNOT", "CRY", "IsingXY", "SWAP", "CSWAP", "Toffoli", "DoubleExcitationPlus",
@@ -100,7 +100,7 @@ def test_apply_matrix(capi, k, dtype):
         sv.upload(st)
         sv.apply_matrix(u.astype(dtype), wires, inverse)
         want = O.apply_matrix(st.astype(np.complex128), u.astype(dtype).astype(np.complex128), wires, inverse)
-        assert np.abs(sv.download() - want).max() < TOL[dtype] * 20 * (1 << k)
+        assert np.abs(sv.download() - want).max() < TOL[dtype]
 
 
 @pytest.mark.parametrize("dtype", [np.complex128, np.complex64])
@@ -120,7 +120,7 @@ def test_apply_matrix_tiled(capi, k, dtype):
         sv.upload(st)
         sv.apply_matrix(u.astype(dtype), wires, inverse)
         want = O.apply_matrix(st.astype(np.complex128), u.astype(dtype).astype(np.complex128), wires, inverse)
-        assert np.abs(sv.download() - want).max() < TOL[dtype] * 20 * (1 << k)
+        assert np.abs(sv.download() - want).max() < TOL[dtype]
 
 
 GENS = ["PhaseShift", "RX", "RY", "RZ", "IsingXX", "IsingXY", "IsingYY", "IsingZZ", "CRX", "CRY", "CRZ",
