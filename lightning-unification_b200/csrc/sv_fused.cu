@@ -1,16 +1,30 @@
 // sv_fused.cu — one HBM pass for a run of gates on a single large state.
 //
 // The per-gate kernels (sv_gates.cu) read and write the whole state once per gate.
-// Here consecutive gates whose wires fit in one shared-memory tile of 2^kt amplitudes
-// form a segment: every CTA of a persistent grid takes tiles (the amplitudes that
-// share the values of the n - kt bits outside the tile), applies all of the segment's
-// gates to the tile in shared memory and writes it back.  Tiles always contain the
-// lowest state bits, so a tile is a set of contiguous 128-byte (or longer) runs, and
-// tiles are double-buffered: cp.async brings the next tile in while the current one
-// is computed and stored.  Gate coefficients come from the same compiled GateDesc as
-// the per-gate path (FP64 on the host, rounded once to the state's precision) and are
-// staged in shared memory once per CTA; complex64 outputs are compensated sums
-// (CAcc<float>), as in the per-gate kernels.
+// Here gates whose wires fit in one shared-memory tile of 2^kt amplitudes form a
+// segment: every CTA of a persistent grid takes tiles (the amplitudes that share the
+// values of the n - kt bits outside the tile), applies all of the segment's gates to
+// the tile and writes it back.  Tiles always contain the lowest state bits, so a tile is
+// a set of contiguous 128-byte (or longer) runs, and tiles are double-buffered: cp.async
+// brings the next tile in while the current one is computed and stored.
+//
+// Inside a tile the gates run in registers.  Each of the 512 threads holds A amplitudes
+// (8 for complex128, 16 for complex64) that differ in a = log2(A) "register bits" of the
+// tile; the other kt - a tile bits come from the thread index.  A phase is a run of gates
+// whose target bits all lie in the phase's register bits: the threads load their
+// amplitudes from shared memory once, apply every gate of the phase in registers and
+// store them back once.  Diagonal gates (phases, controlled phases, MultiRZ) and control
+// bits need no exchange at all, so they join any phase.  Only the hand-over between
+// phases goes through shared memory, and the tile buffers are XOR-swizzled so that those
+// exchanges are free of bank conflicts for most register-bit choices.
+//
+// Segments are formed with look-ahead: a gate joins the current segment when its bits fit
+// the tile and it commutes with every earlier gate that was left out (disjoint bits, or
+// both diagonal), so gates on wires that are already in the tile are pulled forward.
+//
+// Gate coefficients come from the same compiled GateDesc as the per-gate path (FP64 on
+// the host, rounded once to the state's precision); complex64 outputs are compensated
+// sums (CAcc<float>), as in the per-gate kernels.
 #include <algorithm>
 #include <cstring>
 #include <functional>
@@ -27,8 +41,25 @@ constexpr int kMaxGroupBits = 8;
 constexpr int kMaxSegOps = 96;
 constexpr int kMaxSegCoefs = 2048;
 
+// Tile geometry: 2^kt amplitudes (64 KiB) per tile, A = 2^kt / 512 amplitudes per thread.
+template <typename R> struct Geo;
+template <> struct Geo<double> { static constexpr int kt = 12, a = 3, A = 8, reserve = 3; };
+template <> struct Geo<float> { static constexpr int kt = 13, a = 4, A = 16, reserve = 4; };
+
+// Shared-memory position of tile amplitude l.  complex128: the three low bits are XORed
+// with bits 3..5, so eight threads whose amplitudes differ in any three of bits 0..5
+// (bits s and s+3 not both) hit eight different 16-byte bank groups.  complex64: bits
+// 1..3 XOR bits 4..6 (bit 0 stays, so the 16-byte pairs moved by cp.async stay together).
+template <typename R> __host__ __device__ __forceinline__ uint32_t swz(uint32_t l);
+template <> __host__ __device__ __forceinline__ uint32_t swz<double>(uint32_t l) { return l ^ ((l >> 3) & 7u); }
+template <> __host__ __device__ __forceinline__ uint32_t swz<float>(uint32_t l) {
+    return l ^ (((l >> 4) & 7u) << 1);
+}
+
+// ---- shared-memory forms (gates that do not fit the register bits) ---------------------
+
 // One gate in tile-local bit positions.
-struct FOp {
+struct alignas(16) FOp {
     int32_t kind;   // Kind
     int32_t k;      // target bits
     int32_t nb;     // group bits (targets and controls)
@@ -43,15 +74,6 @@ struct FOp {
     uint64_t pm_global;           // Parity: selected bits outside the tile (state positions)
 };
 
-struct SegArgs {
-    const FOp *ops;
-    const void *coefs;
-    int nops, ncoef;
-    int kt, ng;
-    uint8_t lbits[16];  // state position of tile bit i (ascending)
-    uint8_t gbits[48];  // state positions of the bits outside the tile (ascending)
-};
-
 __device__ __forceinline__ uint32_t ins_group(uint32_t g, const uint32_t *low, int nb) {
 #pragma unroll
     for (int j = 0; j < kMaxGroupBits; ++j) {
@@ -63,9 +85,6 @@ __device__ __forceinline__ uint32_t ins_group(uint32_t g, const uint32_t *low, i
     return g;
 }
 
-// The op's masks and offsets (and the coefficients of one- and two-wire gates) are copied
-// to registers before the group loop: the tile and the op records share shared memory, so
-// without the copies every store to the tile would force them to be read again.
 struct OpRegs {
     uint32_t low[kMaxGroupBits];
     uint32_t off[16];
@@ -83,122 +102,229 @@ template <int D> __device__ __forceinline__ OpRegs op_regs(const FOp &op) {
     return r;
 }
 
-template <typename R, int K>
-__device__ __forceinline__ void f_dense(C<R> *s, const FOp &op, const C<R> *cf, int kt) {
-    constexpr int D = 1 << K;
-    constexpr int NCR = K <= 2 ? D * D : 1;  // coefficients held in registers
-    const OpRegs o = op_regs<D>(op);
-    C<R> m[NCR];
-#pragma unroll
-    for (int i = 0; i < NCR; ++i) m[i] = cf[i];
-    const uint32_t ng = 1u << (kt - o.nb);
-    for (uint32_t g = threadIdx.x; g < ng; g += blockDim.x) {
-        const uint32_t b = ins_group(g, o.low, o.nb) | o.cmask;
-        C<R> v[D];
-#pragma unroll
-        for (int r = 0; r < D; ++r) v[r] = s[b + o.off[r]];
-#pragma unroll
-        for (int r = 0; r < D; ++r) {
-            CAcc<R> a;
-#pragma unroll
-            for (int c = 0; c < D; ++c) a.add(K <= 2 ? m[(r * D + c) % NCR] : cf[r * D + c], v[c]);
-            s[b + o.off[r]] = a.get();
-        }
-    }
-}
-
-template <typename R, int K>
-__device__ __forceinline__ void f_diag(C<R> *s, const FOp &op, const C<R> *cf, int kt) {
-    constexpr int D = 1 << K;
-    const OpRegs o = op_regs<D>(op);
-    C<R> m[D];
-#pragma unroll
-    for (int r = 0; r < D; ++r) m[r] = cf[r];
-    const uint32_t ng = 1u << (kt - o.nb);
-    for (uint32_t g = threadIdx.x; g < ng; g += blockDim.x) {
-        const uint32_t b = ins_group(g, o.low, o.nb) | o.cmask;
-#pragma unroll
-        for (int r = 0; r < D; ++r) {
-            CAcc<R> a;
-            a.add(m[r], s[b + o.off[r]]);
-            s[b + o.off[r]] = a.get();
-        }
-    }
-}
-
+// Givens block on two rows of a 2^k group, gamma on the other rows (double excitations):
+// the only form that runs on the shared-memory tile instead of in registers.
 template <typename R>
-__device__ __forceinline__ void f_swap(C<R> *s, const FOp &op, int kt) {
-    const OpRegs o = op_regs<1>(op);
-    const uint32_t ng = 1u << (kt - o.nb);
-    const uint32_t oa = op.off[op.ra], ob = op.off[op.rb];
-    for (uint32_t g = threadIdx.x; g < ng; g += blockDim.x) {
-        const uint32_t b = ins_group(g, o.low, o.nb) | o.cmask;
-        const C<R> t = s[b + oa];
-        s[b + oa] = s[b + ob];
-        s[b + ob] = t;
-    }
-}
-
-template <typename R>
-__device__ __forceinline__ void f_pair(C<R> *s, const FOp &op, const C<R> *cf, int kt) {
+__device__ void f_pair(C<R> *s, const FOp &op, const C<R> *cf, int kt) {
     const OpRegs o = op_regs<16>(op);
     const int D = 1 << op.k, ra = op.ra, rb = op.rb, rest = op.rest;
     C<R> m[5];
 #pragma unroll
     for (int i = 0; i < 5; ++i) m[i] = cf[i];
     const uint32_t ng = 1u << (kt - o.nb);
-    const uint32_t oa = op.off[ra], ob = op.off[rb];  // run-time rows: read from the record, once
+    const uint32_t oa = op.off[ra], ob = op.off[rb];
     for (uint32_t g = threadIdx.x; g < ng; g += blockDim.x) {
         const uint32_t b = ins_group(g, o.low, o.nb) | o.cmask;
-        const C<R> va = s[b + oa], vb = s[b + ob];
+        const C<R> va = s[swz<R>(b + oa)], vb = s[swz<R>(b + ob)];
         CAcc<R> x, y;
         x.add(m[0], va);
         x.add(m[1], vb);
         y.add(m[2], va);
         y.add(m[3], vb);
-        s[b + oa] = x.get();
-        s[b + ob] = y.get();
+        s[swz<R>(b + oa)] = x.get();
+        s[swz<R>(b + ob)] = y.get();
         if (rest) {
 #pragma unroll
             for (int r = 0; r < 16; ++r) {
                 if (r >= D || r == ra || r == rb) continue;
                 CAcc<R> z;
-                z.add(m[4], s[b + o.off[r]]);
-                s[b + o.off[r]] = z.get();
+                z.add(m[4], s[swz<R>(b + o.off[r])]);
+                s[swz<R>(b + o.off[r])] = z.get();
             }
         }
     }
 }
 
-template <typename R>
-__device__ __forceinline__ void f_parity(C<R> *s, const FOp &op, const C<R> *cf, int kt, uint64_t tbase) {
-    const uint32_t n = 1u << kt;
-    const int tp = __popcll(tbase & op.pm_global) & 1;
-    const uint32_t pm = op.pm_local;
-    const C<R> ph0 = cf[tp], ph1 = cf[tp ^ 1];
-    for (uint32_t l = threadIdx.x; l < n; l += blockDim.x) {
-        CAcc<R> a;
-        a.add((__popc(l & pm) & 1) ? ph1 : ph0, s[l]);
-        s[l] = a.get();
+// ---- register forms --------------------------------------------------------------------
+
+// A phase: the threads' register bits and the gates applied in registers.
+struct alignas(16) RPhase {
+    int32_t op_begin, nops;  // register ops (segment-local indices)
+    int32_t fop;             // >= 0: the phase is one shared-memory op (segment-local FOp index)
+    uint32_t comp;           // tile bits taken from the thread index (ascending); the rest are register bits
+    uint32_t rdep[16];       // tile offset of register g (g's bits deposited into the register bits)
+};
+
+// Register op codes: form and, for the forms with targets, the register mask of the targets
+// (index into the list of masks with that many bits).
+enum RCode : int32_t {
+    RC_DIAG = 0,     // phases indexed by up to two tile bits, gated by control bits
+    RC_PARITY = 1,   // phase chosen by the parity of selected bits (MultiRZ)
+    RC_DENSE1 = 16,  // + register bit
+    RC_DENSE2 = 32,  // + index of the two-bit mask
+    RC_DENSE3 = 48,  // + index of the three-bit mask
+    RC_SWAP1 = 64,   // + register bit: exchange of rows 0 and 1, gated by controls
+    RC_SWAP2 = 80,   // + index of the two-bit mask: exchange of |01> and |10>, gated by controls
+    RC_PAIR2 = 96,   // + index of the two-bit mask: 2x2 block on |01>, |10>, gamma on |00>, |11>
+};
+
+struct alignas(16) ROp {
+    int32_t code;
+    int32_t coef;    // first coefficient (segment-local)
+    uint32_t cmask;  // control bits (tile-local)
+    int32_t kd;      // Diag: number of index bits (0..2); Pair: 1 when gamma != 1
+    uint32_t p0, p1; // Diag: tile positions of the index bits (p0 the most significant)
+    uint32_t pm;     // Parity: tile-local bits
+    uint32_t pad;
+    uint64_t pmg;    // Parity: state bits outside the tile
+    uint64_t pad2;
+};
+
+// masks of a-bit registers with two and three bits set, in increasing order
+__host__ __device__ constexpr int mask2(int i) {
+    return i == 0 ? 3 : i == 1 ? 5 : i == 2 ? 6 : i == 3 ? 9 : i == 4 ? 10 : 12;
+}
+__host__ __device__ constexpr int mask3(int i) { return i == 0 ? 7 : i == 1 ? 11 : i == 2 ? 13 : 14; }
+// c's bits deposited into the set bits of mask (ascending)
+__host__ __device__ constexpr int dep_c(int mask, int c) {
+    int r = 0, j = 0;
+    for (int b = 0; b < 8; ++b) {
+        if ((mask >> b) & 1) {
+            if ((c >> j) & 1) r |= 1 << b;
+            ++j;
+        }
+    }
+    return r;
+}
+__host__ __device__ constexpr int popc_c(int m) { return m == 0 ? 0 : (m & 1) + popc_c(m >> 1); }
+__host__ __device__ constexpr int lowbit_c(int m) { return m & -m; }
+
+template <typename R, int A, int MASK>
+__device__ __forceinline__ void r_dense(C<R> (&v)[A], const uint32_t (&l)[A], uint32_t cmask,
+                                        const C<R> *__restrict__ cf) {
+    if constexpr (MASK < A) {
+        constexpr int D = 1 << popc_c(MASK);
+#pragma unroll
+        for (int g = 0; g < A; ++g) {
+            if (g & MASK) continue;
+            if ((l[g] & cmask) != cmask) continue;
+            C<R> x[D];
+#pragma unroll
+            for (int c = 0; c < D; ++c) x[c] = v[g | dep_c(MASK, c)];
+#pragma unroll
+            for (int r = 0; r < D; ++r) {
+                CAcc<R> acc;
+#pragma unroll
+                for (int c = 0; c < D; ++c) acc.add(cf[r * D + c], x[c]);
+                v[g | dep_c(MASK, r)] = acc.get();
+            }
+        }
     }
 }
 
-template <typename R>
-__device__ void apply_fop(C<R> *s, const FOp &op, const C<R> *cf, int kt, uint64_t tbase) {
-    switch (op.kind) {
-    case (int)Kind::Dense:
-        if (op.k == 1) f_dense<R, 1>(s, op, cf, kt);
-        else if (op.k == 2) f_dense<R, 2>(s, op, cf, kt);
-        else f_dense<R, 3>(s, op, cf, kt);
-        break;
-    case (int)Kind::Diag:
-        if (op.k == 0) f_diag<R, 0>(s, op, cf, kt);
-        else if (op.k == 1) f_diag<R, 1>(s, op, cf, kt);
-        else f_diag<R, 2>(s, op, cf, kt);
-        break;
-    case (int)Kind::Swap: f_swap<R>(s, op, kt); break;
-    case (int)Kind::Pair: f_pair<R>(s, op, cf, kt); break;
-    case (int)Kind::Parity: f_parity<R>(s, op, cf, kt, tbase); break;
+template <typename R, int A, int MASK>
+__device__ __forceinline__ void r_swap(C<R> (&v)[A], const uint32_t (&l)[A], uint32_t cmask) {
+    if constexpr (MASK < A) {
+        constexpr int LO = lowbit_c(MASK), HI = MASK ^ LO;  // one bit: rows 0, 1; two bits: |01>, |10>
+#pragma unroll
+        for (int g = 0; g < A; ++g) {
+            if (g & MASK) continue;
+            if ((l[g] & cmask) != cmask) continue;
+            constexpr bool two = HI != 0;
+            const int ia = two ? (g | LO) : g, ib = two ? (g | HI) : (g | LO);
+            const C<R> t = v[ia];
+            v[ia] = v[ib];
+            v[ib] = t;
+        }
+    }
+}
+
+template <typename R, int A, int MASK>
+__device__ __forceinline__ void r_pair(C<R> (&v)[A], const ROp &op, const C<R> *__restrict__ cf) {
+    if constexpr (MASK < A) {
+        constexpr int LO = lowbit_c(MASK), HI = MASK ^ LO;
+        const C<R> m0 = cf[0], m1 = cf[1], m2 = cf[2], m3 = cf[3], gm = cf[4];
+        const bool rest = op.kd != 0;
+#pragma unroll
+        for (int g = 0; g < A; ++g) {
+            if (g & MASK) continue;
+            const C<R> va = v[g | LO], vb = v[g | HI];
+            CAcc<R> x, y;
+            x.add(m0, va);
+            x.add(m1, vb);
+            y.add(m2, va);
+            y.add(m3, vb);
+            v[g | LO] = x.get();
+            v[g | HI] = y.get();
+            if (rest) {
+                CAcc<R> z0, z1;
+                z0.add(gm, v[g]);
+                z1.add(gm, v[g | MASK]);
+                v[g] = z0.get();
+                v[g | MASK] = z1.get();
+            }
+        }
+    }
+}
+
+template <typename R, int A>
+__device__ __forceinline__ void r_diag(C<R> (&v)[A], const uint32_t (&l)[A], const ROp &op,
+                                       const C<R> *__restrict__ cf) {
+    const uint32_t cm = op.cmask, p0 = op.p0, p1 = op.p1;
+    const int kd = op.kd;
+#pragma unroll
+    for (int g = 0; g < A; ++g) {
+        const uint32_t x = l[g];
+        if ((x & cm) != cm) continue;
+        uint32_t idx = 0;
+        if (kd >= 1) idx = (x >> p0) & 1u;
+        if (kd == 2) idx = (idx << 1) | ((x >> p1) & 1u);
+        CAcc<R> acc;
+        acc.add(cf[idx], v[g]);
+        v[g] = acc.get();
+    }
+}
+
+template <typename R, int A>
+__device__ __forceinline__ void r_parity(C<R> (&v)[A], const uint32_t (&l)[A], const ROp &op,
+                                         const C<R> *__restrict__ cf, uint64_t tbase) {
+    const int tp = __popcll(tbase & op.pmg) & 1;
+    const C<R> ph0 = cf[tp], ph1 = cf[tp ^ 1];
+#pragma unroll
+    for (int g = 0; g < A; ++g) {
+        CAcc<R> acc;
+        acc.add((__popc(l[g] & op.pm) & 1) ? ph1 : ph0, v[g]);
+        v[g] = acc.get();
+    }
+}
+
+template <typename R, int A>
+__device__ __forceinline__ void run_rop(C<R> (&v)[A], const uint32_t (&l)[A], const ROp &op,
+                                        const C<R> *__restrict__ scf, uint64_t tbase) {
+    const C<R> *cf = scf + op.coef;
+    switch (op.code) {
+    case RC_DIAG: r_diag<R, A>(v, l, op, cf); break;
+    case RC_PARITY: r_parity<R, A>(v, l, op, cf, tbase); break;
+    case RC_DENSE1 + 0: r_dense<R, A, 1>(v, l, op.cmask, cf); break;
+    case RC_DENSE1 + 1: r_dense<R, A, 2>(v, l, op.cmask, cf); break;
+    case RC_DENSE1 + 2: r_dense<R, A, 4>(v, l, op.cmask, cf); break;
+    case RC_DENSE1 + 3: r_dense<R, A, 8>(v, l, op.cmask, cf); break;
+    case RC_DENSE2 + 0: r_dense<R, A, mask2(0)>(v, l, op.cmask, cf); break;
+    case RC_DENSE2 + 1: r_dense<R, A, mask2(1)>(v, l, op.cmask, cf); break;
+    case RC_DENSE2 + 2: r_dense<R, A, mask2(2)>(v, l, op.cmask, cf); break;
+    case RC_DENSE2 + 3: r_dense<R, A, mask2(3)>(v, l, op.cmask, cf); break;
+    case RC_DENSE2 + 4: r_dense<R, A, mask2(4)>(v, l, op.cmask, cf); break;
+    case RC_DENSE2 + 5: r_dense<R, A, mask2(5)>(v, l, op.cmask, cf); break;
+    case RC_DENSE3 + 0: r_dense<R, A, mask3(0)>(v, l, op.cmask, cf); break;
+    case RC_DENSE3 + 1: r_dense<R, A, mask3(1)>(v, l, op.cmask, cf); break;
+    case RC_DENSE3 + 2: r_dense<R, A, mask3(2)>(v, l, op.cmask, cf); break;
+    case RC_DENSE3 + 3: r_dense<R, A, mask3(3)>(v, l, op.cmask, cf); break;
+    case RC_SWAP1 + 0: r_swap<R, A, 1>(v, l, op.cmask); break;
+    case RC_SWAP1 + 1: r_swap<R, A, 2>(v, l, op.cmask); break;
+    case RC_SWAP1 + 2: r_swap<R, A, 4>(v, l, op.cmask); break;
+    case RC_SWAP1 + 3: r_swap<R, A, 8>(v, l, op.cmask); break;
+    case RC_SWAP2 + 0: r_swap<R, A, mask2(0)>(v, l, op.cmask); break;
+    case RC_SWAP2 + 1: r_swap<R, A, mask2(1)>(v, l, op.cmask); break;
+    case RC_SWAP2 + 2: r_swap<R, A, mask2(2)>(v, l, op.cmask); break;
+    case RC_SWAP2 + 3: r_swap<R, A, mask2(3)>(v, l, op.cmask); break;
+    case RC_SWAP2 + 4: r_swap<R, A, mask2(4)>(v, l, op.cmask); break;
+    case RC_SWAP2 + 5: r_swap<R, A, mask2(5)>(v, l, op.cmask); break;
+    case RC_PAIR2 + 0: r_pair<R, A, mask2(0)>(v, op, cf); break;
+    case RC_PAIR2 + 1: r_pair<R, A, mask2(1)>(v, op, cf); break;
+    case RC_PAIR2 + 2: r_pair<R, A, mask2(2)>(v, op, cf); break;
+    case RC_PAIR2 + 3: r_pair<R, A, mask2(3)>(v, op, cf); break;
+    case RC_PAIR2 + 4: r_pair<R, A, mask2(4)>(v, op, cf); break;
+    case RC_PAIR2 + 5: r_pair<R, A, mask2(5)>(v, op, cf); break;
     default: break;
     }
 }
@@ -209,74 +335,121 @@ __device__ __forceinline__ uint64_t deposit(uint64_t x, const uint8_t *pos, int 
     return r;
 }
 
-// One segment over all tiles.  Shared memory: two tile buffers, the segment's ops and
-// coefficients.  A tile is moved in 16-byte chunks (V amplitudes each, V = 16 / the
-// amplitude size); chunk c of a thread is c = threadIdx.x + j * blockDim.x.
+// x's low bits deposited into the set bits of mask (ascending)
+__device__ __forceinline__ uint32_t pdep32(uint32_t x, uint32_t mask) {
+    uint32_t r = 0;
+    while (mask) {
+        const uint32_t low = mask & (0u - mask);
+        if (x & 1u) r |= low;
+        x >>= 1;
+        mask ^= low;
+    }
+    return r;
+}
+
+struct SegArgs {
+    const RPhase *phases;
+    const ROp *rops;
+    const FOp *fops;
+    const void *coefs;
+    int nph, nrop, nfop, ncoef;
+    int ng;
+    uint8_t lbits[16];  // state position of tile bit i (ascending)
+    uint8_t gbits[48];  // state positions of the bits outside the tile (ascending)
+};
+
+template <typename T> __device__ __forceinline__ void stage(T *dst, const T *src, int n) {
+    static_assert(sizeof(T) % 4 == 0, "staged records are whole words");
+    const uint32_t *s = reinterpret_cast<const uint32_t *>(src);
+    uint32_t *d = reinterpret_cast<uint32_t *>(dst);
+    const int words = n * (int)(sizeof(T) / 4);
+    for (int i = threadIdx.x; i < words; i += blockDim.x) d[i] = s[i];
+}
+
+// One segment over all tiles.  Shared memory: two swizzled tile buffers, then the segment's
+// phases, register ops, shared-memory ops and coefficients.  A tile is moved in 16-byte
+// chunks (V amplitudes each, V = 16 / the amplitude size); chunk c of a thread is
+// c = threadIdx.x + j * blockDim.x, j < A / V.
 template <typename R>
 __global__ void __launch_bounds__(kFThreads, 1) k_fused(C<R> *__restrict__ state, SegArgs a, uint64_t ntiles) {
+    constexpr int KT = Geo<R>::kt, A = Geo<R>::A;
+    constexpr uint32_t TN = 1u << KT;
+    constexpr int V = 16 / (int)sizeof(C<R>);
+    constexpr int PER = (int)(TN / V) / kFThreads;  // 16-byte chunks per thread
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ uint8_t s_lbits[16], s_gbits[48];
-    constexpr int V = 16 / (int)sizeof(C<R>);
-    const uint32_t tn = 1u << a.kt;
     C<R> *const buf0 = reinterpret_cast<C<R> *>(smem_raw);
-    FOp *sops = reinterpret_cast<FOp *>(smem_raw + 2 * sizeof(C<R>) * tn);
-    C<R> *scf = reinterpret_cast<C<R> *>(sops + a.nops);
+    RPhase *sph = reinterpret_cast<RPhase *>(smem_raw + 2 * sizeof(C<R>) * TN);
+    ROp *srop = reinterpret_cast<ROp *>(sph + a.nph);
+    FOp *sfop = reinterpret_cast<FOp *>(srop + a.nrop);
+    C<R> *scf = reinterpret_cast<C<R> *>(sfop + a.nfop);
     if (threadIdx.x == 0) {  // constant indices keep the parameter arrays out of local memory
 #pragma unroll
         for (int i = 0; i < 16; ++i) s_lbits[i] = a.lbits[i];
 #pragma unroll
         for (int i = 0; i < 48; ++i) s_gbits[i] = a.gbits[i];
     }
-    {
-        const uint32_t *src = reinterpret_cast<const uint32_t *>(a.ops);
-        uint32_t *dst = reinterpret_cast<uint32_t *>(sops);
-        const int words = a.nops * (int)(sizeof(FOp) / 4);
-        for (int i = threadIdx.x; i < words; i += blockDim.x) dst[i] = src[i];
-        const C<R> *cs = static_cast<const C<R> *>(a.coefs);
-        for (int i = threadIdx.x; i < a.ncoef; i += blockDim.x) scf[i] = cs[i];
-    }
+    stage(sph, a.phases, a.nph);
+    stage(srop, a.rops, a.nrop);
+    stage(sfop, a.fops, a.nfop);
+    stage(scf, static_cast<const C<R> *>(a.coefs), a.ncoef);
     __syncthreads();
-    // per-thread address parts: chunk c -> local amplitude c * V
-    const int chunks = (int)(tn / V);
-    const int per = chunks / (int)blockDim.x;  // chunks per thread (the host keeps this exact, <= 8)
-    const uint64_t lo = deposit((uint64_t)threadIdx.x * V, s_lbits, a.kt);
-    uint64_t hi[8];
+    // per-thread address parts of the tile moves: chunk c -> tile amplitude c * V
+    const uint64_t lo = deposit((uint64_t)threadIdx.x * V, s_lbits, KT);
+    uint64_t hi[PER];
+    uint32_t sw[PER];  // swizzled shared-memory positions of the chunks
 #pragma unroll
-    for (int j = 0; j < 8; ++j) hi[j] = j < per ? deposit((uint64_t)j * blockDim.x * V, s_lbits, a.kt) : 0;
+    for (int j = 0; j < PER; ++j) {
+        hi[j] = deposit((uint64_t)j * kFThreads * V, s_lbits, KT);
+        sw[j] = swz<R>((threadIdx.x + j * kFThreads) * V);
+    }
 
     uint64_t t = blockIdx.x;
     uint32_t cur = 0;
     if (t < ntiles) {
         const uint64_t tb = deposit(t, s_gbits, a.ng);
 #pragma unroll
-        for (int j = 0; j < 8; ++j)
-            if (j < per) cp_async16(buf0 + (threadIdx.x + j * blockDim.x) * V, state + (tb | lo | hi[j]));
+        for (int j = 0; j < PER; ++j) cp_async16(buf0 + sw[j], state + (tb | lo | hi[j]));
     }
     cp_async_commit();
     for (; t < ntiles; t += gridDim.x) {
         const uint64_t tnext = t + gridDim.x;
         if (tnext < ntiles) {
             const uint64_t tb = deposit(tnext, s_gbits, a.ng);
-            C<R> *dst = buf0 + (cur ^ 1u) * tn;
+            C<R> *dst = buf0 + (cur ^ 1u) * TN;
 #pragma unroll
-            for (int j = 0; j < 8; ++j)
-                if (j < per) cp_async16(dst + (threadIdx.x + j * blockDim.x) * V, state + (tb | lo | hi[j]));
+            for (int j = 0; j < PER; ++j) cp_async16(dst + sw[j], state + (tb | lo | hi[j]));
         }
         cp_async_commit();
         cp_async_wait1();
         __syncthreads();
-        C<R> *s = buf0 + cur * tn;
+        C<R> *s = buf0 + cur * TN;
         const uint64_t tbase = deposit(t, s_gbits, a.ng);
-        for (int o = 0; o < a.nops; ++o) {
-            apply_fop<R>(s, sops[o], scf + sops[o].coef, a.kt, tbase);
+        for (int p = 0; p < a.nph; ++p) {
+            const RPhase &ph = sph[p];
+            if (ph.fop >= 0) {
+                const FOp &f = sfop[ph.fop];
+                f_pair<R>(s, f, scf + f.coef, KT);
+                __syncthreads();
+                continue;
+            }
+            const uint32_t base = pdep32(threadIdx.x, ph.comp);
+            uint32_t l[A];
+            C<R> v[A];
+#pragma unroll
+            for (int g = 0; g < A; ++g) l[g] = base | ph.rdep[g];
+#pragma unroll
+            for (int g = 0; g < A; ++g) v[g] = s[swz<R>(l[g])];
+            const int oe = ph.op_begin + ph.nops;
+            for (int o = ph.op_begin; o < oe; ++o) run_rop<R, A>(v, l, srop[o], scf, tbase);
+#pragma unroll
+            for (int g = 0; g < A; ++g) s[swz<R>(l[g])] = v[g];
             __syncthreads();
         }
 #pragma unroll
-        for (int j = 0; j < 8; ++j) {
-            if (j < per) {
-                const float4 v = *reinterpret_cast<const float4 *>(s + (threadIdx.x + j * blockDim.x) * V);
-                *reinterpret_cast<float4 *>(state + (tbase | lo | hi[j])) = v;
-            }
+        for (int j = 0; j < PER; ++j) {
+            const float4 x = *reinterpret_cast<const float4 *>(s + sw[j]);
+            *reinterpret_cast<float4 *>(state + (tbase | lo | hi[j])) = x;
         }
         __syncthreads();  // the buffer is refilled next iteration
         cur ^= 1u;
@@ -286,13 +459,17 @@ __global__ void __launch_bounds__(kFThreads, 1) k_fused(C<R> *__restrict__ state
 
 template <typename R> C<R> to_r(const cd &z) { return mk<R>((R)z.real(), (R)z.imag()); }
 
-struct Segment {
-    std::vector<uint8_t> lbits, gbits;
-    uint32_t op_begin = 0, nops = 0, coef_begin = 0, ncoef = 0;
-};
+// Bits a descriptor touches (targets, controls, parity bits): gates with disjoint bit sets commute.
+uint64_t dep_bits(const GateDesc &g) {
+    uint64_t b = g.pmask;
+    for (auto x : g.tbits) b |= uint64_t(1) << x;
+    for (auto x : g.cbits) b |= uint64_t(1) << x;
+    return b;
+}
+bool is_diagonal(const GateDesc &g) { return g.kind == Kind::Diag || g.kind == Kind::Parity || g.kind == Kind::Noop; }
 
-// Group bits (targets and controls) of a descriptor the tile kernels cover; false when
-// the descriptor has to run on its own (wide dense matrices and the like).
+// Tile bits (targets and controls) of a descriptor the tile kernel covers; false when the
+// descriptor has to run on its own (wide dense matrices and the like).
 bool tile_bits(const GateDesc &g, uint64_t &bits) {
     bits = 0;
     switch (g.kind) {
@@ -300,7 +477,7 @@ bool tile_bits(const GateDesc &g, uint64_t &bits) {
     case Kind::Parity: return true;
     case Kind::Dense: if (g.k < 1 || g.k > 3) return false; break;
     case Kind::Diag: if (g.k > 2) return false; break;
-    case Kind::Swap: if (g.k > 3) return false; break;
+    case Kind::Swap: if (g.k < 1 || g.k > 2) return false; break;
     case Kind::Pair: if (g.k != 1 && g.k != 2 && g.k != 4) return false; break;
     default: return false;
     }
@@ -320,70 +497,11 @@ int coef_count(const GateDesc &g) {
     }
 }
 
-template <typename R>
-FOp lower_fop(const GateDesc &g, const std::vector<int> &loc, std::vector<C<R>> &coefs) {
-    FOp f{};
-    f.kind = (int)g.kind;
-    f.k = g.k;
-    f.coef = (int32_t)coefs.size();
-    if (g.kind == Kind::Parity) {
-        for (int b = 0; b < 64; ++b) {
-            if (!((g.pmask >> b) & 1)) continue;
-            if (b < (int)loc.size() && loc[b] >= 0) f.pm_local |= 1u << loc[b];
-            else f.pm_global |= uint64_t(1) << b;
-        }
-        coefs.push_back(to_r<R>(g.pphase[0]));
-        coefs.push_back(to_r<R>(g.pphase[1]));
-        return f;
-    }
-    std::vector<uint32_t> grp;
-    for (auto b : g.tbits) grp.push_back((uint32_t)loc[b]);
-    for (auto b : g.cbits) {
-        grp.push_back((uint32_t)loc[b]);
-        f.cmask |= 1u << loc[b];
-    }
-    std::sort(grp.begin(), grp.end());
-    f.nb = (int)grp.size();
-    for (size_t j = 0; j < grp.size(); ++j) f.low[j] = (1u << grp[j]) - 1;
-    const int k = (int)g.tbits.size();
-    for (int r = 0; r < (1 << k); ++r) {
-        uint32_t o = 0;
-        for (int j = 0; j < k; ++j)
-            if (r & (1 << (k - 1 - j))) o |= 1u << loc[g.tbits[j]];
-        f.off[r] = o;
-    }
-    switch (g.kind) {
-    case Kind::Dense:
-    case Kind::Diag:
-        for (auto &z : g.m) coefs.push_back(to_r<R>(z));
-        break;
-    case Kind::Swap:
-        f.ra = (int)g.sa;
-        f.rb = (int)g.sb;
-        break;
-    case Kind::Pair:
-        f.ra = (int)g.pa;
-        f.rb = (int)g.pb;
-        for (auto &z : g.m2) coefs.push_back(to_r<R>(z));
-        coefs.push_back(to_r<R>(g.gamma));
-        f.rest = g.gamma != cd(1.0, 0.0) ? 1 : 0;
-        break;
-    default: break;
-    }
-    return f;
-}
-
-// ---- composing consecutive gates on a few bits ------------------------------------------
-// A step costs one read and one write of the tile in shared memory, which bounds complex128
-// segments; gates whose bits together span at most three tile bits are multiplied into one
-// 8x8 (or smaller) matrix on the host in FP64 and applied as one dense step.  The FP64 work
-// per amplitude grows (8 complex products for three bits) but the FP64 pipe has room.
-// complex64 steps are bound by their compensated sums (twice the FP64 cost per product), so
-// complex64 composes over at most two bits: on 28 qubits a 10-layer RX RY RZ + CNOT circuit
-// takes 204 ms with two bits, 248 with one, 373 with three and 791 without composition.
-// The composed matrix is rounded to complex64 once, from FP64.
-
-constexpr int kComposeBitsC64 = 2;
+// ---- composing consecutive gates ---------------------------------------------------------
+// Consecutive gates on one bit (RZ RY RZ of a Rot, H then RX, ...) are multiplied on the host
+// in FP64 into one 2x2 step, and consecutive diagonal gates on at most two bits into one
+// diagonal step; both need fewer operations than the gates one by one.  Wider products
+// would trade cheap register steps for denser matrices, so they are not formed.
 
 bool fusable(const GateDesc &g) {
     uint64_t b;
@@ -469,21 +587,24 @@ GateDesc compose(const std::vector<const GateDesc *> &gs, uint64_t bits) {
     return out;
 }
 
-// the segment's gates with runs on at most three bits composed
-std::vector<GateDesc> compose_passes(const std::vector<const GateDesc *> &in, int max_bits) {
+std::vector<GateDesc> compose_runs(const std::vector<const GateDesc *> &in) {
     std::vector<GateDesc> out;
     size_t a = 0;
     while (a < in.size()) {
-        uint64_t b0 = 0;
-        if (!fusable(*in[a]) || !tile_bits(*in[a], b0) || __builtin_popcountll(b0) > max_bits) {
+        uint64_t bits = 0, b1 = 0;
+        if (!fusable(*in[a])) {
             out.push_back(*in[a++]);
             continue;
         }
-        uint64_t bits = 0, b1 = 0;
         tile_bits(*in[a], bits);
+        bool alldiag = in[a]->kind == Kind::Diag;
         size_t b = a + 1;
-        while (b < in.size() && fusable(*in[b]) && tile_bits(*in[b], b1) && __builtin_popcountll(bits | b1) <= max_bits) {
-            bits |= b1;
+        while (b < in.size() && fusable(*in[b]) && tile_bits(*in[b], b1)) {
+            const uint64_t nb = bits | b1;
+            const bool nd = alldiag && in[b]->kind == Kind::Diag;
+            if (!(__builtin_popcountll(nb) <= 1 || (nd && __builtin_popcountll(nb) <= 2))) break;
+            bits = nb;
+            alldiag = nd;
             ++b;
         }
         if (b - a == 1) out.push_back(*in[a]);
@@ -493,49 +614,248 @@ std::vector<GateDesc> compose_passes(const std::vector<const GateDesc *> &in, in
     return out;
 }
 
+// ---- lowering a segment into phases ------------------------------------------------------
+
+template <typename R> struct SegCode {
+    std::vector<RPhase> phases;
+    std::vector<ROp> rops;
+    std::vector<FOp> fops;
+    std::vector<C<R>> coefs;
+};
+
+template <typename R>
+FOp lower_fop(const GateDesc &g, const std::vector<int> &loc, std::vector<C<R>> &coefs) {
+    FOp f{};
+    f.kind = (int)g.kind;
+    f.k = g.k;
+    f.coef = (int32_t)coefs.size();
+    std::vector<uint32_t> grp;
+    for (auto b : g.tbits) grp.push_back((uint32_t)loc[b]);
+    for (auto b : g.cbits) {
+        grp.push_back((uint32_t)loc[b]);
+        f.cmask |= 1u << loc[b];
+    }
+    std::sort(grp.begin(), grp.end());
+    f.nb = (int)grp.size();
+    for (size_t j = 0; j < grp.size(); ++j) f.low[j] = (1u << grp[j]) - 1;
+    const int k = (int)g.tbits.size();
+    for (int r = 0; r < (1 << k); ++r) {
+        uint32_t o = 0;
+        for (int j = 0; j < k; ++j)
+            if (r & (1 << (k - 1 - j))) o |= 1u << loc[g.tbits[j]];
+        f.off[r] = o;
+    }
+    f.ra = (int)g.pa;
+    f.rb = (int)g.pb;
+    for (auto &z : g.m2) coefs.push_back(to_r<R>(z));
+    coefs.push_back(to_r<R>(g.gamma));
+    f.rest = g.gamma != cd(1.0, 0.0) ? 1 : 0;
+    return f;
+}
+
+// register targets a descriptor needs in its phase (tile-local mask), or -1 for the
+// shared-memory form, 0 for the forms that work on any register bits
+template <typename R> int64_t reg_targets(const GateDesc &g, const std::vector<int> &loc) {
+    if (g.kind == Kind::Diag || g.kind == Kind::Parity || g.kind == Kind::Noop) return 0;
+    if (g.kind == Kind::Pair && g.k == 4) return -1;
+    uint64_t m = 0;
+    for (auto b : g.tbits) m |= uint64_t(1) << loc[b];
+    return (int64_t)m;
+}
+
+template <typename R>
+void lower_phase(SegCode<R> &sc, uint32_t rmask, const std::vector<const GateDesc *> &ops,
+                 const std::vector<int> &loc) {
+    constexpr int KT = Geo<R>::kt, a = Geo<R>::a, A = Geo<R>::A;
+    // pad the register bits to a bits with the highest free tile bits
+    for (int b = KT - 1; b >= 0 && __builtin_popcount(rmask) < a; --b)
+        if (!((rmask >> b) & 1)) rmask |= 1u << b;
+    int rpos[32];  // tile bit -> register bit
+    int rb[8];
+    {
+        int j = 0;
+        for (int b = 0; b < KT; ++b) {
+            rpos[b] = -1;
+            if ((rmask >> b) & 1) {
+                rpos[b] = j;
+                rb[j++] = b;
+            }
+        }
+    }
+    RPhase ph{};
+    ph.op_begin = (int32_t)sc.rops.size();
+    ph.fop = -1;
+    ph.comp = ((1u << KT) - 1) & ~rmask;
+    for (int g = 0; g < A; ++g) {
+        uint32_t o = 0;
+        for (int j = 0; j < a; ++j)
+            if ((g >> j) & 1) o |= 1u << rb[j];
+        ph.rdep[g] = o;
+    }
+    auto index_of = [](int m, int bits) {
+        for (int i = 0; i < 6; ++i)
+            if ((bits == 2 ? mask2(i) : mask3(i)) == m) return i;
+        return -1;
+    };
+    for (const GateDesc *gp : ops) {
+        const GateDesc &g = *gp;
+        if (g.kind == Kind::Noop) continue;
+        ROp r{};
+        r.coef = (int32_t)sc.coefs.size();
+        for (auto b : g.cbits) r.cmask |= 1u << loc[b];
+        if (g.kind == Kind::Diag) {
+            r.code = RC_DIAG;
+            r.kd = g.k;
+            if (g.k >= 1) r.p0 = (uint32_t)loc[g.tbits[0]];
+            if (g.k >= 2) r.p1 = (uint32_t)loc[g.tbits[1]];
+            for (auto &z : g.m) sc.coefs.push_back(to_r<R>(z));
+            sc.rops.push_back(r);
+            continue;
+        }
+        if (g.kind == Kind::Parity) {
+            r.code = RC_PARITY;
+            for (int b = 0; b < 64; ++b) {
+                if (!((g.pmask >> b) & 1)) continue;
+                if (loc[b] >= 0) r.pm |= 1u << loc[b];
+                else r.pmg |= uint64_t(1) << b;
+            }
+            sc.coefs.push_back(to_r<R>(g.pphase[0]));
+            sc.coefs.push_back(to_r<R>(g.pphase[1]));
+            sc.rops.push_back(r);
+            continue;
+        }
+        // register bit of each target, and the target mask over the register bits
+        const int k = (int)g.tbits.size();
+        std::vector<int> regb(k);
+        int mask = 0;
+        for (int j = 0; j < k; ++j) {
+            regb[j] = rpos[loc[g.tbits[j]]];
+            mask |= 1 << regb[j];
+        }
+        if (g.kind == Kind::Swap) {
+            r.code = k == 1 ? RC_SWAP1 + regb[0] : RC_SWAP2 + index_of(mask, 2);
+            sc.rops.push_back(r);
+            continue;
+        }
+        if (g.kind == Kind::Pair && k == 2) {
+            // rows pa = 1 (tbits[0] clear, tbits[1] set) and pb = 2; canonical rows: the lower
+            // register bit first
+            r.code = RC_PAIR2 + index_of(mask, 2);
+            r.kd = g.gamma != cd(1.0, 0.0) ? 1 : 0;
+            const bool pa_low = regb[1] < regb[0];
+            const cd m00 = g.m2[0], m01 = g.m2[1], m10 = g.m2[2], m11 = g.m2[3];
+            const cd blk[4] = {pa_low ? m00 : m11, pa_low ? m01 : m10, pa_low ? m10 : m01, pa_low ? m11 : m00};
+            for (auto &z : blk) sc.coefs.push_back(to_r<R>(z));
+            sc.coefs.push_back(to_r<R>(g.gamma));
+            sc.rops.push_back(r);
+            continue;
+        }
+        // Dense (and the one-bit Pair form): canonical matrix, index bit i <-> i-th lowest mask bit
+        std::vector<cd> m;
+        if (g.kind == Kind::Pair) m = {g.m2[0], g.m2[1], g.m2[2], g.m2[3]};
+        else m = g.m;
+        const int D = 1 << k;
+        std::vector<int> rank(k);  // position of regb[j] among the mask's set bits
+        for (int j = 0; j < k; ++j) rank[j] = __builtin_popcount(mask & ((1 << regb[j]) - 1));
+        auto orig = [&](int c) {
+            int o = 0;
+            for (int j = 0; j < k; ++j)
+                if ((c >> rank[j]) & 1) o |= 1 << (k - 1 - j);
+            return o;
+        };
+        for (int rr = 0; rr < D; ++rr)
+            for (int cc = 0; cc < D; ++cc) sc.coefs.push_back(to_r<R>(m[orig(rr) * D + orig(cc)]));
+        r.code = k == 1 ? RC_DENSE1 + regb[0] : k == 2 ? RC_DENSE2 + index_of(mask, 2) : RC_DENSE3 + index_of(mask, 3);
+        sc.rops.push_back(r);
+    }
+    ph.nops = (int32_t)sc.rops.size() - ph.op_begin;
+    sc.phases.push_back(ph);
+}
+
+// Phases of one segment: a greedy walk that keeps a gate in the current phase while the
+// union of the phase's target bits fits the register bits.
+template <typename R>
+void lower_segment(SegCode<R> &sc, const std::vector<GateDesc> &ops, const std::vector<int> &loc) {
+    constexpr int a = Geo<R>::a;
+    std::vector<const GateDesc *> cur;
+    uint32_t rmask = 0;
+    auto close = [&]() {
+        if (!cur.empty()) lower_phase<R>(sc, rmask, cur, loc);
+        cur.clear();
+        rmask = 0;
+    };
+    for (const GateDesc &g : ops) {
+        const int64_t t = reg_targets<R>(g, loc);
+        if (t < 0) {  // shared-memory form: its own phase
+            close();
+            RPhase ph{};
+            ph.fop = (int32_t)sc.fops.size();
+            sc.fops.push_back(lower_fop<R>(g, loc, sc.coefs));
+            sc.phases.push_back(ph);
+            continue;
+        }
+        const uint32_t need = (uint32_t)t;
+        if (__builtin_popcount(rmask | need) > a) close();
+        rmask |= need;
+        cur.push_back(&g);
+    }
+    close();
+}
+
+struct Segment {
+    std::vector<uint8_t> lbits, gbits;
+    uint32_t ph_begin = 0, nph = 0, rop_begin = 0, nrop = 0, fop_begin = 0, nfop = 0, coef_begin = 0, ncoef = 0;
+};
+
 template <typename R>
 void run_fused(void *state, uint32_t nq, const std::vector<GateDesc> &descs,
                const std::function<void(const GateDesc &)> &apply_single, cudaStream_t st) {
-    const int kt = fused_tile_bits(sizeof(R) == 4 ? B200SV_C64 : B200SV_C128, nq);
-    const int V = 16 / (int)sizeof(C<R>);
-    // the lowest bits stay in every tile: 2^reserve contiguous amplitudes = 128 bytes
-    const int reserve = sizeof(R) == 4 ? 4 : 3;
-    const uint64_t low = (uint64_t(1) << reserve) - 1;
+    constexpr int kt = Geo<R>::kt;
+    if ((int)nq < kt) throw Unsupported("state narrower than the fused tile");
+    const uint64_t low = (uint64_t(1) << Geo<R>::reserve) - 1;  // 128 contiguous bytes in every tile
     struct Piece {
         bool seg;
         Segment s;
         size_t desc;
     };
     std::vector<Piece> pieces;
-    std::vector<FOp> ops;
-    std::vector<C<R>> coefs;
-    size_t i = 0;
+    SegCode<R> sc;
     const size_t nd = descs.size();
-    while (i < nd) {
+    std::vector<char> done(nd, 0);
+    size_t first = 0;
+    while (true) {
+        while (first < nd && (done[first] || descs[first].kind == Kind::Noop)) ++first;
+        if (first >= nd) break;
         uint64_t b = 0;
-        if (descs[i].kind == Kind::Noop) { ++i; continue; }
-        if (!tile_bits(descs[i], b)) {
-            pieces.push_back(Piece{false, {}, i});
-            ++i;
+        if (!tile_bits(descs[first], b)) {
+            pieces.push_back(Piece{false, {}, first});
+            done[first] = 1;
             continue;
         }
-        uint64_t used = 0;
-        size_t j = i;
+        // look-ahead: take every later gate that fits and commutes with the gates left out
+        uint64_t used = 0, blocked_any = 0, blocked_nondiag = 0;
         int nops = 0, ncf = 0;
-        while (j < nd) {
-            if (descs[j].kind == Kind::Noop) { ++j; continue; }
-            if (!tile_bits(descs[j], b)) break;
-            if (__builtin_popcountll(used | b | low) > kt) break;
-            if (nops + 1 > kMaxSegOps || ncf + coef_count(descs[j]) > kMaxSegCoefs) break;
-            used |= b;
-            ++nops;
-            ncf += coef_count(descs[j]);
-            ++j;
-        }
-        if (j == i) {  // cannot happen for the forms above (a gate uses at most 8 tile bits); kept as a guard
-            pieces.push_back(Piece{false, {}, i});
-            ++i;
-            continue;
+        std::vector<size_t> take;
+        for (size_t j = first; j < nd; ++j) {
+            if (done[j] || descs[j].kind == Kind::Noop) continue;
+            const GateDesc &g = descs[j];
+            const uint64_t db = dep_bits(g);
+            const bool diagonal = is_diagonal(g);
+            const bool blocked = (db & blocked_nondiag) || (!diagonal && (db & blocked_any));
+            bool fits = false;
+            if (!blocked && tile_bits(g, b) && __builtin_popcountll(used | b | low) <= kt &&
+                nops + 1 <= kMaxSegOps && ncf + coef_count(g) <= kMaxSegCoefs)
+                fits = true;
+            if (fits) {
+                used |= b;
+                ++nops;
+                ncf += coef_count(g);
+                take.push_back(j);
+            } else {
+                blocked_any |= db;
+                if (!diagonal) blocked_nondiag |= db;
+                if (__builtin_popcountll(blocked_any) >= (int)nq && blocked_nondiag == blocked_any) break;
+            }
         }
         Segment sg;
         std::vector<int> loc(nq, -1);
@@ -549,53 +869,62 @@ void run_fused(void *state, uint32_t nq, const std::vector<GateDesc> &descs,
                 sg.gbits.push_back((uint8_t)x);
             }
         }
-        sg.op_begin = (uint32_t)ops.size();
-        sg.coef_begin = (uint32_t)coefs.size();
-        std::vector<C<R>> local;
         std::vector<const GateDesc *> seg;
-        for (size_t q = i; q < j; ++q)
-            if (descs[q].kind != Kind::Noop) seg.push_back(&descs[q]);
-        bool composed = false;
-        {
-            const std::vector<GateDesc> fused = compose_passes(seg, sizeof(R) == 8 ? 3 : kComposeBitsC64);
-            size_t nc = 0;
-            for (auto &g : fused) nc += coef_count(g);
-            if (fused.size() < seg.size() && nc <= (size_t)kMaxSegCoefs) {
-                for (auto &g : fused) ops.push_back(lower_fop<R>(g, loc, local));
-                composed = true;
-            }
+        for (size_t j : take) {
+            seg.push_back(&descs[j]);
+            done[j] = 1;
         }
-        if (!composed)
-            for (const GateDesc *g : seg) ops.push_back(lower_fop<R>(*g, loc, local));
-        sg.nops = (uint32_t)(ops.size() - sg.op_begin);
-        sg.ncoef = (uint32_t)local.size();
-        coefs.insert(coefs.end(), local.begin(), local.end());
+        const std::vector<GateDesc> fused = compose_runs(seg);
+        sg.ph_begin = (uint32_t)sc.phases.size();
+        sg.rop_begin = (uint32_t)sc.rops.size();
+        sg.fop_begin = (uint32_t)sc.fops.size();
+        sg.coef_begin = (uint32_t)sc.coefs.size();
+        SegCode<R> local;
+        lower_segment<R>(local, fused, loc);
+        sc.phases.insert(sc.phases.end(), local.phases.begin(), local.phases.end());
+        sc.rops.insert(sc.rops.end(), local.rops.begin(), local.rops.end());
+        sc.fops.insert(sc.fops.end(), local.fops.begin(), local.fops.end());
+        sc.coefs.insert(sc.coefs.end(), local.coefs.begin(), local.coefs.end());
+        sg.nph = (uint32_t)local.phases.size();
+        sg.nrop = (uint32_t)local.rops.size();
+        sg.nfop = (uint32_t)local.fops.size();
+        sg.ncoef = (uint32_t)local.coefs.size();
         pieces.push_back(Piece{true, sg, 0});
-        i = j;
     }
-    if (ops.empty()) {
+    if (sc.phases.empty()) {
         for (auto &p : pieces) apply_single(descs[p.desc]);
         return;
     }
-    if ((uint32_t(1) << kt) / V % kFThreads != 0 || (uint32_t(1) << kt) / V / kFThreads > 8)
-        throw Unsupported("fused tile size does not match the thread count");
-    FOp *d_ops = nullptr;
-    C<R> *d_cf = nullptr;
-    B200SV_CUDA(cudaMallocAsync((void **)&d_ops, ops.size() * sizeof(FOp), st));
-    B200SV_CUDA(cudaMallocAsync((void **)&d_cf, std::max<size_t>(1, coefs.size()) * sizeof(C<R>), st));
+    // one device copy of every segment's records
+    const size_t bph = sc.phases.size() * sizeof(RPhase), brop = sc.rops.size() * sizeof(ROp),
+                 bfop = sc.fops.size() * sizeof(FOp), bcf = sc.coefs.size() * sizeof(C<R>);
+    std::vector<unsigned char> blob(bph + brop + bfop + bcf + 16);
+    std::memcpy(blob.data(), sc.phases.data(), bph);
+    if (brop) std::memcpy(blob.data() + bph, sc.rops.data(), brop);
+    if (bfop) std::memcpy(blob.data() + bph + brop, sc.fops.data(), bfop);
+    if (bcf) std::memcpy(blob.data() + bph + brop + bfop, sc.coefs.data(), bcf);
+    unsigned char *d_blob = nullptr;
+    B200SV_CUDA(cudaMallocAsync((void **)&d_blob, blob.size(), st));
     struct Free {
-        void *a, *b;
+        void *p;
         cudaStream_t s;
-        ~Free() {
-            cudaFreeAsync(a, s);
-            cudaFreeAsync(b, s);
-        }
-    } fr{d_ops, d_cf, st};
-    B200SV_CUDA(cudaMemcpyAsync(d_ops, ops.data(), ops.size() * sizeof(FOp), cudaMemcpyHostToDevice, st));
-    if (!coefs.empty())
-        B200SV_CUDA(cudaMemcpyAsync(d_cf, coefs.data(), coefs.size() * sizeof(C<R>), cudaMemcpyHostToDevice, st));
+        ~Free() { cudaFreeAsync(p, s); }
+    } fr{d_blob, st};
+    B200SV_CUDA(cudaMemcpyAsync(d_blob, blob.data(), blob.size(), cudaMemcpyHostToDevice, st));
+    const RPhase *d_ph = reinterpret_cast<const RPhase *>(d_blob);
+    const ROp *d_rop = reinterpret_cast<const ROp *>(d_blob + bph);
+    const FOp *d_fop = reinterpret_cast<const FOp *>(d_blob + bph + brop);
+    const C<R> *d_cf = reinterpret_cast<const C<R> *>(d_blob + bph + brop + bfop);
     const size_t tile_bytes = sizeof(C<R>) << kt;
-    const size_t smem_max = 2 * tile_bytes + kMaxSegOps * sizeof(FOp) + kMaxSegCoefs * sizeof(C<R>);
+    auto seg_smem = [&](const Segment &s) {
+        return 2 * tile_bytes + s.nph * sizeof(RPhase) + s.nrop * sizeof(ROp) + s.nfop * sizeof(FOp) +
+               s.ncoef * sizeof(C<R>);
+    };
+    size_t smem_max = 0;
+    for (const Piece &p : pieces)
+        if (p.seg) smem_max = std::max(smem_max, seg_smem(p.s));
+    // at most 96 ops per segment: 128 KiB of tiles + 96 x (80 + 48 + 160) B + 32 KiB of coefficients
+    if (smem_max > 227 * 1024) throw Unsupported("fused segment records exceed shared memory");
     B200SV_CUDA(cudaFuncSetAttribute(k_fused<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_max));
     const uint64_t ntiles = uint64_t(1) << (nq - kt);
     const unsigned grid = (unsigned)std::min<uint64_t>(ntiles, (uint64_t)sm_count());
@@ -605,16 +934,18 @@ void run_fused(void *state, uint32_t nq, const std::vector<GateDesc> &descs,
             continue;
         }
         SegArgs a{};
-        a.ops = d_ops + p.s.op_begin;
+        a.phases = d_ph + p.s.ph_begin;
+        a.rops = d_rop + p.s.rop_begin;
+        a.fops = d_fop + p.s.fop_begin;
         a.coefs = d_cf + p.s.coef_begin;
-        a.nops = (int)p.s.nops;
+        a.nph = (int)p.s.nph;
+        a.nrop = (int)p.s.nrop;
+        a.nfop = (int)p.s.nfop;
         a.ncoef = (int)p.s.ncoef;
-        a.kt = kt;
         a.ng = (int)p.s.gbits.size();
         std::memcpy(a.lbits, p.s.lbits.data(), p.s.lbits.size());
         std::memcpy(a.gbits, p.s.gbits.data(), p.s.gbits.size());
-        const size_t smem = 2 * tile_bytes + p.s.nops * sizeof(FOp) + p.s.ncoef * sizeof(C<R>);
-        k_fused<R><<<grid, kFThreads, smem, st>>>(static_cast<C<R> *>(state), a, ntiles);
+        k_fused<R><<<grid, kFThreads, seg_smem(p.s), st>>>(static_cast<C<R> *>(state), a, ntiles);
         B200SV_CUDA(cudaGetLastError());
     }
 }
@@ -622,15 +953,12 @@ void run_fused(void *state, uint32_t nq, const std::vector<GateDesc> &descs,
 }  // namespace
 
 int fused_tile_bits(int dtype, uint32_t nq) {
-    const int kt = dtype == B200SV_C64 ? 13 : 12;
+    const int kt = dtype == B200SV_C64 ? Geo<float>::kt : Geo<double>::kt;
     return (int)std::min<uint32_t>(kt, nq);
 }
 
 // Below 21 qubits (2^8 / 2^9 tiles) a segment has too few tiles to fill 148 SMs and one
-// launch per gate is faster: on a 200-gate random sweep at 20 qubits complex128, 1.5 ms per
-// gate launch against 3.9 ms fused; from 21 qubits on (L2-resident or not) the fused path
-// wins on deep circuits (a 10-layer RX RY RZ + CNOT circuit: 4.2 vs 7.8 ms at 21 qubits,
-// 89 vs 334 ms at 26).
+// launch per gate is faster.
 bool fused_worthwhile(int dtype, uint32_t nq) {
     return nq >= (uint32_t)fused_tile_bits(dtype, nq) + (dtype == B200SV_C64 ? 8 : 9);
 }
