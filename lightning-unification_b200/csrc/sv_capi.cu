@@ -908,20 +908,19 @@ int b200sv_var_sparse(b200sv_handle h, const uint64_t *row_map, uint64_t row_map
 static void sample_impl(b200sv_state *h, uint64_t nshots, const double *uniforms, uint64_t seed, uint64_t *idx_host) {
     const cudaStream_t st = h->stream();
     const uint64_t N = uint64_t(1) << h->nq;
-    const size_t ws = cdf_workspace_doubles(N);
-    double *cdf = nullptr, *work = nullptr, *u = nullptr;
+    const size_t ws = run_offsets_doubles(N);
+    double *work = nullptr, *u = nullptr;
     uint64_t *idx = nullptr;
-    B200SV_CUDA(cudaMallocAsync((void **)&cdf, N * sizeof(double), st));
     B200SV_CUDA(cudaMallocAsync((void **)&work, ws * sizeof(double), st));
     B200SV_CUDA(cudaMallocAsync((void **)&u, std::max<uint64_t>(1, nshots) * sizeof(double), st));
     B200SV_CUDA(cudaMallocAsync((void **)&idx, std::max<uint64_t>(1, nshots) * sizeof(uint64_t), st));
-    if (h->dtype == B200SV_C64) build_cdf<float>(h->d_state, h->nq, cdf, work, st);
-    else build_cdf<double>(h->d_state, h->nq, cdf, work, st);
+    if (h->dtype == B200SV_C64) build_run_offsets<float>(h->d_state, h->nq, work, st);
+    else build_run_offsets<double>(h->d_state, h->nq, work, st);
     if (uniforms) B200SV_CUDA(cudaMemcpyAsync(u, uniforms, nshots * sizeof(double), cudaMemcpyHostToDevice, st));
     else philox_uniforms(u, nshots, seed, st);
-    sample_from_cdf(cdf, N, u, nshots, idx, st);
+    if (h->dtype == B200SV_C64) sample_runs<float>(h->d_state, h->nq, work, u, nshots, idx, st);
+    else sample_runs<double>(h->d_state, h->nq, work, u, nshots, idx, st);
     if (nshots) B200SV_CUDA(cudaMemcpyAsync(idx_host, idx, nshots * sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
-    cudaFreeAsync(cdf, st);
     cudaFreeAsync(work, st);
     cudaFreeAsync(u, st);
     cudaFreeAsync(idx, st);

@@ -38,7 +38,7 @@ namespace {
 
 constexpr int kFThreads = 512;
 constexpr int kMaxGroupBits = 8;
-constexpr int kMaxSegOps = 96;
+constexpr int kMaxSegOps = 192;
 constexpr int kMaxSegCoefs = 2048;
 
 // Tile geometry: 2^kt amplitudes (64 KiB) per tile, A = 2^kt / 512 amplitudes per thread.
@@ -143,16 +143,19 @@ struct alignas(16) RPhase {
     int32_t fop;             // >= 0: the phase is one shared-memory op (segment-local FOp index)
     uint32_t comp;           // tile bits taken from the thread index (ascending); the rest are register bits
     uint32_t rdep[16];       // tile offset of register g (g's bits deposited into the register bits)
+    uint32_t srdep[16];      // swz(rdep[g]): the swizzle is linear over XOR, so a register's shared-memory
+                             // position is swz(thread part) ^ srdep[g]
 };
 
 // Register op codes: form and, for the forms with targets, the register mask of the targets
 // (index into the list of masks with that many bits).
 enum RCode : int32_t {
-    RC_DIAG = 0,     // phases indexed by up to two tile bits, gated by control bits
+    RC_DIAG = 0,     // phases indexed by up to three tile bits (controls folded into the table)
     RC_PARITY = 1,   // phase chosen by the parity of selected bits (MultiRZ)
     RC_DENSE1 = 16,  // + register bit
     RC_DENSE2 = 32,  // + index of the two-bit mask
     RC_DENSE3 = 48,  // + index of the three-bit mask
+    RC_CTL = 128,    // added to a dense code: the gate has control bits
     RC_SWAP1 = 64,   // + register bit: exchange of rows 0 and 1, gated by controls
     RC_SWAP2 = 80,   // + index of the two-bit mask: exchange of |01> and |10>, gated by controls
     RC_PAIR2 = 96,   // + index of the two-bit mask: 2x2 block on |01>, |10>, gamma on |00>, |11>
@@ -162,10 +165,9 @@ struct alignas(16) ROp {
     int32_t code;
     int32_t coef;    // first coefficient (segment-local)
     uint32_t cmask;  // control bits (tile-local)
-    int32_t kd;      // Diag: number of index bits (0..2); Pair: 1 when gamma != 1
-    uint32_t p0, p1; // Diag: tile positions of the index bits (p0 the most significant)
+    int32_t kd;      // Diag: number of index bits (0..3); Pair: 1 when gamma != 1
+    uint32_t p0, p1, p2; // Diag: tile positions of the index bits (p0 the most significant)
     uint32_t pm;     // Parity: tile-local bits
-    uint32_t pad;
     uint64_t pmg;    // Parity: state bits outside the tile
     uint64_t pad2;
 };
@@ -189,7 +191,19 @@ __host__ __device__ constexpr int dep_c(int mask, int c) {
 __host__ __device__ constexpr int popc_c(int m) { return m == 0 ? 0 : (m & 1) + popc_c(m >> 1); }
 __host__ __device__ constexpr int lowbit_c(int m) { return m & -m; }
 
-template <typename R, int A, int MASK>
+// One complex product m * v, the value a one-term compensated sum (CAcc) returns: complex64
+// forms each component with one FMA (cmul2), so the compensation word would stay zero.
+template <typename R> __device__ __forceinline__ C<R> cprod(C<R> m, C<R> v) {
+    if constexpr (sizeof(R) == 4) {
+        return cmul2(m, v);
+    } else {
+        CAcc<R> acc;
+        acc.add(m, v);
+        return acc.get();
+    }
+}
+
+template <typename R, int A, int MASK, bool CTL>
 __device__ __forceinline__ void r_dense(C<R> (&v)[A], const uint32_t (&l)[A], uint32_t cmask,
                                         const C<R> *__restrict__ cf) {
     if constexpr (MASK < A) {
@@ -197,7 +211,7 @@ __device__ __forceinline__ void r_dense(C<R> (&v)[A], const uint32_t (&l)[A], ui
 #pragma unroll
         for (int g = 0; g < A; ++g) {
             if (g & MASK) continue;
-            if ((l[g] & cmask) != cmask) continue;
+            if (CTL && (l[g] & cmask) != cmask) continue;
             C<R> x[D];
 #pragma unroll
             for (int c = 0; c < D; ++c) x[c] = v[g | dep_c(MASK, c)];
@@ -219,12 +233,12 @@ __device__ __forceinline__ void r_swap(C<R> (&v)[A], const uint32_t (&l)[A], uin
 #pragma unroll
         for (int g = 0; g < A; ++g) {
             if (g & MASK) continue;
-            if ((l[g] & cmask) != cmask) continue;
+            const bool on = (l[g] & cmask) == cmask;
             constexpr bool two = HI != 0;
             const int ia = two ? (g | LO) : g, ib = two ? (g | HI) : (g | LO);
-            const C<R> t = v[ia];
-            v[ia] = v[ib];
-            v[ib] = t;
+            const C<R> x = v[ia], y = v[ib];
+            v[ia] = on ? y : x;
+            v[ib] = on ? x : y;
         }
     }
 }
@@ -247,31 +261,23 @@ __device__ __forceinline__ void r_pair(C<R> (&v)[A], const ROp &op, const C<R> *
             v[g | LO] = x.get();
             v[g | HI] = y.get();
             if (rest) {
-                CAcc<R> z0, z1;
-                z0.add(gm, v[g]);
-                z1.add(gm, v[g | MASK]);
-                v[g] = z0.get();
-                v[g | MASK] = z1.get();
+                v[g] = cprod<R>(gm, v[g]);
+                v[g | MASK] = cprod<R>(gm, v[g | MASK]);
             }
         }
     }
 }
 
+// phases indexed by up to three tile bits; bits beyond kd read a position-31 bit (always 0)
 template <typename R, int A>
 __device__ __forceinline__ void r_diag(C<R> (&v)[A], const uint32_t (&l)[A], const ROp &op,
                                        const C<R> *__restrict__ cf) {
-    const uint32_t cm = op.cmask, p0 = op.p0, p1 = op.p1;
-    const int kd = op.kd;
+    const uint32_t p0 = op.p0, p1 = op.p1, p2 = op.p2;
 #pragma unroll
     for (int g = 0; g < A; ++g) {
         const uint32_t x = l[g];
-        if ((x & cm) != cm) continue;
-        uint32_t idx = 0;
-        if (kd >= 1) idx = (x >> p0) & 1u;
-        if (kd == 2) idx = (idx << 1) | ((x >> p1) & 1u);
-        CAcc<R> acc;
-        acc.add(cf[idx], v[g]);
-        v[g] = acc.get();
+        const uint32_t idx = (((x >> p0) & 1u) << 2) | (((x >> p1) & 1u) << 1) | ((x >> p2) & 1u);
+        v[g] = cprod<R>(cf[idx], v[g]);
     }
 }
 
@@ -281,11 +287,7 @@ __device__ __forceinline__ void r_parity(C<R> (&v)[A], const uint32_t (&l)[A], c
     const int tp = __popcll(tbase & op.pmg) & 1;
     const C<R> ph0 = cf[tp], ph1 = cf[tp ^ 1];
 #pragma unroll
-    for (int g = 0; g < A; ++g) {
-        CAcc<R> acc;
-        acc.add((__popc(l[g] & op.pm) & 1) ? ph1 : ph0, v[g]);
-        v[g] = acc.get();
-    }
+    for (int g = 0; g < A; ++g) v[g] = cprod<R>((__popc(l[g] & op.pm) & 1) ? ph1 : ph0, v[g]);
 }
 
 template <typename R, int A>
@@ -295,20 +297,34 @@ __device__ __forceinline__ void run_rop(C<R> (&v)[A], const uint32_t (&l)[A], co
     switch (op.code) {
     case RC_DIAG: r_diag<R, A>(v, l, op, cf); break;
     case RC_PARITY: r_parity<R, A>(v, l, op, cf, tbase); break;
-    case RC_DENSE1 + 0: r_dense<R, A, 1>(v, l, op.cmask, cf); break;
-    case RC_DENSE1 + 1: r_dense<R, A, 2>(v, l, op.cmask, cf); break;
-    case RC_DENSE1 + 2: r_dense<R, A, 4>(v, l, op.cmask, cf); break;
-    case RC_DENSE1 + 3: r_dense<R, A, 8>(v, l, op.cmask, cf); break;
-    case RC_DENSE2 + 0: r_dense<R, A, mask2(0)>(v, l, op.cmask, cf); break;
-    case RC_DENSE2 + 1: r_dense<R, A, mask2(1)>(v, l, op.cmask, cf); break;
-    case RC_DENSE2 + 2: r_dense<R, A, mask2(2)>(v, l, op.cmask, cf); break;
-    case RC_DENSE2 + 3: r_dense<R, A, mask2(3)>(v, l, op.cmask, cf); break;
-    case RC_DENSE2 + 4: r_dense<R, A, mask2(4)>(v, l, op.cmask, cf); break;
-    case RC_DENSE2 + 5: r_dense<R, A, mask2(5)>(v, l, op.cmask, cf); break;
-    case RC_DENSE3 + 0: r_dense<R, A, mask3(0)>(v, l, op.cmask, cf); break;
-    case RC_DENSE3 + 1: r_dense<R, A, mask3(1)>(v, l, op.cmask, cf); break;
-    case RC_DENSE3 + 2: r_dense<R, A, mask3(2)>(v, l, op.cmask, cf); break;
-    case RC_DENSE3 + 3: r_dense<R, A, mask3(3)>(v, l, op.cmask, cf); break;
+    case RC_DENSE1 + 0: r_dense<R, A, 1, false>(v, l, op.cmask, cf); break;
+    case RC_CTL + RC_DENSE1 + 0: r_dense<R, A, 1, true>(v, l, op.cmask, cf); break;
+    case RC_DENSE1 + 1: r_dense<R, A, 2, false>(v, l, op.cmask, cf); break;
+    case RC_CTL + RC_DENSE1 + 1: r_dense<R, A, 2, true>(v, l, op.cmask, cf); break;
+    case RC_DENSE1 + 2: r_dense<R, A, 4, false>(v, l, op.cmask, cf); break;
+    case RC_CTL + RC_DENSE1 + 2: r_dense<R, A, 4, true>(v, l, op.cmask, cf); break;
+    case RC_DENSE1 + 3: r_dense<R, A, 8, false>(v, l, op.cmask, cf); break;
+    case RC_CTL + RC_DENSE1 + 3: r_dense<R, A, 8, true>(v, l, op.cmask, cf); break;
+    case RC_DENSE2 + 0: r_dense<R, A, mask2(0), false>(v, l, op.cmask, cf); break;
+    case RC_CTL + RC_DENSE2 + 0: r_dense<R, A, mask2(0), true>(v, l, op.cmask, cf); break;
+    case RC_DENSE2 + 1: r_dense<R, A, mask2(1), false>(v, l, op.cmask, cf); break;
+    case RC_CTL + RC_DENSE2 + 1: r_dense<R, A, mask2(1), true>(v, l, op.cmask, cf); break;
+    case RC_DENSE2 + 2: r_dense<R, A, mask2(2), false>(v, l, op.cmask, cf); break;
+    case RC_CTL + RC_DENSE2 + 2: r_dense<R, A, mask2(2), true>(v, l, op.cmask, cf); break;
+    case RC_DENSE2 + 3: r_dense<R, A, mask2(3), false>(v, l, op.cmask, cf); break;
+    case RC_CTL + RC_DENSE2 + 3: r_dense<R, A, mask2(3), true>(v, l, op.cmask, cf); break;
+    case RC_DENSE2 + 4: r_dense<R, A, mask2(4), false>(v, l, op.cmask, cf); break;
+    case RC_CTL + RC_DENSE2 + 4: r_dense<R, A, mask2(4), true>(v, l, op.cmask, cf); break;
+    case RC_DENSE2 + 5: r_dense<R, A, mask2(5), false>(v, l, op.cmask, cf); break;
+    case RC_CTL + RC_DENSE2 + 5: r_dense<R, A, mask2(5), true>(v, l, op.cmask, cf); break;
+    case RC_DENSE3 + 0: r_dense<R, A, mask3(0), false>(v, l, op.cmask, cf); break;
+    case RC_CTL + RC_DENSE3 + 0: r_dense<R, A, mask3(0), true>(v, l, op.cmask, cf); break;
+    case RC_DENSE3 + 1: r_dense<R, A, mask3(1), false>(v, l, op.cmask, cf); break;
+    case RC_CTL + RC_DENSE3 + 1: r_dense<R, A, mask3(1), true>(v, l, op.cmask, cf); break;
+    case RC_DENSE3 + 2: r_dense<R, A, mask3(2), false>(v, l, op.cmask, cf); break;
+    case RC_CTL + RC_DENSE3 + 2: r_dense<R, A, mask3(2), true>(v, l, op.cmask, cf); break;
+    case RC_DENSE3 + 3: r_dense<R, A, mask3(3), false>(v, l, op.cmask, cf); break;
+    case RC_CTL + RC_DENSE3 + 3: r_dense<R, A, mask3(3), true>(v, l, op.cmask, cf); break;
     case RC_SWAP1 + 0: r_swap<R, A, 1>(v, l, op.cmask); break;
     case RC_SWAP1 + 1: r_swap<R, A, 2>(v, l, op.cmask); break;
     case RC_SWAP1 + 2: r_swap<R, A, 4>(v, l, op.cmask); break;
@@ -434,16 +450,17 @@ __global__ void __launch_bounds__(kFThreads, 1) k_fused(C<R> *__restrict__ state
                 continue;
             }
             const uint32_t base = pdep32(threadIdx.x, ph.comp);
+            const uint32_t sbase = swz<R>(base);
             uint32_t l[A];
             C<R> v[A];
 #pragma unroll
             for (int g = 0; g < A; ++g) l[g] = base | ph.rdep[g];
 #pragma unroll
-            for (int g = 0; g < A; ++g) v[g] = s[swz<R>(l[g])];
+            for (int g = 0; g < A; ++g) v[g] = s[sbase ^ ph.srdep[g]];
             const int oe = ph.op_begin + ph.nops;
             for (int o = ph.op_begin; o < oe; ++o) run_rop<R, A>(v, l, srop[o], scf, tbase);
 #pragma unroll
-            for (int g = 0; g < A; ++g) s[swz<R>(l[g])] = v[g];
+            for (int g = 0; g < A; ++g) s[sbase ^ ph.srdep[g]] = v[g];
             __syncthreads();
         }
 #pragma unroll
@@ -490,7 +507,7 @@ bool tile_bits(const GateDesc &g, uint64_t &bits) {
 int coef_count(const GateDesc &g) {
     switch (g.kind) {
     case Kind::Dense: return 1 << (2 * g.k);
-    case Kind::Diag: return 1 << g.k;
+    case Kind::Diag: return 8;  // a table over up to three bits (targets and controls)
     case Kind::Pair: return 5;
     case Kind::Parity: return 2;
     default: return 0;
@@ -691,6 +708,7 @@ void lower_phase(SegCode<R> &sc, uint32_t rmask, const std::vector<const GateDes
         for (int j = 0; j < a; ++j)
             if ((g >> j) & 1) o |= 1u << rb[j];
         ph.rdep[g] = o;
+        ph.srdep[g] = swz<R>(o);
     }
     auto index_of = [](int m, int bits) {
         for (int i = 0; i < 6; ++i)
@@ -704,11 +722,30 @@ void lower_phase(SegCode<R> &sc, uint32_t rmask, const std::vector<const GateDes
         r.coef = (int32_t)sc.coefs.size();
         for (auto b : g.cbits) r.cmask |= 1u << loc[b];
         if (g.kind == Kind::Diag) {
+            // one table over the target bits then the control bits: entry 1 where a control is clear
             r.code = RC_DIAG;
-            r.kd = g.k;
-            if (g.k >= 1) r.p0 = (uint32_t)loc[g.tbits[0]];
-            if (g.k >= 2) r.p1 = (uint32_t)loc[g.tbits[1]];
-            for (auto &z : g.m) sc.coefs.push_back(to_r<R>(z));
+            r.cmask = 0;
+            std::vector<uint32_t> ib(g.tbits.begin(), g.tbits.end());
+            ib.insert(ib.end(), g.cbits.begin(), g.cbits.end());
+            if (ib.size() > 3) throw Unsupported("fused diagonal step over more than three bits");
+            r.kd = (int32_t)ib.size();
+            uint32_t pos[3] = {31, 31, 31};
+            for (size_t j = 0; j < ib.size(); ++j) pos[j] = (uint32_t)loc[ib[j]];
+            r.p0 = pos[0];
+            r.p1 = pos[1];
+            r.p2 = pos[2];
+            const int kt_ = g.k, kc = (int)g.cbits.size();
+            for (int idx = 0; idx < 8; ++idx) {
+                // idx bit (2 - j) holds index bit j; absent bits are zero in every address
+                int t = 0;
+                bool all_c = true;
+                for (int j = 0; j < kt_ + kc; ++j) {
+                    const int bit = (idx >> (2 - j)) & 1;
+                    if (j < kt_) t = (t << 1) | bit;
+                    else if (!bit) all_c = false;
+                }
+                sc.coefs.push_back(to_r<R>(all_c ? g.m[t] : cd(1.0, 0.0)));
+            }
             sc.rops.push_back(r);
             continue;
         }
@@ -766,40 +803,70 @@ void lower_phase(SegCode<R> &sc, uint32_t rmask, const std::vector<const GateDes
         for (int rr = 0; rr < D; ++rr)
             for (int cc = 0; cc < D; ++cc) sc.coefs.push_back(to_r<R>(m[orig(rr) * D + orig(cc)]));
         r.code = k == 1 ? RC_DENSE1 + regb[0] : k == 2 ? RC_DENSE2 + index_of(mask, 2) : RC_DENSE3 + index_of(mask, 3);
+        if (r.cmask) r.code += RC_CTL;
         sc.rops.push_back(r);
     }
     ph.nops = (int32_t)sc.rops.size() - ph.op_begin;
     sc.phases.push_back(ph);
 }
 
-// Phases of one segment: a greedy walk that keeps a gate in the current phase while the
-// union of the phase's target bits fits the register bits.
+// Phases of one segment.  Gates commute when their bit sets are disjoint or both are
+// diagonal, so a phase takes every gate that is ready (no earlier gate left behind shares a
+// bit with it, unless both are diagonal) and whose targets still fit the register bits,
+// scanning the segment in order until nothing more fits; the next phase starts from the
+// earliest gate left.  A gate of the shared-memory form runs as a phase of its own once it
+// is ready and no register gate can move.
 template <typename R>
 void lower_segment(SegCode<R> &sc, const std::vector<GateDesc> &ops, const std::vector<int> &loc) {
     constexpr int a = Geo<R>::a;
-    std::vector<const GateDesc *> cur;
-    uint32_t rmask = 0;
-    auto close = [&]() {
-        if (!cur.empty()) lower_phase<R>(sc, rmask, cur, loc);
-        cur.clear();
-        rmask = 0;
+    const size_t n = ops.size();
+    std::vector<int64_t> tgt(n);
+    std::vector<uint64_t> bits(n);
+    std::vector<char> diag(n), done(n, 0);
+    for (size_t i = 0; i < n; ++i) {
+        tgt[i] = reg_targets<R>(ops[i], loc);
+        bits[i] = dep_bits(ops[i]);
+        diag[i] = is_diagonal(ops[i]);
+        if (ops[i].kind == Kind::Noop) done[i] = 1;
+    }
+    auto ready = [&](size_t i) {
+        for (size_t j = 0; j < i; ++j)
+            if (!done[j] && (bits[j] & bits[i]) && !(diag[j] && diag[i])) return false;
+        return true;
     };
-    for (const GateDesc &g : ops) {
-        const int64_t t = reg_targets<R>(g, loc);
-        if (t < 0) {  // shared-memory form: its own phase
-            close();
-            RPhase ph{};
-            ph.fop = (int32_t)sc.fops.size();
-            sc.fops.push_back(lower_fop<R>(g, loc, sc.coefs));
-            sc.phases.push_back(ph);
+    size_t left = 0;
+    for (size_t i = 0; i < n; ++i) left += done[i] ? 0 : 1;
+    while (left > 0) {
+        std::vector<const GateDesc *> cur;
+        uint32_t rmask = 0;
+        for (bool progress = true; progress;) {
+            progress = false;
+            for (size_t i = 0; i < n; ++i) {
+                if (done[i] || tgt[i] < 0 || !ready(i)) continue;
+                const uint32_t need = (uint32_t)tgt[i];
+                if (__builtin_popcount(rmask | need) > a) continue;
+                rmask |= need;
+                cur.push_back(&ops[i]);
+                done[i] = 1;
+                --left;
+                progress = true;
+            }
+        }
+        if (!cur.empty()) {
+            lower_phase<R>(sc, rmask, cur, loc);
             continue;
         }
-        const uint32_t need = (uint32_t)t;
-        if (__builtin_popcount(rmask | need) > a) close();
-        rmask |= need;
-        cur.push_back(&g);
+        // no register gate can move: the earliest ready shared-memory gate goes next
+        size_t i = 0;
+        while (i < n && (done[i] || tgt[i] >= 0 || !ready(i))) ++i;
+        if (i == n) throw Unsupported("fused phase planning made no progress");
+        RPhase ph{};
+        ph.fop = (int32_t)sc.fops.size();
+        sc.fops.push_back(lower_fop<R>(ops[i], loc, sc.coefs));
+        sc.phases.push_back(ph);
+        done[i] = 1;
+        --left;
     }
-    close();
 }
 
 struct Segment {
@@ -923,7 +990,8 @@ void run_fused(void *state, uint32_t nq, const std::vector<GateDesc> &descs,
     size_t smem_max = 0;
     for (const Piece &p : pieces)
         if (p.seg) smem_max = std::max(smem_max, seg_smem(p.s));
-    // at most 96 ops per segment: 128 KiB of tiles + 96 x (80 + 48 + 160) B + 32 KiB of coefficients
+    // at most 192 ops per segment: 128 KiB of tiles + 192 x (144 + 48) B + 32 KiB of coefficients
+    // (+ 160 B per double excitation)
     if (smem_max > 227 * 1024) throw Unsupported("fused segment records exceed shared memory");
     B200SV_CUDA(cudaFuncSetAttribute(k_fused<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_max));
     const uint64_t ntiles = uint64_t(1) << (nq - kt);
@@ -957,10 +1025,11 @@ int fused_tile_bits(int dtype, uint32_t nq) {
     return (int)std::min<uint32_t>(kt, nq);
 }
 
-// Below 21 qubits (2^8 / 2^9 tiles) a segment has too few tiles to fill 148 SMs and one
-// launch per gate is faster.
+// From one tile up: a narrow state leaves SMs idle during a segment, but one launch per
+// segment instead of one per gate is still the shorter path for L2-resident states, where
+// per-gate launches are bound by launch latency.
 bool fused_worthwhile(int dtype, uint32_t nq) {
-    return nq >= (uint32_t)fused_tile_bits(dtype, nq) + (dtype == B200SV_C64 ? 8 : 9);
+    return nq >= (uint32_t)(dtype == B200SV_C64 ? Geo<float>::kt : Geo<double>::kt);
 }
 
 void apply_fused(void *state, uint32_t nq, int dtype, const std::vector<GateDesc> &descs,

@@ -131,12 +131,14 @@ void axpy_pauli(void *acc, const void *psi, uint32_t nq, const PauliWord &w, dou
 template <typename R> void axpy(void *acc, const void *x, uint32_t nq, double c, cudaStream_t st);
 
 // ---- sampling (sv_sample.cu) ---------------------------------------------
-// Number of doubles of workspace needed besides the N-double CDF.
-size_t cdf_workspace_doubles(uint64_t N);
-template <typename R>
-void build_cdf(const void *psi, uint32_t nq, double *cdf, double *work, cudaStream_t st);
+// Doubles of workspace for the run offsets of the fixed-order CDF (about N / 31).
+size_t run_offsets_doubles(uint64_t N);
+// O_1 (the CDF at every 32nd index) into the start of work
+template <typename R> void build_run_offsets(const void *psi, uint32_t nq, double *work, cudaStream_t st);
 void philox_uniforms(double *u, uint64_t n, uint64_t seed, cudaStream_t st);
-void sample_from_cdf(const double *cdf, uint64_t N, const double *u, uint64_t nshots, uint64_t *idx,
-                     cudaStream_t st);
+// inverse-CDF indices for nshots uniforms, CDF entries formed from O_1 and the state
+template <typename R>
+void sample_runs(const void *psi, uint32_t nq, const double *o1, const double *u, uint64_t nshots, uint64_t *idx,
+                 cudaStream_t st);
 
 }  // namespace b200sv

@@ -12,7 +12,16 @@
 //           prefix inside each run; x_{l+1}[g] = sequential sum of run g;
 //   levels stop when one run covers the level; O_top = E_top;
 //   O_l[j] = O_{l+1}[j / 32] + E_l[j]  (top down);  cdf = O_0.
-// Every kernel stages runs through shared memory so global accesses coalesce.
+//
+// Only the run offsets O_1 (N / 32 doubles) are stored.  The search forms
+// cdf[j] = O_1[j / 32] + (sequential sum of p over the first j mod 32 entries of
+// run j / 32) when it needs it, with the same additions in the same order as the
+// full CDF, so every compared value is bit-identical to it.  Searches that start
+// at (1, N] probe indices of the form k * 2^m + 1 while the range is wide, so most
+// probes add one probability; the state is read in place and no N-entry array is
+// allocated (a 33-qubit complex64 state needs 2 GiB of offsets instead of a 64 GiB CDF).
+// Each thread searches four shots in lock step, so four independent memory reads
+// are in flight per thread.
 #include <vector>
 
 #include "sv_device.cuh"
@@ -84,36 +93,6 @@ __global__ void k_add_offsets(const double *__restrict__ parent, double *__restr
         e[j] = __dadd_rn(parent[j / kRun], e[j]);
 }
 
-// cdf[i] = O_1[i / 32] + (sequential exclusive prefix of p inside run i / 32)
-template <typename R>
-__global__ void __launch_bounds__(kST) k_cdf_final(const C<R> *__restrict__ a, uint64_t n,
-                                                   const double *__restrict__ o1, double *__restrict__ cdf) {
-    __shared__ double s[kST * kPad];
-    const uint64_t e0 = (uint64_t)blockIdx.x * kST * kRun;
-    for (int e = threadIdx.x; e < kST * kRun; e += kST) {
-        const uint64_t i = e0 + e;
-        s[(e / kRun) * kPad + (e % kRun)] = i < n ? prob_of<R>(a[i]) : 0.0;
-    }
-    __syncthreads();
-    const uint64_t g = (uint64_t)blockIdx.x * kST + threadIdx.x;
-    const uint64_t nruns = (n + kRun - 1) / kRun;
-    if (g < nruns) {
-        const int cnt = (int)min((uint64_t)kRun, n - g * kRun);
-        const double off = o1[g];
-        double acc = 0.0;
-        for (int j = 0; j < cnt; ++j) {
-            const double v = s[threadIdx.x * kPad + j];
-            s[threadIdx.x * kPad + j] = __dadd_rn(off, acc);
-            acc = __dadd_rn(acc, v);
-        }
-    }
-    __syncthreads();
-    for (int e = threadIdx.x; e < kST * kRun; e += kST) {
-        const uint64_t i = e0 + e;
-        if (i < n) cdf[i] = s[(e / kRun) * kPad + (e % kRun)];
-    }
-}
-
 // Philox4x32-10 (Salmon, Moraes, Dror, Shaw, "Parallel random numbers: as easy
 // as 1, 2, 3", SC 2011): counter = (i_lo, i_hi, 0, 0), key = (seed_lo, seed_hi);
 // u = ((out1 << 32 | out0) >> 11) * 2^-53 in [0, 1).
@@ -139,24 +118,58 @@ __global__ void k_philox(double *__restrict__ u, uint64_t n, uint64_t seed) {
         u[i] = philox_u01(i, seed);
 }
 
-__global__ void k_sample(const double *__restrict__ cdf, uint64_t N, const double *__restrict__ u, uint64_t nshots,
-                         uint64_t *__restrict__ idx) {
-    for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < nshots; k += (uint64_t)gridDim.x * blockDim.x) {
-        const double U = u[k];
-        uint64_t index;
-        if (U <= cdf[1]) {
-            index = 0;
-        } else {
-            uint64_t lo = 1, hi = N;
-            while (hi - lo > 1) {
-                const uint64_t mid = hi - ((hi - lo) >> 1);
-                const double c = (mid == N) ? 1.0 : cdf[mid];
-                if (c < U) lo = mid;
-                else hi = mid;
-            }
-            index = hi - 1;
+// cdf[j] of the rule (j < N): O_1[j / 32] plus the sequential sum of the run's first j mod 32
+// probabilities, added in the order of the full CDF
+template <typename R>
+__device__ __forceinline__ double cdf_at(const C<R> *__restrict__ a, const double *__restrict__ o1, uint64_t j) {
+    const uint64_t g = j >> 5;
+    const int r = (int)(j & 31u);
+    const double off = o1[g];
+    double acc = 0.0;
+    const C<R> *run = a + (g << 5);
+    for (int i = 0; i < r; ++i) acc = __dadd_rn(acc, prob_of<R>(run[i]));
+    return __dadd_rn(off, acc);
+}
+
+constexpr int kShotsPerThread = 4;
+
+template <typename R>
+__global__ void k_sample_runs(const C<R> *__restrict__ a, const double *__restrict__ o1, uint64_t N,
+                              const double *__restrict__ u, uint64_t nshots, uint64_t *__restrict__ idx) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x * kShotsPerThread;
+    for (uint64_t k0 = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) * kShotsPerThread; k0 < nshots;
+         k0 += stride) {
+        double U[kShotsPerThread];
+        uint64_t lo[kShotsPerThread], hi[kShotsPerThread];
+        bool act[kShotsPerThread];
+        const double c1 = N > 1 ? cdf_at<R>(a, o1, 1) : 1.0;
+#pragma unroll
+        for (int s = 0; s < kShotsPerThread; ++s) {
+            const bool in = k0 + s < nshots;
+            U[s] = in ? u[k0 + s] : 0.0;
+            lo[s] = 1;
+            hi[s] = N;
+            // index 0 when U <= cdf[1]; the search runs for the others
+            act[s] = in && !(U[s] <= c1);
+            if (!act[s]) hi[s] = 1;
         }
-        idx[k] = index;
+        for (;;) {
+            bool any = false;
+#pragma unroll
+            for (int s = 0; s < kShotsPerThread; ++s) {
+                if (act[s] && hi[s] - lo[s] > 1) {
+                    any = true;
+                    const uint64_t mid = hi[s] - ((hi[s] - lo[s]) >> 1);
+                    const double c = (mid == N) ? 1.0 : cdf_at<R>(a, o1, mid);
+                    if (c < U[s]) lo[s] = mid;
+                    else hi[s] = mid;
+                }
+            }
+            if (!any) break;
+        }
+#pragma unroll
+        for (int s = 0; s < kShotsPerThread; ++s)
+            if (k0 + s < nshots) idx[k0 + s] = hi[s] - 1;
     }
 }
 
@@ -174,7 +187,7 @@ dim3 ew(uint64_t n) {
 
 }  // namespace
 
-size_t cdf_workspace_doubles(uint64_t N) {
+size_t run_offsets_doubles(uint64_t N) {
     auto L = level_lengths(N);
     size_t s = 1;
     for (size_t l = 1; l < L.size(); ++l) s += L[l];
@@ -182,16 +195,13 @@ size_t cdf_workspace_doubles(uint64_t N) {
 }
 
 template <typename R>
-void build_cdf(const void *psi, uint32_t nq, double *cdf, double *work, cudaStream_t st) {
+void build_run_offsets(const void *psi, uint32_t nq, double *work, cudaStream_t st) {
     const uint64_t n = uint64_t(1) << nq;
     const C<R> *a = static_cast<const C<R> *>(psi);
     const auto L = level_lengths(n);
     const uint64_t per_block = (uint64_t)kST * kRun;
-    if (L.size() == 1) {
-        // one run: O_1 = [0]
+    if (L.size() == 1) {  // one run: O_1 = [0]
         B200SV_CUDA(cudaMemsetAsync(work, 0, sizeof(double), st));
-        k_cdf_final<R><<<1, kST, 0, st>>>(a, n, work, cdf);
-        B200SV_CUDA(cudaGetLastError());
         return;
     }
     // x_l for l >= 1 live consecutively in work: x_1 at work + 0, x_2 after it, ...
@@ -213,8 +223,6 @@ void build_cdf(const void *psi, uint32_t nq, double *cdf, double *work, cudaStre
         k_add_offsets<<<ew(L[l]), 256, 0, st>>>(x[l + 1], x[l], L[l]);
         B200SV_CUDA(cudaGetLastError());
     }
-    k_cdf_final<R><<<(unsigned)((n + per_block - 1) / per_block), kST, 0, st>>>(a, n, x[1], cdf);
-    B200SV_CUDA(cudaGetLastError());
 }
 
 void philox_uniforms(double *u, uint64_t n, uint64_t seed, cudaStream_t st) {
@@ -222,14 +230,20 @@ void philox_uniforms(double *u, uint64_t n, uint64_t seed, cudaStream_t st) {
     B200SV_CUDA(cudaGetLastError());
 }
 
-void sample_from_cdf(const double *cdf, uint64_t N, const double *u, uint64_t nshots, uint64_t *idx,
-                     cudaStream_t st) {
+template <typename R>
+void sample_runs(const void *psi, uint32_t nq, const double *o1, const double *u, uint64_t nshots, uint64_t *idx,
+                 cudaStream_t st) {
     if (nshots == 0) return;
-    k_sample<<<ew(nshots), 256, 0, st>>>(cdf, N, u, nshots, idx);
+    k_sample_runs<R><<<ew((nshots + kShotsPerThread - 1) / kShotsPerThread), 256, 0, st>>>(
+        static_cast<const C<R> *>(psi), o1, uint64_t(1) << nq, u, nshots, idx);
     B200SV_CUDA(cudaGetLastError());
 }
 
-template void build_cdf<float>(const void *, uint32_t, double *, double *, cudaStream_t);
-template void build_cdf<double>(const void *, uint32_t, double *, double *, cudaStream_t);
+template void build_run_offsets<float>(const void *, uint32_t, double *, cudaStream_t);
+template void build_run_offsets<double>(const void *, uint32_t, double *, cudaStream_t);
+template void sample_runs<float>(const void *, uint32_t, const double *, const double *, uint64_t, uint64_t *,
+                                 cudaStream_t);
+template void sample_runs<double>(const void *, uint32_t, const double *, const double *, uint64_t, uint64_t *,
+                                  cudaStream_t);
 
 }  // namespace b200sv

@@ -184,7 +184,7 @@ def test_apply_ops_sequence_and_errors(capi):
 
 
 @pytest.mark.parametrize("dtype", [np.complex128, np.complex64])
-@pytest.mark.parametrize("n", [20, 22])
+@pytest.mark.parametrize("n", [13, 15, 20, 22])
 def test_fused_apply_matches_oracle(capi, n, dtype):
     """b200sv_apply_ops_fused (segments of gates applied per shared-memory tile) on the gate-sweep
     family plus gates the tile forms do not cover (three-wire matrices, four-wire excitations,
@@ -197,7 +197,7 @@ def test_fused_apply_matches_oracle(capi, n, dtype):
              ("MultiRZ", list(range(0, n, 2)), False, [0.9]), ("QubitUnitary", [1, 7, n - 2], False, [],
                                                                   random_unitary(rng, 3)),
              ("CRot", [n - 1, 2], True, [0.2, 0.3, 0.4]), ("IsingXY", [4, n - 3], False, [1.1]),
-             ("PhaseShift", [n - 1], False, [0.5]), ("S", [0], True, []), ("CSWAP", [2, 9, 14], False, [])]
+             ("PhaseShift", [n - 1], False, [0.5]), ("S", [0], True, []), ("CSWAP", [2, 9, min(14, n - 1)], False, [])]
     for k, op in enumerate(extra):
         ops.insert(10 * k + 5, op)
     st = rs(n, seed=n, dtype=dtype)
