@@ -35,7 +35,7 @@ enum Form : uint8_t { F_MAT1 = 1, F_MAT2 = 2, F_DIAG = 3, F_SWAP = 4, F_PARITY =
 enum GForm : uint8_t { G_NONE = 0, G_MAT = 1, G_PARITY = 2 };
 constexpr uint8_t kConstGate = 255;
 constexpr int kMaxKt = 14;
-constexpr int kMaxObsPerCircuit = 16;
+constexpr int kObsPerPass = 16;  // observables whose expectation values one forward pass accumulates
 
 // One gate with bit positions local to its segment's tile.
 struct DOp {
@@ -125,8 +125,8 @@ __device__ __forceinline__ void apply_pair_k(const C<R> (&m)[4], C<R> &v0, C<R> 
         v1 = mk<R>(dot2r<R>(-m[2].y, a.y, m[3].x, b.x), dot2r<R>(m[2].y, a.x, m[3].x, b.y));
     } else {
         CAcc<R> p, q;
-        p.add(m[0], v0); p.add(m[1], v1);
-        q.add(m[2], v0); q.add(m[3], v1);
+        p.set(m[0], v0); p.add(m[1], v1);
+        q.set(m[2], v0); q.add(m[3], v1);
         v0 = p.get();
         v1 = q.get();
     }
@@ -303,7 +303,7 @@ __device__ __forceinline__ void apply_mat2(C<R> *const (&s)[NS], int kt, int wl,
             for (int r = 0; r < 4; ++r) {
                 CAcc<R> a;
 #pragma unroll
-                for (int c = 0; c < 4; ++c) a.add(m[r * 4 + c], v[c]);
+                for (int c = 0; c < 4; ++c) cacc_term<R>(a, c, m[r * 4 + c], v[c]);
                 t[base + op.off[r]] = a.get();
             }
         }
@@ -322,7 +322,7 @@ __device__ __forceinline__ void apply_op(C<R> *const (&s)[NS], int kt, int wl, b
 #pragma unroll
             for (int q = 0; q < NS; ++q) {
                 CAcc<R> a;
-                a.add(f, s[q][i]);
+                a.set(f, s[q][i]);
                 s[q][i] = a.get();
             }
         }
@@ -355,8 +355,8 @@ __device__ __forceinline__ void apply_op(C<R> *const (&s)[NS], int kt, int wl, b
             case F_MAT1: {
                 const C<R> v0 = t[base + op.off[0]], v1 = t[base + op.off[1]];
                 CAcc<R> a, b;
-                a.add(m[0], v0); a.add(m[1], v1);
-                b.add(m[2], v0); b.add(m[3], v1);
+                a.set(m[0], v0); a.add(m[1], v1);
+                b.set(m[2], v0); b.add(m[3], v1);
                 t[base + op.off[0]] = a.get();
                 t[base + op.off[1]] = b.get();
                 break;
@@ -367,7 +367,7 @@ __device__ __forceinline__ void apply_op(C<R> *const (&s)[NS], int kt, int wl, b
                 for (int r = 0; r < 4; ++r) {
                     if (r < rows) {
                         CAcc<R> a;
-                        a.add(m[r], t[base + op.off[r]]);
+                        a.set(m[r], t[base + op.off[r]]);
                         t[base + op.off[r]] = a.get();
                     }
                 }
@@ -402,7 +402,7 @@ __device__ __forceinline__ void apply_op_general(C<R> *const (&s)[NS], int kt, i
 #pragma unroll
             for (int q = 0; q < NS; ++q) {
                 CAcc<R> a;
-                a.add(f, s[q][i]);
+                a.set(f, s[q][i]);
                 s[q][i] = a.get();
             }
         }
@@ -643,8 +643,8 @@ __device__ void exec_run(C<R> *const (&s)[NS], int kt, int wl, bool wloc, const 
             for (int q = 0; q < NS; ++q) {
                 const C<R> a0 = s[q][i0], a1 = s[q][i1];
                 CAcc<R> p, r;
-                p.add(m[0], a0); p.add(m[1], a1);
-                r.add(m[2], a0); r.add(m[3], a1);
+                p.set(m[0], a0); p.add(m[1], a1);
+                r.set(m[2], a0); r.add(m[3], a1);
                 s[q][i0] = p.get();
                 s[q][i1] = r.get();
             }
@@ -801,9 +801,12 @@ __device__ __forceinline__ uint64_t insert_zeros64(uint64_t v, const uint8_t *bi
 // sum_t coeff_t <psi|P_t|psi> per observable into acc[obs] (per-thread part)
 template <typename R>
 __device__ void expval_terms(const C<R> *psi, uint64_t n_amp, const DTerm *__restrict__ terms, uint32_t nterms,
-                             double (&acc)[kMaxObsPerCircuit]) {
+                             uint32_t obs0, double (&acc)[kObsPerPass]) {
+    // observables obs0 .. obs0 + kObsPerPass - 1 of the circuit (accumulator o <-> obs0 + o)
     for (uint32_t t = 0; t < nterms; ++t) {
-        const DTerm tm = terms[t];
+        DTerm tm = terms[t];
+        if (tm.obs < obs0 || tm.obs >= obs0 + kObsPerPass) continue;
+        tm.obs -= obs0;
         double a = 0.0;
         if (tm.xmask == 0) {  // diagonal word (ny is 0): sum of +-|psi_i|^2, one read per amplitude
             for (uint64_t i = threadIdx.x; i < n_amp; i += blockDim.x) {
@@ -812,7 +815,7 @@ __device__ void expval_terms(const C<R> *psi, uint64_t n_amp, const DTerm *__res
                 a += (__popcll(i & tm.zmask) & 1) ? -p : p;
             }
 #pragma unroll
-            for (int o = 0; o < kMaxObsPerCircuit; ++o)
+            for (int o = 0; o < kObsPerPass; ++o)
                 if (o == (int)tm.obs) acc[o] += tm.coeff * a;
             continue;
         }
@@ -830,7 +833,7 @@ __device__ void expval_terms(const C<R> *psi, uint64_t n_amp, const DTerm *__res
             a += (__popcll(i & tm.zmask) & 1) ? -r : r;
         }
 #pragma unroll
-        for (int o = 0; o < kMaxObsPerCircuit; ++o)  // constant indices keep acc in registers
+        for (int o = 0; o < kObsPerPass; ++o)  // constant indices keep acc in registers
             if (o == (int)tm.obs) acc[o] += tm.coeff * a;
     }
 }
@@ -1114,7 +1117,7 @@ template <typename R, int MODE, bool FULL>
 __global__ void __launch_bounds__(512) k_batch(KArgs A) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ uint32_t s_next;
-    __shared__ double s_red[kMaxObsPerCircuit * 32];
+    __shared__ double s_red[kObsPerPass * 32];
     __shared__ __align__(8) DSeg s_seg;
     __shared__ __align__(8) DOp s_ops[kMaxSegOpsStaged];
     __shared__ __align__(16) C<R> s_cf[kMaxSegOpsStaged][4];
@@ -1134,18 +1137,21 @@ __global__ void __launch_bounds__(512) k_batch(KArgs A) {
         if (!reuse) run_forward<R, FULL>(A, c, sm0, pa, &s_seg, s_ops, s_cf);
         const C<R> *psi = c.resident ? sm0 : pa;
         if (MODE == 0) {
-            double acc[kMaxObsPerCircuit];
+            const DTerm *T = stage_terms(reinterpret_cast<DTerm *>(s_ops), A, c, nullptr);
+            // observables in groups of kObsPerPass, one group of accumulators at a time
+            for (uint32_t obs0 = 0; obs0 < c.nobs; obs0 += kObsPerPass) {
+                double acc[kObsPerPass];
 #pragma unroll
-            for (int o = 0; o < kMaxObsPerCircuit; ++o) acc[o] = 0.0;
-            expval_terms<R>(psi, namp, stage_terms(reinterpret_cast<DTerm *>(s_ops), A, c, nullptr), c.nterms,
-                            acc);
-            block_reduce<kMaxObsPerCircuit>(acc, s_red);
-            if (threadIdx.x == 0) {
+                for (int o = 0; o < kObsPerPass; ++o) acc[o] = 0.0;
+                expval_terms<R>(psi, namp, T, c.nterms, obs0, acc);
+                block_reduce<kObsPerPass>(acc, s_red);
+                if (threadIdx.x == 0) {
 #pragma unroll
-                for (int o = 0; o < kMaxObsPerCircuit; ++o)
-                    if (o < (int)c.nobs) A.out[c.out_begin + o] = acc[o];
+                    for (int o = 0; o < kObsPerPass; ++o)
+                        if (obs0 + o < c.nobs) A.out[c.out_begin + obs0 + o] = acc[o];
+                }
+                __syncthreads();
             }
-            __syncthreads();
             continue;
         }
         // ---- VJP: bra = sum_o dy_o O_o psi, then the reverse sweep ----
@@ -1835,7 +1841,7 @@ void build_program(Batch &B, const Config &cfg) {
     int dev = 0, maxsm = 0, nsm = sm_count();
     B200SV_CUDA(cudaGetDevice(&dev));
     B200SV_CUDA(cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-    const size_t static_smem = kMaxObsPerCircuit * 32 * 8 + 2 * 16 * 16 + 64 + sizeof(DSeg) +
+    const size_t static_smem = kObsPerPass * 32 * 8 + 2 * 16 * 16 + 64 + sizeof(DSeg) +
                                kMaxSegOpsStaged * (sizeof(DOp) + 4 * B.amp());
     if (B.smem_bytes + static_smem > (size_t)maxsm)
         throw Unsupported("batch: tile does not fit in shared memory; lower kt");
@@ -1981,7 +1987,6 @@ int b200sv_batch_create(int dtype, const b200sv_batch_circuit *circuits, uint32_
             const b200sv_batch_circuit &bc = circuits[c];
             if (bc.num_qubits < 1 || bc.num_qubits > 30) throw ArgError("batch circuits have 1..30 qubits");
             if (bc.nops && !bc.ops) throw ArgError("NULL ops");
-            if (bc.nobs > (uint32_t)kMaxObsPerCircuit) throw Unsupported("batch: at most 16 observables per circuit");
             B->nq.push_back(bc.num_qubits);
             std::vector<HostOp> hv;
             for (uint32_t i = 0; i < bc.nops; ++i) {

@@ -102,9 +102,10 @@ void *scratch(b200sv_state *h, int i) {
 }
 
 void apply_desc(b200sv_state *h, void *const *states, int nstates, const GateDesc &g) {
-    if (g.kind == Kind::Dense && g.k >= 4) {
-        const size_t need_b = h->amp_bytes() * g.m.size();
-        ensure_matrix(h, need_b);
+    if (g.kind == Kind::Dense && g.k >= 3) {
+        size_t need_b = g.k >= 4 ? h->amp_bytes() * g.m.size() : 0;
+        if (h->dtype == B200SV_C64 && dense_tc_applies(h->nq, g)) need_b = std::max(need_b, dense_tc_scratch_bytes(g.k));
+        if (need_b) ensure_matrix(h, need_b);
     }
     if (h->dtype == B200SV_C64) launch_gate<float>(states, nstates, h->nq, g, h->d_matrix, h->stream());
     else launch_gate<double>(states, nstates, h->nq, g, h->d_matrix, h->stream());
@@ -536,6 +537,8 @@ int b200sv_synchronize(b200sv_handle h) {
         check_handle(h);
         DeviceGuard dg(h->device);
         B200SV_CUDA(cudaStreamSynchronize(h->stream()));
+        if (dense_tc_timeouts() != 0)
+            throw CudaError("a tensor-core matrix launch gave up waiting for its MMAs (results are invalid)");
     });
 }
 int b200sv_device_ptr(b200sv_handle h, void **out) {

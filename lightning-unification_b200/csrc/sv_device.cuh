@@ -63,6 +63,12 @@ template <> struct CAcc<double> {
         im = fma(m.y, v.x, im);
     }
     __device__ __forceinline__ double2 get() const { return make_double2(re, im); }
+    // the first term of a sum: the same value as add() on an empty accumulator
+    __device__ __forceinline__ void set(double2 m, double2 v) {
+        re = 0.0;
+        im = 0.0;
+        add(m, v);
+    }
 };
 __device__ __forceinline__ void two_sum_acc(float &s, float &c, float t) {
     const float u = s + t;
@@ -92,7 +98,19 @@ template <> struct CAcc<float> {
     float2 s = make_float2(0.0f, 0.0f), c = make_float2(0.0f, 0.0f);
     __device__ __forceinline__ void add(float2 m, float2 v) { two_sum_acc2(s, c, cmul2(m, v)); }
     __device__ __forceinline__ float2 get() const { return __fadd2_rn(s, c); }
+    // the first term of a sum: TwoSum with an empty accumulator is exact (value t, error 0),
+    // so the term is stored directly — the same value as add() without its six additions
+    __device__ __forceinline__ void set(float2 m, float2 v) {
+        s = cmul2(m, v);
+        c = make_float2(0.0f, 0.0f);
+    }
 };
+// term c of a sum formed in a loop unrolled at compile time: the first term starts the sum
+template <typename R>
+__device__ __forceinline__ void cacc_term(CAcc<R> &a, int c, C<R> m, C<R> v) {
+    if (c == 0) a.set(m, v);
+    else a.add(m, v);
+}
 
 // ---- deterministic FP64 block reduction -----------------------------------
 // Shuffle-down tree inside each warp, then warp totals tree-reduced by warp 0.

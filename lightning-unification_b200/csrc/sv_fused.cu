@@ -219,7 +219,7 @@ __device__ __forceinline__ void r_dense(C<R> (&v)[A], const uint32_t (&l)[A], ui
             for (int r = 0; r < D; ++r) {
                 CAcc<R> acc;
 #pragma unroll
-                for (int c = 0; c < D; ++c) acc.add(cf[r * D + c], x[c]);
+                for (int c = 0; c < D; ++c) cacc_term<R>(acc, c, cf[r * D + c], x[c]);
                 v[g | dep_c(MASK, r)] = acc.get();
             }
         }
@@ -254,9 +254,9 @@ __device__ __forceinline__ void r_pair(C<R> (&v)[A], const ROp &op, const C<R> *
             if (g & MASK) continue;
             const C<R> va = v[g | LO], vb = v[g | HI];
             CAcc<R> x, y;
-            x.add(m0, va);
+            x.set(m0, va);
             x.add(m1, vb);
-            y.add(m2, va);
+            y.set(m2, va);
             y.add(m3, vb);
             v[g | LO] = x.get();
             v[g | HI] = y.get();

@@ -120,8 +120,8 @@ __global__ void __launch_bounds__(kThreads) k_dense(States s, DenseP<R, K> p) {
                 CAcc<R> a, b;
 #pragma unroll
                 for (int c = 0; c < D; ++c) {
-                    a.add(p.m[r * D + c], v[c]);
-                    b.add(p.m[r * D + D + c], v[c]);
+                    cacc_term<R>(a, c, p.m[r * D + c], v[c]);
+                    cacc_term<R>(b, c, p.m[r * D + D + c], v[c]);
                 }
                 sv[base + p.off[r]] = a.get();
                 sv[base + p.off[r + 1]] = b.get();
@@ -131,7 +131,7 @@ __global__ void __launch_bounds__(kThreads) k_dense(States s, DenseP<R, K> p) {
             for (int r = 0; r < D; ++r) {
                 CAcc<R> a;
 #pragma unroll
-                for (int c = 0; c < D; ++c) a.add(p.m[r * D + c], v[c]);
+                for (int c = 0; c < D; ++c) cacc_term<R>(a, c, p.m[r * D + c], v[c]);
                 sv[base + p.off[r]] = a.get();
             }
         }
@@ -158,7 +158,7 @@ __global__ void __launch_bounds__(kThreads) k_dense1_low(States s, Dense1LowP<R>
         o.y = __shfl_xor_sync(0xffffffffu, v.y, 1);
         const bool hi = i & 1;
         CAcc<R> a;
-        a.add(hi ? p.m[2] : p.m[0], hi ? o : v);
+        a.set(hi ? p.m[2] : p.m[0], hi ? o : v);
         a.add(hi ? p.m[3] : p.m[1], hi ? v : o);
         sv[i] = a.get();
     }
@@ -179,8 +179,8 @@ __global__ void __launch_bounds__(kThreads) k_dense_dev(States s, DenseDevP<R, K
             CAcc<R> a, b;
 #pragma unroll
             for (int c = 0; c < D; ++c) {
-                a.add(__ldg(&p.m[r * D + c]), v[c]);
-                b.add(__ldg(&p.m[r * D + D + c]), v[c]);
+                cacc_term<R>(a, c, __ldg(&p.m[r * D + c]), v[c]);
+                cacc_term<R>(b, c, __ldg(&p.m[r * D + D + c]), v[c]);
             }
             sv[base + p.off[r]] = a.get();
             sv[base + p.off[r + 1]] = b.get();
@@ -427,6 +427,12 @@ bool launch_dense_k(const States &S, int ns, uint32_t nq, const GateDesc &g, voi
     std::vector<uint32_t> all = g.tbits;
     all.insert(all.end(), g.cbits.begin(), g.cbits.end());
     const uint64_t ngroups = uint64_t(1) << (nq - all.size());
+    if constexpr (sizeof(R) == 4 && K >= 3 && K <= 5) {
+        if (dense_tc_applies(nq, g)) {  // complex64: tcgen05 with split TF32 operands
+            launch_dense_tc(S.p, ns, nq, g, scratch, st);
+            return true;
+        }
+    }
     // the tiled kernel where it measured faster than k_dense_dev on a 30-qubit state:
     // complex128 from K = 5 (17.3 vs 21.0 ms at K = 5; 10.8 vs 9.8 ms at K = 4), complex64,
     // whose compensated sums cost twice the FP64 ones, from K = 6 (42 vs 61 ms)

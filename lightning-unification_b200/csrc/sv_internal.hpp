@@ -41,6 +41,15 @@ template <typename R>
 void launch_gate(void *const *states, int nstates, uint32_t nq, const GateDesc &g,
                  void *dev_matrix_scratch, cudaStream_t st);
 
+// complex64 dense matrices on 3..5 wires on the tensor cores (sv_tensor.cu): applies when
+// the descriptor has no controls and the state holds at least one 128-group tile;
+// `scratch` must hold dense_tc_scratch_bytes(k) bytes (the split real-embedded matrix).
+bool dense_tc_applies(uint32_t nq, const GateDesc &g);
+size_t dense_tc_scratch_bytes(int k);
+void launch_dense_tc(void *const *states, int ns, uint32_t nq, const GateDesc &g, void *scratch, cudaStream_t st);
+// MMA-completion waits that gave up since the library was loaded (0 in a healthy run)
+unsigned int dense_tc_timeouts();
+
 // ---- reductions (sv_reduce.cu) -------------------------------------------
 // All reductions are two-pass and deterministic: per-block partials into
 // `partials` (kPartialsCapacity doubles), then one block finalises into a

@@ -25,7 +25,7 @@ INCLUDE = REPO / "include"
 BUILD = ROOT / "_build"
 
 CU_SOURCES = ["sv_gates.cu", "sv_reduce.cu", "sv_sample.cu", "sv_sparse.cu", "sv_fused.cu", "sv_mcmc.cu",
-              "sv_capi.cu", "sv_batch.cu", "sv_noalloc.cu"]
+              "sv_capi.cu", "sv_batch.cu", "sv_noalloc.cu", "sv_tensor.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
               "-Xcompiler", "-Wall"]

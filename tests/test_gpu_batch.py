@@ -360,3 +360,33 @@ def test_hea_batch_wide_vs_reference(ref_module, dtype):
         for col, i in enumerate(pops):
             want_g[c["param_index"][i]] += dy[ci] * jac[col]
     assert np.abs(g.cpu().numpy() - want_g).max() < GRAD_TOL[dtype]
+
+
+@pytest.mark.parametrize("dtype", [np.complex128, np.complex64])
+def test_batch_many_observables(dtype):
+    """Circuits with more observables than one forward pass accumulates (16): 37 and 5 Pauli sums,
+    forward values and the VJP against the oracle."""
+    import torch
+    from lightning_b200.batch import BatchedCircuits
+    from lightning_b200.autograd import batched_expval
+    circuits, params = hea_batch_small_many_obs()
+    eng = BatchedCircuits(circuits, len(params), dtype=dtype, use_graphs=False)
+    p = torch.tensor(params, dtype=torch.float64, device="cuda", requires_grad=True)
+    out = batched_expval(p, eng)
+    assert out.numel() == 37 + 5
+    want = oracle_outputs(circuits, params)
+    assert np.abs(out.detach().cpu().numpy() - want).max() < (1e-12 if dtype == np.complex128 else 2e-5)
+    dy = np.random.default_rng(4).normal(size=out.numel())
+    (out * torch.tensor(dy, device="cuda")).sum().backward()
+    assert np.abs(p.grad.cpu().numpy() - oracle_vjp(circuits, params, dy)).max() < GRAD_TOL[dtype]
+
+
+def hea_batch_small_many_obs():
+    from lightning_b200.workloads import hea_batch
+    circuits, params = hea_batch(ncirc=2, nmin=9, nmax=14, dmin=2, dmax=2, seed=44)
+    n0, n1 = circuits[0]["num_qubits"], circuits[1]["num_qubits"]
+    obs0 = [[(1.0, "Z", [q])] for q in range(n0)] + [[(0.5, "ZZ", [q, (q + 1) % n0])] for q in range(n0)]
+    obs0 += [[(0.3, "X", [q]), (-0.2, "Y", [(q + 2) % n0])] for q in range(37 - len(obs0))]
+    circuits[0] = dict(circuits[0], observables=obs0[:37])
+    circuits[1] = dict(circuits[1], observables=[[(1.0, "Z", [q])] for q in range(5)])
+    return circuits, params

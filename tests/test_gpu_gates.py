@@ -244,3 +244,28 @@ def test_fused_every_gate_kind_vs_reference(capi, ref_module, dtype):
     sv.upload(st)
     sv.apply_ops(ops)
     assert np.abs(sv.download() - got).max() < tol
+
+
+@pytest.mark.parametrize("k", [3, 4, 5])
+@pytest.mark.parametrize("n", [12, 13, 20])
+def test_apply_matrix_tensor_cores_c64(capi, k, n):
+    """complex64 applyMatrix on 3..5 wires runs on the tensor cores (tcgen05 kind::tf32 with split
+    operands) once the state holds a 128-group tile (n >= k + 7): lowest, highest and scattered
+    wires, both directions, against the FP64 oracle at the complex64 bound."""
+    import lq_oracle as O
+    from lightning_b200.workloads import random_unitary
+    if n < k + 7:
+        pytest.skip("state narrower than one tile")
+    rng = np.random.default_rng(300 + 10 * k + n)
+    st = random_state(rng, n, np.complex64)
+    placements = [list(range(n - k, n)), list(range(k)), [int(w) for w in rng.choice(n, k, replace=False)]]
+    for wires, inverse in zip(placements, (False, True, False)):
+        u = random_unitary(rng, k).astype(np.complex64)
+        sv = capi.StateVector(n, np.complex64)
+        sv.upload(st)
+        sv.apply_matrix(u, wires, inverse)
+        got = sv.download()
+        sv.synchronize()
+        want = O.apply_matrix(st.astype(np.complex128), u.astype(np.complex128), wires, inverse)
+        assert np.abs(got - want).max() < TOL[np.complex64], (wires, inverse)
+        assert abs(np.linalg.norm(got.astype(np.complex128)) - 1.0) < 1e-5
