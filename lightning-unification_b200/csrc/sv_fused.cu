@@ -152,6 +152,8 @@ struct alignas(16) RPhase {
 enum RCode : int32_t {
     RC_DIAG = 0,     // phases indexed by up to three tile bits (controls folded into the table)
     RC_PARITY = 1,   // phase chosen by the parity of selected bits (MultiRZ)
+    RC_DIAG_T = 2,   // RC_DIAG whose index bits are all thread bits: one factor for the thread
+    RC_PARITY_T = 3, // RC_PARITY whose tile bits are all thread bits
     RC_DENSE1 = 16,  // + register bit
     RC_DENSE2 = 32,  // + index of the two-bit mask
     RC_DENSE3 = 48,  // + index of the three-bit mask
@@ -218,8 +220,9 @@ __device__ __forceinline__ void r_dense(C<R> (&v)[A], const uint32_t (&l)[A], ui
 #pragma unroll
             for (int r = 0; r < D; ++r) {
                 CAcc<R> acc;
+                acc.set(cf[r * D], x[0]);
 #pragma unroll
-                for (int c = 0; c < D; ++c) cacc_term<R>(acc, c, cf[r * D + c], x[c]);
+                for (int c = 1; c < D; ++c) acc.add(cf[r * D + c], x[c]);
                 v[g | dep_c(MASK, r)] = acc.get();
             }
         }
@@ -290,11 +293,29 @@ __device__ __forceinline__ void r_parity(C<R> (&v)[A], const uint32_t (&l)[A], c
     for (int g = 0; g < A; ++g) v[g] = cprod<R>((__popc(l[g] & op.pm) & 1) ? ph1 : ph0, v[g]);
 }
 
+// A diagonal step whose index bits all come from the thread index multiplies every amplitude
+// the thread holds by the same factor.  Such a scalar commutes with every step of the phase
+// (they act linearly within the thread's registers), so the factors are multiplied into one
+// value tf, applied once when the phase ends: one product per step and thread instead of one
+// per amplitude, with as many roundings per amplitude as applying the steps one by one.
 template <typename R, int A>
 __device__ __forceinline__ void run_rop(C<R> (&v)[A], const uint32_t (&l)[A], const ROp &op,
-                                        const C<R> *__restrict__ scf, uint64_t tbase) {
+                                        const C<R> *__restrict__ scf, uint64_t tbase, uint32_t base, C<R> &tf,
+                                        bool &has_tf) {
     const C<R> *cf = scf + op.coef;
     switch (op.code) {
+    case RC_DIAG_T: {
+        const uint32_t idx = (((base >> op.p0) & 1u) << 2) | (((base >> op.p1) & 1u) << 1) | ((base >> op.p2) & 1u);
+        tf = has_tf ? cprod<R>(cf[idx], tf) : cf[idx];
+        has_tf = true;
+        break;
+    }
+    case RC_PARITY_T: {
+        const int par = (__popcll(tbase & op.pmg) + __popc(base & op.pm)) & 1;
+        tf = has_tf ? cprod<R>(cf[par], tf) : cf[par];
+        has_tf = true;
+        break;
+    }
     case RC_DIAG: r_diag<R, A>(v, l, op, cf); break;
     case RC_PARITY: r_parity<R, A>(v, l, op, cf, tbase); break;
     case RC_DENSE1 + 0: r_dense<R, A, 1, false>(v, l, op.cmask, cf); break;
@@ -394,6 +415,7 @@ __global__ void __launch_bounds__(kFThreads, 1) k_fused(C<R> *__restrict__ state
     constexpr int PER = (int)(TN / V) / kFThreads;  // 16-byte chunks per thread
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ uint8_t s_lbits[16], s_gbits[48];
+    __shared__ uint64_t s_hi[PER];  // state offset of chunk row j (the same for every thread)
     C<R> *const buf0 = reinterpret_cast<C<R> *>(smem_raw);
     RPhase *sph = reinterpret_cast<RPhase *>(smem_raw + 2 * sizeof(C<R>) * TN);
     ROp *srop = reinterpret_cast<ROp *>(sph + a.nph);
@@ -410,22 +432,19 @@ __global__ void __launch_bounds__(kFThreads, 1) k_fused(C<R> *__restrict__ state
     stage(sfop, a.fops, a.nfop);
     stage(scf, static_cast<const C<R> *>(a.coefs), a.ncoef);
     __syncthreads();
-    // per-thread address parts of the tile moves: chunk c -> tile amplitude c * V
+    // address parts of the tile moves: chunk c = threadIdx.x + j * 512 -> tile amplitude c * V
+    if (threadIdx.x < PER) s_hi[threadIdx.x] = deposit((uint64_t)threadIdx.x * kFThreads * V, s_lbits, KT);
+    __syncthreads();
     const uint64_t lo = deposit((uint64_t)threadIdx.x * V, s_lbits, KT);
-    uint64_t hi[PER];
-    uint32_t sw[PER];  // swizzled shared-memory positions of the chunks
-#pragma unroll
-    for (int j = 0; j < PER; ++j) {
-        hi[j] = deposit((uint64_t)j * kFThreads * V, s_lbits, KT);
-        sw[j] = swz<R>((threadIdx.x + j * kFThreads) * V);
-    }
+    // swizzled shared-memory position of chunk j of this thread
+    auto sw = [&](int j) { return swz<R>((threadIdx.x + (uint32_t)j * kFThreads) * V); };
 
     uint64_t t = blockIdx.x;
     uint32_t cur = 0;
     if (t < ntiles) {
         const uint64_t tb = deposit(t, s_gbits, a.ng);
 #pragma unroll
-        for (int j = 0; j < PER; ++j) cp_async16(buf0 + sw[j], state + (tb | lo | hi[j]));
+        for (int j = 0; j < PER; ++j) cp_async16(buf0 + sw(j), state + (tb | lo | s_hi[j]));
     }
     cp_async_commit();
     for (; t < ntiles; t += gridDim.x) {
@@ -434,7 +453,7 @@ __global__ void __launch_bounds__(kFThreads, 1) k_fused(C<R> *__restrict__ state
             const uint64_t tb = deposit(tnext, s_gbits, a.ng);
             C<R> *dst = buf0 + (cur ^ 1u) * TN;
 #pragma unroll
-            for (int j = 0; j < PER; ++j) cp_async16(dst + sw[j], state + (tb | lo | hi[j]));
+            for (int j = 0; j < PER; ++j) cp_async16(dst + sw(j), state + (tb | lo | s_hi[j]));
         }
         cp_async_commit();
         cp_async_wait1();
@@ -458,15 +477,21 @@ __global__ void __launch_bounds__(kFThreads, 1) k_fused(C<R> *__restrict__ state
 #pragma unroll
             for (int g = 0; g < A; ++g) v[g] = s[sbase ^ ph.srdep[g]];
             const int oe = ph.op_begin + ph.nops;
-            for (int o = ph.op_begin; o < oe; ++o) run_rop<R, A>(v, l, srop[o], scf, tbase);
+            C<R> tf = mk<R>(1, 0);
+            bool has_tf = false;
+            for (int o = ph.op_begin; o < oe; ++o) run_rop<R, A>(v, l, srop[o], scf, tbase, base, tf, has_tf);
+            if (has_tf) {
+#pragma unroll
+                for (int g = 0; g < A; ++g) v[g] = cprod<R>(tf, v[g]);
+            }
 #pragma unroll
             for (int g = 0; g < A; ++g) s[sbase ^ ph.srdep[g]] = v[g];
             __syncthreads();
         }
 #pragma unroll
         for (int j = 0; j < PER; ++j) {
-            const float4 x = *reinterpret_cast<const float4 *>(s + sw[j]);
-            *reinterpret_cast<float4 *>(state + (tbase | lo | hi[j])) = x;
+            const float4 x = *reinterpret_cast<const float4 *>(s + sw(j));
+            *reinterpret_cast<float4 *>(state + (tbase | lo | s_hi[j])) = x;
         }
         __syncthreads();  // the buffer is refilled next iteration
         cur ^= 1u;
@@ -734,6 +759,9 @@ void lower_phase(SegCode<R> &sc, uint32_t rmask, const std::vector<const GateDes
             r.p0 = pos[0];
             r.p1 = pos[1];
             r.p2 = pos[2];
+            uint32_t used = 0;
+            for (size_t j = 0; j < ib.size(); ++j) used |= 1u << pos[j];
+            if ((used & rmask) == 0) r.code = RC_DIAG_T;  // thread bits only (also with no index bits)
             const int kt_ = g.k, kc = (int)g.cbits.size();
             for (int idx = 0; idx < 8; ++idx) {
                 // idx bit (2 - j) holds index bit j; absent bits are zero in every address
@@ -756,6 +784,7 @@ void lower_phase(SegCode<R> &sc, uint32_t rmask, const std::vector<const GateDes
                 if (loc[b] >= 0) r.pm |= 1u << loc[b];
                 else r.pmg |= uint64_t(1) << b;
             }
+            if ((r.pm & rmask) == 0) r.code = RC_PARITY_T;
             sc.coefs.push_back(to_r<R>(g.pphase[0]));
             sc.coefs.push_back(to_r<R>(g.pphase[1]));
             sc.rops.push_back(r);

@@ -142,16 +142,24 @@ __global__ void __launch_bounds__(kTcThreads) k_dense_tc(TcStates s, TcP p) {
     uint32_t phase = 0;
     bool ok = true;
 
-    for (uint64_t t = blockIdx.x; t < p.ntiles && ok; t += gridDim.x) {
-        const uint64_t base = p.ins(t * kTcM + threadIdx.x);
-        // row threadIdx.x: load, split, store to the operand layouts
+    // Software pipeline: the amplitudes of the thread's next row are loaded into registers while
+    // the MMAs and the epilogue of the current tile run (tiles are disjoint sets of amplitudes).
+    float2 x[D];
+    uint64_t t = blockIdx.x;
+    uint64_t base = 0;
+    if (t < p.ntiles) {
+        base = p.ins(t * kTcM + threadIdx.x);
+#pragma unroll
+        for (int c = 0; c < D; ++c) x[c] = sv[base + p.off[c]];
+    }
+    for (; t < p.ntiles && ok; t += gridDim.x) {
+        // row threadIdx.x: split and store to the operand layouts
 #pragma unroll
         for (int c = 0; c < D; ++c) {
-            const float2 x = sv[base + p.off[c]];
-            const float hx = tf32_rna(x.x), hy = tf32_rna(x.y);
+            const float hx = tf32_rna(x[c].x), hy = tf32_rna(x[c].y);
             const uint32_t o = core_off(threadIdx.x, 2 * c, KK);
             *reinterpret_cast<float2 *>(sa_hi + o) = make_float2(hx, hy);
-            *reinterpret_cast<float2 *>(sa_lo + o) = make_float2(x.x - hx, x.y - hy);
+            *reinterpret_cast<float2 *>(sa_lo + o) = make_float2(x[c].x - hx, x[c].y - hy);
         }
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncthreads();
@@ -170,6 +178,14 @@ __global__ void __launch_bounds__(kTcThreads) k_dense_tc(TcStates s, TcP p) {
             asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
                              smem_u32(&mbar))
                          : "memory");
+        }
+        // the next tile's row, in flight during the MMAs and the epilogue
+        const uint64_t cur = base;
+        const uint64_t tn = t + gridDim.x;
+        if (tn < p.ntiles) {
+            base = p.ins(tn * kTcM + threadIdx.x);
+#pragma unroll
+            for (int c = 0; c < D; ++c) x[c] = sv[base + p.off[c]];
         }
         // wait for the MMAs (bounded)
         uint32_t done = 0;
@@ -196,7 +212,7 @@ __global__ void __launch_bounds__(kTcThreads) k_dense_tc(TcStates s, TcP p) {
                 float v[16];
                 tmem_ld<16>(lane_base + chunk * 16, v);
 #pragma unroll
-                for (int j = 0; j < 8; ++j) sv[base + p.off[chunk * 8 + j]] = make_float2(v[2 * j], v[2 * j + 1]);
+                for (int j = 0; j < 8; ++j) sv[cur + p.off[chunk * 8 + j]] = make_float2(v[2 * j], v[2 * j + 1]);
             }
         }
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -255,7 +271,7 @@ void launch_tc(float2 *const *states, int ns, uint32_t nq, const GateDesc &g, vo
     p.b = static_cast<const float *>(scratch);
     const int smem = 2 * (kTcM * KK * 4) + 2 * (NN * KK * 4);
     B200SV_CUDA(cudaFuncSetAttribute(k_dense_tc<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    const int per_sm = K == 3 ? 8 : K == 4 ? 4 : 2;
+    const int per_sm = K == 3 ? 12 : K == 4 ? 5 : 2;  // CTAs that fit an SM's shared memory
     const uint64_t grid = std::min<uint64_t>(p.ntiles, (uint64_t)sm_count() * per_sm);
     TcStates S{};
     for (int i = 0; i < ns; ++i) S.p[i] = states[i];
