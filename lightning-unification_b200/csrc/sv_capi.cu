@@ -1044,66 +1044,85 @@ int b200sv_adjoint_jacobian(b200sv_handle psi, const b200sv_op *ops, uint32_t no
 
         B200SV_CUDA(cudaMemcpyAsync(lambda, h->d_state, h->state_bytes(), cudaMemcpyDeviceToDevice, st));
         if (apply_operations) {
-            for (auto &o : rec) {
-                void *s[1] = {lambda};
-                apply_desc(h, s, 1, compile_op(o, o.inverse, h->nq));
-            }
+            std::vector<GateDesc> fwd;
+            for (auto &o : rec) fwd.push_back(compile_op(o, o.inverse, h->nq));
+            void *s1[1] = {lambda};
+            if (fused_worthwhile(h->dtype, h->nq))
+                apply_fused(lambda, h->nq, h->dtype, fwd, [&](const GateDesc &g) { apply_desc(h, s1, 1, g); }, st);
+            else
+                for (auto &g : fwd) apply_desc(h, s1, 1, g);
         }
         for (uint32_t o = 0; o < nobs; ++o) apply_observable(h, orec[o], lambda, bras[o], tmp);
 
-        int64_t tp_pos = (int64_t)ntp - 1;  // reverse iterator over trainable
-        int64_t trainable_number = (int64_t)ntp - 1;
-        int64_t current_param_idx = (int64_t)num_param_ops - 1;
-        std::vector<void *> lambda_and_bras{lambda};
-        lambda_and_bras.insert(lambda_and_bras.end(), bras.begin(), bras.end());
-        for (int64_t op_idx = (int64_t)rec.size() - 1; op_idx >= 0; --op_idx) {
-            const OpRec &op = rec[op_idx];
-            if (op.params.size() > 1)
-                throw ArgError("The operation is not supported using the adjoint differentiation method");
-            if (op.gate == B200SV_OP_SKIP) continue;
-            if (tp_pos < 0) break;
-            if (!op.params.empty()) {
-                if ((uint64_t)current_param_idx == trainable[tp_pos]) {
-                    const int gen = generator_of_gate(op.gate);
-                    if (gen < 0)
-                        throw ArgError("The operation is not supported using the adjoint differentiation method");
-                    double sc = 0.0;
-                    GateDesc G = compile_generator((uint32_t)gen, op.wires.data(), (uint32_t)op.wires.size(), h->nq, &sc);
-                    const double scaling = sc * (op.inverse ? -1.0 : 1.0);
-                    // one-wire gates: the products and the inverse gate in one pass over the pairs
-                    GateDesc adj1 = compile_op(op, !op.inverse, h->nq);
-                    cd g2[4], u2[4];
-                    if (nobs >= 1 && nobs <= 16 && as_one_wire(G, g2) && as_one_wire(adj1, u2) &&
-                        G.tbits[0] == adj1.tbits[0]) {
-                        double *dst = d_jac + (size_t)trainable_number * nobs;
-                        if (h->dtype == B200SV_C64)
-                            adjoint_rot_step<float>(lambda, bras.data(), (int)nobs, h->nq, G.tbits[0], g2, u2,
-                                                    -2.0 * scaling, h->d_partials, dst, 1, h->arrival(), st);
-                        else
-                            adjoint_rot_step<double>(lambda, bras.data(), (int)nobs, h->nq, G.tbits[0], g2, u2,
-                                                     -2.0 * scaling, h->d_partials, dst, 1, h->arrival(), st);
+        // the reverse sweep as a list of steps, with the reference's bookkeeping: reverse
+        // traversal, trainable-parameter cursor, early exit once every trainable parameter is done
+        std::vector<AdjItem> items;
+        {
+            int64_t tp_pos = (int64_t)ntp - 1;  // reverse iterator over trainable
+            int64_t trainable_number = (int64_t)ntp - 1;
+            int64_t current_param_idx = (int64_t)num_param_ops - 1;
+            for (int64_t op_idx = (int64_t)rec.size() - 1; op_idx >= 0; --op_idx) {
+                const OpRec &op = rec[op_idx];
+                if (op.params.size() > 1)
+                    throw ArgError("The operation is not supported using the adjoint differentiation method");
+                if (op.gate == B200SV_OP_SKIP) continue;
+                if (tp_pos < 0) break;
+                AdjItem it;
+                it.adj = compile_op(op, !op.inverse, h->nq);
+                if (!op.params.empty()) {
+                    if ((uint64_t)current_param_idx == trainable[tp_pos]) {
+                        const int gen = generator_of_gate(op.gate);
+                        if (gen < 0)
+                            throw ArgError("The operation is not supported using the adjoint differentiation method");
+                        double sc = 0.0;
+                        it.G = compile_generator((uint32_t)gen, op.wires.data(), (uint32_t)op.wires.size(), h->nq, &sc);
+                        it.diff = true;
+                        it.alpha = -2.0 * sc * (op.inverse ? -1.0 : 1.0);
+                        it.col = trainable_number;
                         --trainable_number;
                         --tp_pos;
-                        --current_param_idx;
-                        continue;
                     }
-                    for (uint32_t o0 = 0; o0 < nobs; o0 += 16) {
-                        const int cnt = (int)std::min<uint32_t>(16, nobs - o0);
-                        double *dst = d_jac + (size_t)trainable_number * nobs + o0;
-                        if (h->dtype == B200SV_C64)
-                            reduce_generator_inner<float>(bras.data() + o0, cnt, lambda, h->nq, G, -2.0 * scaling,
-                                                          h->d_partials, dst, 1, st, h->arrival());
-                        else
-                            reduce_generator_inner<double>(bras.data() + o0, cnt, lambda, h->nq, G, -2.0 * scaling,
-                                                           h->d_partials, dst, 1, st, h->arrival());
-                    }
-                    --trainable_number;
-                    --tp_pos;
+                    --current_param_idx;
                 }
-                --current_param_idx;
+                items.push_back(std::move(it));
             }
-            GateDesc adj = compile_op(op, !op.inverse, h->nq);
-            apply_desc_multi(h, lambda_and_bras, adj);  // lambda and every bra in one launch
+        }
+        std::vector<void *> lambda_and_bras{lambda};
+        lambda_and_bras.insert(lambda_and_bras.end(), bras.begin(), bras.end());
+        // one step: the products (one-wire gates: products and inverse in one pass over the pairs)
+        auto exec_single = [&](size_t i) {
+            const AdjItem &it = items[i];
+            if (it.diff) {
+                cd g2[4], u2[4];
+                if (nobs >= 1 && nobs <= 16 && as_one_wire(it.G, g2) && as_one_wire(it.adj, u2) &&
+                    it.G.tbits[0] == it.adj.tbits[0]) {
+                    double *dst = d_jac + (size_t)it.col * nobs;
+                    if (h->dtype == B200SV_C64)
+                        adjoint_rot_step<float>(lambda, bras.data(), (int)nobs, h->nq, it.G.tbits[0], g2, u2, it.alpha,
+                                                h->d_partials, dst, 1, h->arrival(), st);
+                    else
+                        adjoint_rot_step<double>(lambda, bras.data(), (int)nobs, h->nq, it.G.tbits[0], g2, u2, it.alpha,
+                                                 h->d_partials, dst, 1, h->arrival(), st);
+                    return;
+                }
+                for (uint32_t o0 = 0; o0 < nobs; o0 += 16) {
+                    const int cnt = (int)std::min<uint32_t>(16, nobs - o0);
+                    double *dst = d_jac + (size_t)it.col * nobs + o0;
+                    if (h->dtype == B200SV_C64)
+                        reduce_generator_inner<float>(bras.data() + o0, cnt, lambda, h->nq, it.G, it.alpha,
+                                                      h->d_partials, dst, 1, st, h->arrival());
+                    else
+                        reduce_generator_inner<double>(bras.data() + o0, cnt, lambda, h->nq, it.G, it.alpha,
+                                                       h->d_partials, dst, 1, st, h->arrival());
+                }
+            }
+            apply_desc_multi(h, lambda_and_bras, it.adj);  // lambda and every bra in one launch
+        };
+        if (nobs == 1 && fused_adjoint_worthwhile(h->dtype, h->nq)) {
+            // one bra (the VJP form): fused passes over lambda and the bra
+            apply_fused_adjoint(lambda, bras[0], h->nq, h->dtype, items, exec_single, d_jac, st);
+        } else {
+            for (size_t i = 0; i < items.size(); ++i) exec_single(i);
         }
         std::vector<double> jt((size_t)ntp * nobs);
         if (!jt.empty())

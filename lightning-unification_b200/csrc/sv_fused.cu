@@ -171,7 +171,8 @@ struct alignas(16) ROp {
     uint32_t p0, p1, p2; // Diag: tile positions of the index bits (p0 the most significant)
     uint32_t pm;     // Parity: tile-local bits
     uint64_t pmg;    // Parity: state bits outside the tile
-    uint64_t pad2;
+    int32_t prod;    // adjoint sweep: generator product computed before this step (index), or -1
+    int32_t pad3;
 };
 
 // masks of a-bit registers with two and three bits set, in increasing order
@@ -705,10 +706,13 @@ template <typename R> int64_t reg_targets(const GateDesc &g, const std::vector<i
     return (int64_t)m;
 }
 
-template <typename R>
+// hook(i, rop, rpos) runs before op i's record is stored (rpos: tile bit -> register bit)
+using RopHook = std::function<void(size_t, ROp &, const int *)>;
+
+template <typename R, typename G = Geo<R>>
 void lower_phase(SegCode<R> &sc, uint32_t rmask, const std::vector<const GateDesc *> &ops,
-                 const std::vector<int> &loc) {
-    constexpr int KT = Geo<R>::kt, a = Geo<R>::a, A = Geo<R>::A;
+                 const std::vector<int> &loc, const RopHook &hook = nullptr) {
+    constexpr int KT = G::kt, a = G::a, A = G::A;
     // pad the register bits to a bits with the highest free tile bits
     for (int b = KT - 1; b >= 0 && __builtin_popcount(rmask) < a; --b)
         if (!((rmask >> b) & 1)) rmask |= 1u << b;
@@ -740,10 +744,15 @@ void lower_phase(SegCode<R> &sc, uint32_t rmask, const std::vector<const GateDes
             if ((bits == 2 ? mask2(i) : mask3(i)) == m) return i;
         return -1;
     };
-    for (const GateDesc *gp : ops) {
-        const GateDesc &g = *gp;
+    auto emit = [&](size_t i, ROp &r) {
+        if (hook) hook(i, r, rpos);
+        sc.rops.push_back(r);
+    };
+    for (size_t oi = 0; oi < ops.size(); ++oi) {
+        const GateDesc &g = *ops[oi];
         if (g.kind == Kind::Noop) continue;
         ROp r{};
+        r.prod = -1;
         r.coef = (int32_t)sc.coefs.size();
         for (auto b : g.cbits) r.cmask |= 1u << loc[b];
         if (g.kind == Kind::Diag) {
@@ -774,7 +783,7 @@ void lower_phase(SegCode<R> &sc, uint32_t rmask, const std::vector<const GateDes
                 }
                 sc.coefs.push_back(to_r<R>(all_c ? g.m[t] : cd(1.0, 0.0)));
             }
-            sc.rops.push_back(r);
+            emit(oi, r);
             continue;
         }
         if (g.kind == Kind::Parity) {
@@ -787,7 +796,7 @@ void lower_phase(SegCode<R> &sc, uint32_t rmask, const std::vector<const GateDes
             if ((r.pm & rmask) == 0) r.code = RC_PARITY_T;
             sc.coefs.push_back(to_r<R>(g.pphase[0]));
             sc.coefs.push_back(to_r<R>(g.pphase[1]));
-            sc.rops.push_back(r);
+            emit(oi, r);
             continue;
         }
         // register bit of each target, and the target mask over the register bits
@@ -800,7 +809,7 @@ void lower_phase(SegCode<R> &sc, uint32_t rmask, const std::vector<const GateDes
         }
         if (g.kind == Kind::Swap) {
             r.code = k == 1 ? RC_SWAP1 + regb[0] : RC_SWAP2 + index_of(mask, 2);
-            sc.rops.push_back(r);
+            emit(oi, r);
             continue;
         }
         if (g.kind == Kind::Pair && k == 2) {
@@ -813,7 +822,7 @@ void lower_phase(SegCode<R> &sc, uint32_t rmask, const std::vector<const GateDes
             const cd blk[4] = {pa_low ? m00 : m11, pa_low ? m01 : m10, pa_low ? m10 : m01, pa_low ? m11 : m00};
             for (auto &z : blk) sc.coefs.push_back(to_r<R>(z));
             sc.coefs.push_back(to_r<R>(g.gamma));
-            sc.rops.push_back(r);
+            emit(oi, r);
             continue;
         }
         // Dense (and the one-bit Pair form): canonical matrix, index bit i <-> i-th lowest mask bit
@@ -833,7 +842,7 @@ void lower_phase(SegCode<R> &sc, uint32_t rmask, const std::vector<const GateDes
             for (int cc = 0; cc < D; ++cc) sc.coefs.push_back(to_r<R>(m[orig(rr) * D + orig(cc)]));
         r.code = k == 1 ? RC_DENSE1 + regb[0] : k == 2 ? RC_DENSE2 + index_of(mask, 2) : RC_DENSE3 + index_of(mask, 3);
         if (r.cmask) r.code += RC_CTL;
-        sc.rops.push_back(r);
+        emit(oi, r);
     }
     ph.nops = (int32_t)sc.rops.size() - ph.op_begin;
     sc.phases.push_back(ph);
@@ -1047,6 +1056,492 @@ void run_fused(void *state, uint32_t nq, const std::vector<GateDesc> &descs,
     }
 }
 
+// ==== fused adjoint sweep ====================================================================
+// The reverse sweep of the adjoint method (AdjointJacobianLQubit.hpp:212-335) over lambda
+// and one bra: for each op, from the last, the product -2 scale Im<bra|G|lambda> when the op
+// is differentiated, then the op's inverse on both states.  Runs of these steps whose bits
+// fit a tile run as one pass over both states: the tile holds 2^kt amplitudes of each state,
+// each thread A of each in registers (fewer than the forward kernel: two states share the
+// register budget), and the phases apply each step to both states.  A product is formed per
+// thread in FP64, summed over the warp with shuffles and added to the warp's slot of the
+// step's accumulator in shared memory; after its tiles each CTA writes the sum of its warps'
+// slots (fixed order), and a finalize kernel adds the CTAs' values (fixed order), so results
+// are reproducible run to run.
+
+template <typename R> struct GeoA;
+template <> struct GeoA<double> { static constexpr int kt = 11, a = 2, A = 4, reserve = 3; };
+template <> struct GeoA<float> { static constexpr int kt = 12, a = 3, A = 8, reserve = 4; };
+
+constexpr int kMaxAdjItems = 96;
+constexpr int kMaxAdjCoefs = 1024;
+constexpr int kWarps = kFThreads / 32;
+
+enum PCode : int32_t { PG_DIAG = 0, PG_PARITY = 1, PG_PAIR1 = 16 /* + register bit */ };
+
+struct alignas(16) PProd {
+    int32_t kind;
+    int32_t item;   // accumulator row (differentiated step of the segment)
+    int32_t coef;   // first FP64 coefficient (segment-local)
+    uint32_t p0, p1, p2, pm;
+    uint32_t pad;
+    uint64_t pmg;
+};
+
+struct AdjSegArgs {
+    const RPhase *phases;
+    const ROp *rops;
+    const PProd *prods;
+    const void *coefs;      // gate coefficients (C<R>)
+    const double2 *gcoefs;  // generator coefficients (FP64)
+    int nph, nrop, nprod, ncoef, ngcoef, nitems;
+    int ng;
+    uint8_t lbits[16];
+    uint8_t gbits[48];
+};
+
+__device__ __forceinline__ double im_conj(double2 w, double2 v) { return w.x * v.y - w.y * v.x; }
+__device__ __forceinline__ double re_conj(double2 w, double2 v) { return w.x * v.x + w.y * v.y; }
+
+// sum over this thread's amplitude groups of Im(conj(w) . G v), FP64
+template <typename R, int A, int BIT>
+__device__ __forceinline__ double prod_pair1(const C<R> (&v)[A], const C<R> (&w)[A], const double2 *__restrict__ m) {
+    double p = 0.0;
+    if constexpr ((1 << BIT) < A) {
+        constexpr int B = 1 << BIT;
+#pragma unroll
+        for (int g = 0; g < A; ++g) {
+            if (g & B) continue;
+            const double2 v0 = widen<R>(v[g]), v1 = widen<R>(v[g | B]);
+            const double2 w0 = widen<R>(w[g]), w1 = widen<R>(w[g | B]);
+            // (G v)_r = m[2r] v0 + m[2r+1] v1
+            const double2 g0 = make_double2(m[0].x * v0.x - m[0].y * v0.y + m[1].x * v1.x - m[1].y * v1.y,
+                                            m[0].x * v0.y + m[0].y * v0.x + m[1].x * v1.y + m[1].y * v1.x);
+            const double2 g1 = make_double2(m[2].x * v0.x - m[2].y * v0.y + m[3].x * v1.x - m[3].y * v1.y,
+                                            m[2].x * v0.y + m[2].y * v0.x + m[3].x * v1.y + m[3].y * v1.x);
+            p += im_conj(w0, g0) + im_conj(w1, g1);
+        }
+    }
+    return p;
+}
+
+template <typename R, int A>
+__device__ __forceinline__ double r_product(const C<R> (&v)[A], const C<R> (&w)[A], const uint32_t (&l)[A],
+                                            const PProd &q, const double2 *__restrict__ gcf, uint64_t tbase) {
+    const double2 *m = gcf + q.coef;
+    double p = 0.0;
+    switch (q.kind) {
+    case PG_DIAG:
+#pragma unroll
+        for (int g = 0; g < A; ++g) {
+            const uint32_t x = l[g];
+            const uint32_t idx = (((x >> q.p0) & 1u) << 2) | (((x >> q.p1) & 1u) << 1) | ((x >> q.p2) & 1u);
+            const double2 d = m[idx], vv = widen<R>(v[g]), ww = widen<R>(w[g]);
+            p += d.x * im_conj(ww, vv) + d.y * re_conj(ww, vv);
+        }
+        break;
+    case PG_PARITY: {
+        const int tp = __popcll(tbase & q.pmg) & 1;
+#pragma unroll
+        for (int g = 0; g < A; ++g) {
+            const double2 d = m[(__popc(l[g] & q.pm) & 1) ^ tp], vv = widen<R>(v[g]), ww = widen<R>(w[g]);
+            p += d.x * im_conj(ww, vv) + d.y * re_conj(ww, vv);
+        }
+        break;
+    }
+    case PG_PAIR1 + 0: p = prod_pair1<R, A, 0>(v, w, m); break;
+    case PG_PAIR1 + 1: p = prod_pair1<R, A, 1>(v, w, m); break;
+    case PG_PAIR1 + 2: p = prod_pair1<R, A, 2>(v, w, m); break;
+    default: break;
+    }
+    return p;
+}
+
+template <typename R>
+__global__ void __launch_bounds__(kFThreads, 1) k_fused_adj(C<R> *__restrict__ lam, C<R> *__restrict__ bra,
+                                                            AdjSegArgs a, uint64_t ntiles, double *partials) {
+    constexpr int KT = GeoA<R>::kt, A = GeoA<R>::A;
+    constexpr uint32_t TN = 1u << KT;
+    constexpr int V = 16 / (int)sizeof(C<R>);
+    constexpr int PER = (int)(TN / V) / kFThreads;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ uint8_t s_lbits[16], s_gbits[48];
+    __shared__ uint64_t s_hi[PER];
+    // buffers: [cur][state] tiles of TN amplitudes
+    C<R> *const buf = reinterpret_cast<C<R> *>(smem_raw);
+    RPhase *sph = reinterpret_cast<RPhase *>(smem_raw + 4 * sizeof(C<R>) * TN);
+    ROp *srop = reinterpret_cast<ROp *>(sph + a.nph);
+    PProd *sprod = reinterpret_cast<PProd *>(srop + a.nrop);
+    double2 *sgcf = reinterpret_cast<double2 *>(sprod + a.nprod);
+    double *sacc = reinterpret_cast<double *>(sgcf + a.ngcoef);
+    C<R> *scf = reinterpret_cast<C<R> *>(sacc + (size_t)a.nitems * kWarps);
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int i = 0; i < 16; ++i) s_lbits[i] = a.lbits[i];
+#pragma unroll
+        for (int i = 0; i < 48; ++i) s_gbits[i] = a.gbits[i];
+    }
+    stage(sph, a.phases, a.nph);
+    stage(srop, a.rops, a.nrop);
+    stage(sprod, a.prods, a.nprod);
+    stage(sgcf, a.gcoefs, a.ngcoef);
+    stage(scf, static_cast<const C<R> *>(a.coefs), a.ncoef);
+    for (int i = threadIdx.x; i < a.nitems * kWarps; i += blockDim.x) sacc[i] = 0.0;
+    __syncthreads();
+    if (threadIdx.x < PER) s_hi[threadIdx.x] = deposit((uint64_t)threadIdx.x * kFThreads * V, s_lbits, KT);
+    __syncthreads();
+    const uint64_t lo = deposit((uint64_t)threadIdx.x * V, s_lbits, KT);
+    auto sw = [&](int j) { return swz<R>((threadIdx.x + (uint32_t)j * kFThreads) * V); };
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+    uint64_t t = blockIdx.x;
+    uint32_t cur = 0;
+    auto load = [&](uint64_t tile, uint32_t b) {
+        const uint64_t tb = deposit(tile, s_gbits, a.ng);
+        C<R> *dl = buf + (2 * b) * TN, *db = buf + (2 * b + 1) * TN;
+#pragma unroll
+        for (int j = 0; j < PER; ++j) {
+            cp_async16(dl + sw(j), lam + (tb | lo | s_hi[j]));
+            cp_async16(db + sw(j), bra + (tb | lo | s_hi[j]));
+        }
+    };
+    if (t < ntiles) load(t, 0);
+    cp_async_commit();
+    for (; t < ntiles; t += gridDim.x) {
+        const uint64_t tnext = t + gridDim.x;
+        if (tnext < ntiles) load(tnext, cur ^ 1u);
+        cp_async_commit();
+        cp_async_wait1();
+        __syncthreads();
+        C<R> *sl = buf + (2 * cur) * TN, *sb = buf + (2 * cur + 1) * TN;
+        const uint64_t tbase = deposit(t, s_gbits, a.ng);
+        for (int p = 0; p < a.nph; ++p) {
+            const RPhase &ph = sph[p];
+            const uint32_t base = pdep32(threadIdx.x, ph.comp);
+            const uint32_t sbase = swz<R>(base);
+            uint32_t l[A];
+            C<R> v[A], w[A];
+#pragma unroll
+            for (int g = 0; g < A; ++g) l[g] = base | ph.rdep[g];
+#pragma unroll
+            for (int g = 0; g < A; ++g) {
+                v[g] = sl[sbase ^ ph.srdep[g]];
+                w[g] = sb[sbase ^ ph.srdep[g]];
+            }
+            C<R> tf = mk<R>(1, 0), tf2 = mk<R>(1, 0);
+            bool has_tf = false, unused = false;
+            const int oe = ph.op_begin + ph.nops;
+            for (int o = ph.op_begin; o < oe; ++o) {
+                const ROp &op = srop[o];
+                if (op.prod >= 0) {
+                    // the deferred thread factor is a unit scalar common to both states: the
+                    // product does not see it
+                    const PProd &q = sprod[op.prod];
+                    double pr = r_product<R, A>(v, w, l, q, sgcf, tbase);
+#pragma unroll
+                    for (int off = 16; off > 0; off >>= 1) pr += __shfl_xor_sync(0xffffffffu, pr, off);
+                    if (lane == 0) sacc[q.item * kWarps + warp] += pr;
+                }
+                run_rop<R, A>(v, l, op, scf, tbase, base, tf, has_tf);
+                if (op.code != RC_DIAG_T && op.code != RC_PARITY_T)
+                    run_rop<R, A>(w, l, op, scf, tbase, base, tf2, unused);
+            }
+            if (has_tf) {
+#pragma unroll
+                for (int g = 0; g < A; ++g) {
+                    v[g] = cprod<R>(tf, v[g]);
+                    w[g] = cprod<R>(tf, w[g]);
+                }
+            }
+#pragma unroll
+            for (int g = 0; g < A; ++g) {
+                sl[sbase ^ ph.srdep[g]] = v[g];
+                sb[sbase ^ ph.srdep[g]] = w[g];
+            }
+            __syncthreads();
+        }
+#pragma unroll
+        for (int j = 0; j < PER; ++j) {
+            *reinterpret_cast<float4 *>(lam + (tbase | lo | s_hi[j])) = *reinterpret_cast<const float4 *>(sl + sw(j));
+            *reinterpret_cast<float4 *>(bra + (tbase | lo | s_hi[j])) = *reinterpret_cast<const float4 *>(sb + sw(j));
+        }
+        __syncthreads();
+        cur ^= 1u;
+    }
+    cp_async_wait0();
+    __syncthreads();
+    for (int i = threadIdx.x; i < a.nitems; i += blockDim.x) {
+        double sum = 0.0;
+        for (int wv = 0; wv < kWarps; ++wv) sum += sacc[i * kWarps + wv];
+        partials[(size_t)i * gridDim.x + blockIdx.x] = sum;
+    }
+}
+
+// jac[col[i]] = alpha[i] * sum_b partials[i * nb + b]   (one block per item, fixed order)
+__global__ void k_adj_fused_final(const double *__restrict__ partials, int nb, const double *__restrict__ alpha,
+                                  const int64_t *__restrict__ col, double *__restrict__ jac) {
+    __shared__ double sm[32];
+    double s[1] = {0.0};
+    for (int b = threadIdx.x; b < nb; b += blockDim.x) s[0] += partials[(size_t)blockIdx.x * nb + b];
+    block_reduce<1>(s, sm);
+    if (threadIdx.x == 0) jac[col[blockIdx.x]] = alpha[blockIdx.x] * s[0];
+}
+
+// generator -> product record (false when the product has no register form)
+bool lower_prod(const GateDesc &G, const std::vector<int> &loc, const int *rpos, int item, PProd &q,
+                std::vector<double2> &gcf) {
+    q = PProd{};
+    q.item = item;
+    q.coef = (int32_t)gcf.size();
+    auto d2 = [](const cd &z) { return make_double2(z.real(), z.imag()); };
+    switch (G.kind) {
+    case Kind::Diag: {
+        if (!G.cbits.empty() || G.k > 3) return false;
+        uint32_t pos[3] = {31, 31, 31};
+        for (int j = 0; j < G.k; ++j) pos[j] = (uint32_t)loc[G.tbits[j]];
+        q.kind = PG_DIAG;
+        q.p0 = pos[0];
+        q.p1 = pos[1];
+        q.p2 = pos[2];
+        for (int idx = 0; idx < 8; ++idx) {
+            int t = 0;
+            for (int j = 0; j < G.k; ++j) t = (t << 1) | ((idx >> (2 - j)) & 1);
+            gcf.push_back(d2(G.m[t]));
+        }
+        return true;
+    }
+    case Kind::Parity:
+        q.kind = PG_PARITY;
+        for (int b = 0; b < 64; ++b) {
+            if (!((G.pmask >> b) & 1)) continue;
+            if (b < (int)loc.size() && loc[b] >= 0) q.pm |= 1u << loc[b];
+            else q.pmg |= uint64_t(1) << b;
+        }
+        gcf.push_back(d2(G.pphase[0]));
+        gcf.push_back(d2(G.pphase[1]));
+        return true;
+    case Kind::Pair:
+        if (G.k != 1 || !rpos) return false;
+        q.kind = PG_PAIR1 + rpos[loc[G.tbits[0]]];
+        for (int i = 0; i < 4; ++i) gcf.push_back(d2(G.m2[i]));
+        return true;
+    default: return false;
+    }
+}
+
+// the product of an adjoint item has a register form: which register bit it needs (0: none), or -1
+int64_t prod_targets(const GateDesc &G, const std::vector<int> &loc) {
+    switch (G.kind) {
+    case Kind::Diag: return G.cbits.empty() && G.k <= 3 ? 0 : -1;
+    case Kind::Parity: return 0;
+    case Kind::Pair: return G.k == 1 ? (int64_t)(uint64_t(1) << loc[G.tbits[0]]) : -1;
+    default: return -1;
+    }
+}
+
+template <typename R>
+void run_fused_adjoint(void *lam, void *bra, uint32_t nq, const std::vector<AdjItem> &items,
+                       const std::function<void(size_t)> &exec_single, double *d_jac, cudaStream_t st) {
+    using G = GeoA<R>;
+    constexpr int kt = G::kt, a = G::a;
+    if ((int)nq < kt) throw Unsupported("state narrower than the adjoint tile");
+    const uint64_t low = (uint64_t(1) << G::reserve) - 1;
+    const size_t n = items.size();
+    // which items have a register form (checked with the tile-local map of a full tile)
+    std::vector<int> ident(nq);
+    for (uint32_t x = 0; x < nq; ++x) ident[x] = (int)x;
+    auto fusable = [&](const AdjItem &it) {
+        uint64_t b = 0;
+        if (it.adj.kind == Kind::Noop) return false;
+        if (!tile_bits(it.adj, b)) return false;
+        const int64_t rt = reg_targets<R>(it.adj, ident);
+        if (rt < 0) return false;
+        int64_t pt = 0;
+        if (it.diff && (pt = prod_targets(it.G, ident)) < 0) return false;
+        // the step's targets (and its product's) must fit one phase's register bits
+        return __builtin_popcountll((uint64_t)rt | (uint64_t)pt) <= a;
+    };
+    struct Piece {
+        bool seg;
+        size_t first;              // single item
+        std::vector<size_t> take;  // segment items
+    };
+    std::vector<Piece> pieces;
+    std::vector<char> done(n, 0);
+    size_t first = 0;
+    while (true) {
+        while (first < n && done[first]) ++first;
+        if (first >= n) break;
+        if (!fusable(items[first])) {
+            pieces.push_back(Piece{false, first, {}});
+            done[first] = 1;
+            continue;
+        }
+        uint64_t used = 0, blocked_any = 0, blocked_nondiag = 0;
+        int ncf = 0, nitems = 0;
+        std::vector<size_t> take;
+        for (size_t j = first; j < n; ++j) {
+            if (done[j]) continue;
+            const AdjItem &it = items[j];
+            const uint64_t db = dep_bits(it.adj) | (it.diff ? dep_bits(it.G) : 0);
+            const bool diagonal = is_diagonal(it.adj);
+            const bool blocked = (db & blocked_nondiag) || (!diagonal && (db & blocked_any));
+            uint64_t b = 0;
+            bool fits = !blocked && fusable(it) && tile_bits(it.adj, b);
+            if (fits) {
+                b |= it.diff ? dep_bits(it.G) : 0;
+                fits = __builtin_popcountll(used | b | low) <= kt && (int)take.size() + 1 <= kMaxAdjItems &&
+                       ncf + coef_count(it.adj) <= kMaxAdjCoefs && nitems + (it.diff ? 1 : 0) <= kMaxAdjItems;
+            }
+            if (fits) {
+                used |= b;
+                ncf += coef_count(it.adj);
+                nitems += it.diff ? 1 : 0;
+                take.push_back(j);
+            } else {
+                blocked_any |= db;
+                if (!diagonal) blocked_nondiag |= db;
+            }
+        }
+        for (size_t j : take) done[j] = 1;
+        pieces.push_back(Piece{true, 0, take});
+    }
+    // lower every segment (records per segment, launched in order with the singles between)
+    struct SegRec {
+        std::vector<uint8_t> lbits, gbits;
+        SegCode<R> sc;
+        std::vector<PProd> prods;
+        std::vector<double2> gcf;
+        std::vector<double> alpha;
+        std::vector<int64_t> col;
+    };
+    std::vector<SegRec> recs;
+    for (const Piece &pc : pieces) {
+        if (!pc.seg) continue;
+        SegRec r;
+        uint64_t used = 0;
+        for (size_t j : pc.take) {
+            uint64_t b = 0;
+            tile_bits(items[j].adj, b);
+            used |= b | (items[j].diff ? dep_bits(items[j].G) : 0);
+        }
+        std::vector<int> loc(nq, -1);
+        uint64_t inl = used | low;
+        for (uint32_t x = 0; x < nq && __builtin_popcountll(inl) < kt; ++x) inl |= uint64_t(1) << x;
+        for (uint32_t x = 0; x < nq; ++x) {
+            if ((inl >> x) & 1) {
+                loc[x] = (int)r.lbits.size();
+                r.lbits.push_back((uint8_t)x);
+            } else {
+                r.gbits.push_back((uint8_t)x);
+            }
+        }
+        // phases over the items in sweep order (no reordering inside a segment: products must
+        // see exactly the steps before them)
+        std::vector<const GateDesc *> cur;
+        std::vector<size_t> cur_items;
+        uint32_t rmask = 0;
+        auto close = [&]() {
+            if (cur.empty()) return;
+            RopHook hook = [&](size_t i, ROp &rop, const int *rpos) {
+                const AdjItem &it = items[cur_items[i]];
+                if (!it.diff) return;
+                PProd q;
+                const int item = (int)r.alpha.size();
+                if (!lower_prod(it.G, loc, rpos, item, q, r.gcf)) throw Unsupported("adjoint product form");
+                rop.prod = (int32_t)r.prods.size();
+                r.prods.push_back(q);
+                r.alpha.push_back(it.alpha);
+                r.col.push_back(it.col);
+            };
+            lower_phase<R, G>(r.sc, rmask, cur, loc, hook);
+            cur.clear();
+            cur_items.clear();
+            rmask = 0;
+        };
+        for (size_t j : pc.take) {
+            const AdjItem &it = items[j];
+            uint32_t need = (uint32_t)reg_targets<R>(it.adj, loc);
+            if (it.diff) need |= (uint32_t)prod_targets(it.G, loc);
+            if (__builtin_popcount(rmask | need) > a) close();
+            rmask |= need;
+            cur.push_back(&it.adj);
+            cur_items.push_back(j);
+        }
+        close();
+        recs.push_back(std::move(r));
+    }
+    // device copies and launches
+    const size_t tile_bytes = sizeof(C<R>) << kt;
+    const uint64_t ntiles = uint64_t(1) << (nq - kt);
+    const unsigned grid = (unsigned)std::min<uint64_t>(ntiles, (uint64_t)sm_count());
+    size_t max_items = 1;
+    for (auto &r : recs) max_items = std::max(max_items, r.alpha.size());
+    double *d_partials = nullptr;
+    B200SV_CUDA(cudaMallocAsync((void **)&d_partials, max_items * grid * sizeof(double), st));
+    std::vector<void *> frees{d_partials};
+    struct Free {
+        std::vector<void *> &p;
+        cudaStream_t s;
+        ~Free() {
+            for (void *x : p) cudaFreeAsync(x, s);
+        }
+    } fr{frees, st};
+    size_t si = 0;
+    for (const Piece &pc : pieces) {
+        if (!pc.seg) {
+            exec_single(pc.first);
+            continue;
+        }
+        SegRec &r = recs[si++];
+        const size_t bph = r.sc.phases.size() * sizeof(RPhase), brop = r.sc.rops.size() * sizeof(ROp),
+                     bpr = r.prods.size() * sizeof(PProd), bg = r.gcf.size() * sizeof(double2),
+                     bcf = r.sc.coefs.size() * sizeof(C<R>), bal = r.alpha.size() * sizeof(double),
+                     bco = r.col.size() * sizeof(int64_t);
+        std::vector<unsigned char> blob(bph + brop + bpr + bg + bcf + bal + bco + 64);
+        size_t off = 0;
+        auto put = [&](const void *src, size_t bytes) {
+            const size_t o = off;
+            if (bytes) std::memcpy(blob.data() + off, src, bytes);
+            off += (bytes + 15) & ~size_t(15);
+            return o;
+        };
+        const size_t o_ph = put(r.sc.phases.data(), bph), o_rop = put(r.sc.rops.data(), brop),
+                     o_pr = put(r.prods.data(), bpr), o_g = put(r.gcf.data(), bg), o_cf = put(r.sc.coefs.data(), bcf),
+                     o_al = put(r.alpha.data(), bal), o_co = put(r.col.data(), bco);
+        unsigned char *d_blob = nullptr;
+        B200SV_CUDA(cudaMallocAsync((void **)&d_blob, std::max<size_t>(off, 16), st));
+        frees.push_back(d_blob);
+        B200SV_CUDA(cudaMemcpyAsync(d_blob, blob.data(), off, cudaMemcpyHostToDevice, st));
+        AdjSegArgs A{};
+        A.phases = reinterpret_cast<const RPhase *>(d_blob + o_ph);
+        A.rops = reinterpret_cast<const ROp *>(d_blob + o_rop);
+        A.prods = reinterpret_cast<const PProd *>(d_blob + o_pr);
+        A.gcoefs = reinterpret_cast<const double2 *>(d_blob + o_g);
+        A.coefs = d_blob + o_cf;
+        A.nph = (int)r.sc.phases.size();
+        A.nrop = (int)r.sc.rops.size();
+        A.nprod = (int)r.prods.size();
+        A.ngcoef = (int)r.gcf.size();
+        A.ncoef = (int)r.sc.coefs.size();
+        A.nitems = (int)r.alpha.size();
+        A.ng = (int)r.gbits.size();
+        std::memcpy(A.lbits, r.lbits.data(), r.lbits.size());
+        std::memcpy(A.gbits, r.gbits.data(), r.gbits.size());
+        const size_t smem = 4 * tile_bytes + bph + brop + bpr + bg + (size_t)A.nitems * kWarps * sizeof(double) + bcf;
+        if (smem > 227 * 1024) throw Unsupported("fused adjoint segment exceeds shared memory");
+        B200SV_CUDA(cudaFuncSetAttribute(k_fused_adj<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        k_fused_adj<R><<<grid, kFThreads, smem, st>>>(static_cast<C<R> *>(lam), static_cast<C<R> *>(bra), A, ntiles,
+                                                      d_partials);
+        B200SV_CUDA(cudaGetLastError());
+        if (A.nitems) {
+            k_adj_fused_final<<<A.nitems, 128, 0, st>>>(d_partials, (int)grid,
+                                                         reinterpret_cast<const double *>(d_blob + o_al),
+                                                         reinterpret_cast<const int64_t *>(d_blob + o_co), d_jac);
+            B200SV_CUDA(cudaGetLastError());
+        }
+    }
+}
+
 }  // namespace
 
 int fused_tile_bits(int dtype, uint32_t nq) {
@@ -1066,6 +1561,17 @@ void apply_fused(void *state, uint32_t nq, int dtype, const std::vector<GateDesc
     if (nq > 48 + 16) throw Unsupported("state too wide for the fused path");
     if (dtype == B200SV_C64) run_fused<float>(state, nq, descs, apply_single, st);
     else run_fused<double>(state, nq, descs, apply_single, st);
+}
+
+bool fused_adjoint_worthwhile(int dtype, uint32_t nq) {
+    return nq >= (uint32_t)(dtype == B200SV_C64 ? GeoA<float>::kt : GeoA<double>::kt);
+}
+
+void apply_fused_adjoint(void *lambda, void *bra, uint32_t nq, int dtype, const std::vector<AdjItem> &items,
+                         const std::function<void(size_t)> &exec_single, double *d_jac, cudaStream_t st) {
+    if (nq > 48 + 16) throw Unsupported("state too wide for the fused path");
+    if (dtype == B200SV_C64) run_fused_adjoint<float>(lambda, bra, nq, items, exec_single, d_jac, st);
+    else run_fused_adjoint<double>(lambda, bra, nq, items, exec_single, d_jac, st);
 }
 
 }  // namespace b200sv

@@ -123,6 +123,20 @@ void sample_mcmc(const void *state, uint32_t nq, int dtype, int proposal, uint64
 // state; other gates go through apply_single, in order.
 int fused_tile_bits(int dtype, uint32_t nq);
 bool fused_worthwhile(int dtype, uint32_t nq);
+// One step of the adjoint reverse sweep: the inverse of an op and, when the op is
+// differentiated, its generator G with alpha = -2 * scale, and the Jacobian column.
+struct AdjItem {
+    GateDesc adj;
+    bool diff = false;
+    GateDesc G;
+    double alpha = 0.0;
+    int64_t col = -1;
+};
+// The sweep over lambda and one bra in fused passes; items without a register form run
+// through exec_single(i) in order.  Products land in d_jac[col].
+bool fused_adjoint_worthwhile(int dtype, uint32_t nq);
+void apply_fused_adjoint(void *lambda, void *bra, uint32_t nq, int dtype, const std::vector<AdjItem> &items,
+                         const std::function<void(size_t)> &exec_single, double *d_jac, cudaStream_t st);
 void apply_fused(void *state, uint32_t nq, int dtype, const std::vector<GateDesc> &descs,
                  const std::function<void(const GateDesc &)> &apply_single, cudaStream_t st);
 // Marginal probabilities over `bits` (bits[0] = MSB of the output index).

@@ -210,3 +210,53 @@ def test_vjp_state(capi, dtype):
         [np.zeros(0, dtype=dtype) for _ in ops])
     res = getattr(ours.algorithms, "VectorJacobianProduct" + sfx)()(svo, opsd, dy.astype(dtype), tp)
     assert np.abs(np.asarray(res) - want).max() < tol * 10
+
+
+@pytest.mark.parametrize("dtype", [np.complex128, np.complex64])
+def test_adjoint_fused_sweep_every_generator(capi, dtype):
+    """A 13-qubit state takes the fused reverse sweep (one observable: a Hamiltonian, the VJP
+    form).  Every differentiable gate kind, constant gates and matrices on 1..4 wires, a trainable
+    subset with gaps and an early exit; against the oracle's AdjointJacobianLQubit restatement,
+    and against the unfused sweep of the same engine (two observables)."""
+    import lq_oracle as O
+    from lightning_b200.workloads import random_unitary
+    rng = np.random.default_rng(1313)
+    n = 13
+    diff_gates = {"RX": 1, "RY": 1, "RZ": 1, "PhaseShift": 1, "CRX": 2, "CRY": 2, "CRZ": 2,
+                  "ControlledPhaseShift": 2, "IsingXX": 2, "IsingYY": 2, "IsingZZ": 2, "IsingXY": 2,
+                  "SingleExcitation": 2, "SingleExcitationMinus": 2, "SingleExcitationPlus": 2,
+                  "DoubleExcitation": 4, "DoubleExcitationMinus": 4, "DoubleExcitationPlus": 4, "MultiRZ": 3}
+    names = list(diff_gates)
+    ops = [("Hadamard", [q], False, []) for q in range(n)]
+    for _ in range(140):
+        r = rng.random()
+        if r < 0.65:
+            name = names[int(rng.integers(len(names)))]
+            k = diff_gates[name]
+            ops.append((name, [int(w) for w in rng.choice(n, k, replace=False)], bool(rng.random() < 0.3),
+                        [float(rng.uniform(0, 2 * np.pi))]))
+        elif r < 0.8:
+            name = ["CNOT", "CZ", "SWAP", "Toffoli"][int(rng.integers(4))]
+            ops.append((name, [int(w) for w in rng.choice(n, 3 if name == "Toffoli" else 2, replace=False)],
+                        False, []))
+        elif r < 0.9:
+            k = int(rng.integers(1, 5))
+            ops.append(("QubitUnitary", [int(w) for w in rng.choice(n, k, replace=False)], False, [],
+                        random_unitary(rng, k)))
+        else:
+            ops.append((["S", "T", "PauliY", "Hadamard"][int(rng.integers(4))], [int(rng.integers(n))], False, []))
+    npar = sum(1 for op in ops if op[3])
+    tp = sorted(int(x) for x in rng.choice(npar - 10, (npar - 10) // 2, replace=False))  # gaps, early exit
+    ham = [[(0.7, [("PauliZ", [0]), ("PauliZ", [5])]), (-1.2, [("PauliX", [12])]), (0.4, [("PauliY", [3])])]]
+    st = O.run_circuit(n, ops)
+    want = O.adjoint_jacobian(st, ops, ham, tp)
+    sv = capi.StateVector(n, dtype)
+    sv.upload(st.astype(dtype))
+    got = sv.adjoint_jacobian(ops, ham, tp)
+    tol = 1e-12 if dtype == np.complex128 else 1e-5
+    assert np.abs(got - want).max() < tol
+    # unfused sweep of the same engine: two observables
+    got2 = sv.adjoint_jacobian(ops, ham + [[(1.0, [("PauliZ", [7])])]], tp)
+    assert np.abs(got2[0] - got[0]).max() < tol
+    want2 = O.adjoint_jacobian(st, ops, [[(1.0, [("PauliZ", [7])])]], tp)
+    assert np.abs(got2[1] - want2[0]).max() < tol
