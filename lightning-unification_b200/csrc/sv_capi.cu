@@ -273,10 +273,12 @@ void apply_observable(b200sv_state *h, const ObsRec &o, const void *psi, void *o
 
 // per-term Pauli values of an all-Pauli observable (host vector, term order).  Words sorted by
 // X mask.  Diagonal words (two or more, 12+ qubits) share Walsh-Hadamard passes of
-// reduce_pauli_diag, up to 256 per pass.  Words whose X mask stays below 4 MiB of amplitudes
-// share passes of reduce_pauli_multi, up to 32 per pass, their partner amplitudes coming from
-// L2; each wider X mask gets pair passes of reduce_pauli_group, where a thread reads both
-// amplitudes of a pair, so the state crosses HBM once per pass either way.
+// reduce_pauli_diag, up to 256 per pass.  The other words are packed, first fit in X-mask
+// order, into tiles (pauli_tile_bits): a tile holding two or more distinct X masks is one
+// tiled pass of reduce_pauli_tiled (up to 32 words).  The rest: words whose X mask stays below
+// 4 MiB of amplitudes share passes of reduce_pauli_multi, up to 32 per pass, their partner
+// amplitudes coming from L2; each wider X mask gets pair passes of reduce_pauli_group, where a
+// thread reads both amplitudes of a pair.  The state crosses HBM once per pass in every kind.
 std::vector<double> pauli_term_values(b200sv_state *h, const void *psi, const std::vector<PauliWord> &words) {
     const cudaStream_t st = h->stream();
     std::vector<double> vals(words.size(), 0.0);
@@ -284,41 +286,96 @@ std::vector<double> pauli_term_values(b200sv_state *h, const void *psi, const st
     for (size_t i = 0; i < order.size(); ++i) order[i] = i;
     std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) { return words[a].xmask < words[b].xmask; });
     const uint64_t near = (uint64_t(4) << 20) / h->amp_bytes();  // partner distance kept in L2
+    enum Kind { DIAG, MULTI, PAIR, TILED };
     struct Pass {
-        size_t begin, count;
-        bool multi;
-        bool diag = false;
+        size_t begin, count;  // into seq
+        Kind kind;
     };
+    std::vector<size_t> seq;  // word indices, each pass's words contiguous
+    seq.reserve(words.size());
     std::vector<Pass> passes;
     size_t i = 0;
     // diagonal words (sorted first): Walsh-Hadamard passes, any number of words per read
     size_t ndiag = 0;
     while (ndiag < order.size() && words[order[ndiag]].xmask == 0) ++ndiag;
-    const bool diag_pass = h->nq >= 12 && ndiag >= 2;
-    if (diag_pass) {
-        for (size_t d = 0; d < ndiag; d += 256) passes.push_back(Pass{d, std::min<size_t>(256, ndiag - d), true, true});
+    if (h->nq >= 12 && ndiag >= 2) {
+        for (size_t d = 0; d < ndiag; d += 256) {
+            passes.push_back(Pass{seq.size(), std::min<size_t>(256, ndiag - d), DIAG});
+            for (size_t q = d; q < d + passes.back().count; ++q) seq.push_back(order[q]);
+        }
         i = ndiag;
     }
-    while (i < order.size() && words[order[i]].xmask < near) {
+    // tiles: first fit of the distinct X masks (chunks of <= 32 words) in ascending order
+    struct Tile {
+        uint64_t xunion;
+        int nmasks;
+        std::vector<size_t> w;  // positions in order
+    };
+    std::vector<Tile> tiles;
+    std::vector<size_t> rest;  // positions in order left to the multi and pair passes
+    for (size_t r = i; r < order.size();) {
+        const uint64_t m = words[order[r]].xmask;
+        size_t e = r;
+        while (e < order.size() && words[order[e]].xmask == m) ++e;
+        for (size_t c = r; c < e; c += 32) {
+            const size_t n = std::min<size_t>(32, e - c);
+            Tile *t = nullptr;
+            if (m != 0 && pauli_tile_bits(m, h->nq, h->amp_bytes())) {
+                for (auto &tl : tiles)
+                    if (tl.w.size() + n <= 32 && pauli_tile_bits(tl.xunion | m, h->nq, h->amp_bytes())) {
+                        t = &tl;
+                        break;
+                    }
+                if (!t) {
+                    tiles.push_back(Tile{0, 0, {}});
+                    t = &tiles.back();
+                }
+            }
+            if (!t) {
+                for (size_t q = c; q < c + n; ++q) rest.push_back(q);
+                continue;
+            }
+            const bool fresh = t->w.empty() || words[order[t->w.back()]].xmask != m;
+            t->xunion |= m;
+            t->nmasks += fresh;
+            for (size_t q = c; q < c + n; ++q) t->w.push_back(q);
+        }
+        r = e;
+    }
+    for (auto &tl : tiles) {
+        if (tl.nmasks < 2) {
+            rest.insert(rest.end(), tl.w.begin(), tl.w.end());
+            continue;
+        }
+        passes.push_back(Pass{seq.size(), tl.w.size(), TILED});
+        for (size_t q : tl.w) seq.push_back(order[q]);
+    }
+    std::sort(rest.begin(), rest.end());  // X-mask order
+    size_t k = 0;
+    while (k < rest.size() && words[order[rest[k]]].xmask < near) {
         // up to 32 words and 8 distinct X masks per pass: each mask adds a partner read per
         // amplitude, so wider passes cost as much as pair passes
         size_t c = 0;
         int masks = 0;
-        while (i + c < order.size() && c < 32 && words[order[i + c]].xmask < near) {
-            const bool fresh = c == 0 || words[order[i + c]].xmask != words[order[i + c - 1]].xmask;
-            if (fresh && words[order[i + c]].xmask != 0 && masks == 8) break;
-            if (fresh && words[order[i + c]].xmask != 0) ++masks;
+        while (k + c < rest.size() && c < 32 && words[order[rest[k + c]]].xmask < near) {
+            const uint64_t m = words[order[rest[k + c]]].xmask;
+            const bool fresh = c == 0 || m != words[order[rest[k + c - 1]]].xmask;
+            if (fresh && m != 0 && masks == 8) break;
+            if (fresh && m != 0) ++masks;
             ++c;
         }
-        passes.push_back(Pass{i, c, true});
-        i += c;
+        passes.push_back(Pass{seq.size(), c, MULTI});
+        for (size_t q = k; q < k + c; ++q) seq.push_back(order[rest[q]]);
+        k += c;
     }
-    while (i < order.size()) {
+    while (k < rest.size()) {
         size_t c = 1;
-        while (i + c < order.size() && c < 32 && words[order[i + c]].xmask == words[order[i]].xmask) ++c;
-        passes.push_back(Pass{i, c, false});
-        i += c;
+        while (k + c < rest.size() && c < 32 && words[order[rest[k + c]]].xmask == words[order[rest[k]]].xmask) ++c;
+        passes.push_back(Pass{seq.size(), c, PAIR});
+        for (size_t q = k; q < k + c; ++q) seq.push_back(order[rest[q]]);
+        k += c;
     }
+    const bool c64 = h->dtype == B200SV_C64;
     size_t pi = 0;
     while (pi < passes.size()) {
         size_t batch = 0;
@@ -326,37 +383,39 @@ std::vector<double> pauli_term_values(b200sv_state *h, const void *psi, const st
         while (pi < passes.size() && batch + passes[pi].count <= kSmall) {
             const Pass &ps = passes[pi];
             std::vector<PauliWord> grp;
-            for (size_t q = 0; q < ps.count; ++q) grp.push_back(words[order[ps.begin + q]]);
+            for (size_t q = 0; q < ps.count; ++q) grp.push_back(words[seq[ps.begin + q]]);
             const int cnt = (int)ps.count;
-            if (ps.diag) {
+            double *out = h->d_small + batch;
+            switch (ps.kind) {
+            case DIAG: {
                 // the Z masks ride at the end of the partials buffer, past what the pass uses
                 std::vector<uint64_t> zm(ps.count);
                 for (size_t q = 0; q < ps.count; ++q) zm[q] = grp[q].zmask;
                 uint64_t *dz = reinterpret_cast<uint64_t *>(h->d_partials + kPartialsCapacity - 256);
                 B200SV_CUDA(cudaMemcpyAsync(dz, zm.data(), zm.size() * sizeof(uint64_t), cudaMemcpyHostToDevice, st));
-                if (h->dtype == B200SV_C64)
-                    reduce_pauli_diag<float>(psi, h->nq, dz, cnt, h->d_partials, kPartialsCapacity - 256,
-                                             h->d_small + batch, st);
-                else
-                    reduce_pauli_diag<double>(psi, h->nq, dz, cnt, h->d_partials, kPartialsCapacity - 256,
-                                              h->d_small + batch, st);
-                batch += ps.count;
-                ++pi;
-                continue;
+                if (c64) reduce_pauli_diag<float>(psi, h->nq, dz, cnt, h->d_partials, kPartialsCapacity - 256, out, st);
+                else reduce_pauli_diag<double>(psi, h->nq, dz, cnt, h->d_partials, kPartialsCapacity - 256, out, st);
+                break;
             }
-            if (h->dtype == B200SV_C64) {
-                if (ps.multi) reduce_pauli_multi<float>(psi, h->nq, grp.data(), cnt, h->d_partials, h->d_small + batch, st);
-                else reduce_pauli_group<float>(psi, h->nq, grp.data(), cnt, h->d_partials, h->d_small + batch, st);
-            } else {
-                if (ps.multi) reduce_pauli_multi<double>(psi, h->nq, grp.data(), cnt, h->d_partials, h->d_small + batch, st);
-                else reduce_pauli_group<double>(psi, h->nq, grp.data(), cnt, h->d_partials, h->d_small + batch, st);
+            case TILED:
+                if (c64) reduce_pauli_tiled<float>(psi, h->nq, grp.data(), cnt, h->d_partials, out, st);
+                else reduce_pauli_tiled<double>(psi, h->nq, grp.data(), cnt, h->d_partials, out, st);
+                break;
+            case MULTI:
+                if (c64) reduce_pauli_multi<float>(psi, h->nq, grp.data(), cnt, h->d_partials, out, st);
+                else reduce_pauli_multi<double>(psi, h->nq, grp.data(), cnt, h->d_partials, out, st);
+                break;
+            case PAIR:
+                if (c64) reduce_pauli_group<float>(psi, h->nq, grp.data(), cnt, h->d_partials, out, st);
+                else reduce_pauli_group<double>(psi, h->nq, grp.data(), cnt, h->d_partials, out, st);
+                break;
             }
             batch += ps.count;
             ++pi;
         }
         B200SV_CUDA(cudaMemcpyAsync(h->h_small, h->d_small, batch * sizeof(double), cudaMemcpyDeviceToHost, st));
         B200SV_CUDA(cudaStreamSynchronize(st));
-        for (size_t q = 0; q < batch; ++q) vals[order[first + q]] = h->h_small[q];
+        for (size_t q = 0; q < batch; ++q) vals[seq[first + q]] = h->h_small[q];
     }
     return vals;
 }

@@ -84,6 +84,15 @@ void reduce_pauli_diag(const void *psi, uint32_t nq, const uint64_t *zmask_dev, 
 template <typename R>
 void reduce_pauli_multi(const void *psi, uint32_t nq, const PauliWord *terms, int nterms,
                         double *partials, double *out_dev, cudaStream_t st);
+// tile bits (state positions) of a tiled Pauli pass over words whose X masks OR to xunion:
+// those bits, the lowest 3 (complex128) or 4 (complex64) state bits, then the lowest others up
+// to 12 bits; 0 when they do not fit
+uint64_t pauli_tile_bits(uint64_t xunion, uint32_t nq, size_t amp_bytes);
+// words with X factors, sorted by X mask, whose X masks fit one tile (pauli_tile_bits): one
+// read of the state for the group (<= 32 words)
+template <typename R>
+void reduce_pauli_tiled(const void *psi, uint32_t nq, const PauliWord *terms, int nterms, double *partials,
+                        double *out, cudaStream_t st);
 // out_dev[0] = Re <psi| M |psi> for a dense Hermitian M on k <= 4 bits (matrix on device).
 template <typename R>
 void reduce_dense_expval(const void *psi, uint32_t nq, const GateDesc &g, void *dev_matrix,

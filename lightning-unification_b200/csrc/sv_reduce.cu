@@ -622,6 +622,266 @@ void reduce_pauli_group(const void *psi, uint32_t nq, const PauliWord *terms, in
     finalize(partials, nb, nterms + (with_norm ? 1 : 0), out, 1, 1.0, st);
 }
 
+// ---- Pauli words with wide X masks, one pass over tiles -------------------------------------
+// A word whose X mask reaches beyond the shared passes' partner distance costs one read of
+// the state as a pair pass.  A group of words whose X bits, together with the lowest state
+// bits, fit in 12 tile bits is evaluated per tile instead: a tile is the 4096 amplitudes that
+// share the values of the other bits, staged in shared memory, so the group reads the state
+// once.  Tile element r = t + 256 j is thread t's register j.
+//
+// For P = i^ny X^x Z^z the expectation value is sum_k Re(conj(psi_(k^x)) i^ny (-1)^(k.z) psi_k),
+// and because P is Hermitian the terms of k and k^x have equal real parts, so either member
+// of a pair may stand for it (counted twice).  A thread takes its register element as k and
+// reads the partner from shared memory, for one member of each pair:
+//  * x reaches a register bit (tile bits 8..11): the registers j whose copy of the highest such
+//    bit is 0 — the same 8 registers in every thread;
+//  * x lies in the thread bits only: registers j with (j & 1) equal to the thread's bit under
+//    the highest bit of x — a pair's two owners differ in that bit, so each pair is taken once,
+//    and every thread takes 8.
+// Words sharing an X mask form runs of up to 4 that share the partner read and the products.
+constexpr int kPTileBits = 12;
+constexpr int kPTileThreads = 256;
+constexpr int kPTileMaxWords = 32;
+constexpr int kPTileLowBits[2] = {4, 3};  // state bits always in the tile: 128-byte runs (c64, c128)
+struct PauliTiledP {
+    uint64_t ntiles;
+    int nterms, ng, nruns;
+    uint8_t lbits[kPTileBits];          // state position of tile bit b (ascending)
+    uint8_t gbits[52];                  // state positions of the other bits (ascending)
+    uint8_t run_begin[kPTileMaxWords + 1];
+    uint32_t xl[kPTileMaxWords];        // tile-local X mask of each run
+    uint32_t zl[kPTileMaxWords];        // tile-local Z mask of each word
+    uint64_t zg[kPTileMaxWords];        // Z mask outside the tile (state positions) of each word
+    uint8_t ny[kPTileMaxWords];         // number of Y factors mod 4 of each word
+    uint8_t run_kinds[kPTileMaxWords];  // bit 0: a word of the run has even ny, bit 1: odd
+};
+// parity of bit b of the register index j, as a 16-bit table over j
+__constant__ const uint32_t kRegParity[4] = {0xAAAAu, 0xCCCCu, 0xF0F0u, 0xFF00u};
+__device__ __forceinline__ uint64_t deposit_bits_u8(uint64_t x, const uint8_t *pos, int nbits) {
+    uint64_t r = 0;
+    for (int i = 0; i < nbits; ++i) r |= ((x >> i) & 1u) << pos[i];
+    return r;
+}
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+// Per word, packed once per block: bits 0-7 the Z mask on the thread bits, 8-23 the parity of
+// (j & Z) over the 16 registers j as a table, bit 24 the word takes Im (odd ny), bit 25 the
+// i^ny factor is negative (ny = 1, 2).  Per run: bits 0-11 the tile-local X mask, 12-17 the
+// first word, 18-20 the number of words, 21-22 which parts its words take (bit 0 Re, bit 1 Im).
+__device__ __forceinline__ uint32_t tiled_word_bits(uint32_t zl, int ny) {
+    uint32_t m = 0;
+#pragma unroll
+    for (int b = 0; b < 4; ++b)
+        if ((zl >> (8 + b)) & 1) m ^= kRegParity[b];
+    return (zl & 255u) | (m << 8) | ((uint32_t)(ny & 1) << 24) | ((uint32_t)(ny == 1 || ny == 2) << 25);
+}
+
+// One run of words over a tile.  NW words (1, 2 or 4; a run of 3 carries a fourth word whose
+// value is dropped), KIND which part of conj(partner) own they take (0: Re, 1: Im, 2: each word
+// its own), TB the highest register bit of the X mask (-1: the mask lies in the thread bits).
+// Every branch on these is resolved at compile time, so the inner step is a shared-memory
+// load, the product and one signed add per word.  The run's sums go, signed, into the warp's
+// accumulators.
+template <typename R, int NW, int KIND, int TB>
+__device__ __forceinline__ void tiled_run(const C<R> *tile, const C<R> (&v)[16], int tid, uint32_t xl, int w0, int nw,
+                                          const uint32_t *s_word, uint32_t tmask, double *s_acc_warp) {
+    uint32_t jpar[NW];
+    bool im[NW];
+    double sg[NW];
+#pragma unroll
+    for (int w = 0; w < NW; ++w) {
+        const int t = w0 + (w < nw ? w : nw - 1);
+        const uint32_t wb = s_word[t];
+        jpar[w] = (wb >> 8) & 0xffffu;
+        im[w] = (wb >> 24) & 1u;
+        const int odd = (__popc(tid & wb & 255u) + (tmask >> t) + (wb >> 25)) & 1;
+        sg[w] = odd ? -2.0 : 2.0;  // 2: each pair is taken once for both of its terms
+    }
+    double acc[2][NW];
+#pragma unroll
+    for (int w = 0; w < NW; ++w) acc[0][w] = acc[1][w] = 0.0;
+    auto step = [&](const double2 vi, const double2 vj, int jbit_pos, const uint32_t (&jp)[NW], int half) {
+        double zr = 0.0, zi = 0.0;
+        if (KIND != 1) zr = fma(vj.x, vi.x, vj.y * vi.y);
+        if (KIND != 0) zi = fma(vj.x, vi.y, -(vj.y * vi.x));
+#pragma unroll
+        for (int w = 0; w < NW; ++w) {
+            const double val = KIND == 0 ? zr : KIND == 1 ? zi : (im[w] ? zi : zr);
+            acc[half][w] += ((jp[w] >> jbit_pos) & 1u) ? -val : val;
+        }
+    };
+    if constexpr (TB >= 0) {
+        // registers j with bit TB clear; partner in register j ^ xj of thread tid ^ (xl & 255)
+        const C<R> *pb = tile + (tid ^ (xl & 255u));
+        const uint32_t xj = xl >> 8;
+        int k = 0;
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+            if (j & (1 << TB)) continue;
+            step(widen<R>(v[j]), widen<R>(pb[((uint32_t)j ^ xj) << 8]), j, jpar, (k++) & 1);
+        }
+    } else {
+        // registers j = 2m + hb (own element read back from shared memory); partner in the same
+        // register of thread tid ^ xl
+        const int hb = (tid >> (31 - __clz(xl))) & 1;
+        const C<R> *po = tile + tid + (hb << 8);
+        const C<R> *pb = tile + (tid ^ xl) + (hb << 8);
+        uint32_t jp[NW];
+#pragma unroll
+        for (int w = 0; w < NW; ++w) jp[w] = jpar[w] >> hb;
+#pragma unroll
+        for (int m = 0; m < 8; ++m) step(widen<R>(po[m << 9]), widen<R>(pb[m << 9]), 2 * m, jp, m & 1);
+    }
+    const int lane = tid & 31;
+#pragma unroll
+    for (int w = 0; w < NW; ++w) {
+        if (w >= nw) break;
+        const double s = warp_sum(sg[w] * (acc[0][w] + acc[1][w]));  // sg holds the thread's Z parity
+        if (lane == 0) s_acc_warp[w0 + w] += s;
+    }
+}
+template <typename R, int NW, int KIND>
+__device__ __forceinline__ void tiled_run_tb(int tb, const C<R> *tile, const C<R> (&v)[16], int tid, uint32_t xl,
+                                             int w0, int nw, const uint32_t *s_word, uint32_t tmask, double *acc) {
+    switch (tb) {
+    case 0: tiled_run<R, NW, KIND, 0>(tile, v, tid, xl, w0, nw, s_word, tmask, acc); break;
+    case 1: tiled_run<R, NW, KIND, 1>(tile, v, tid, xl, w0, nw, s_word, tmask, acc); break;
+    case 2: tiled_run<R, NW, KIND, 2>(tile, v, tid, xl, w0, nw, s_word, tmask, acc); break;
+    case 3: tiled_run<R, NW, KIND, 3>(tile, v, tid, xl, w0, nw, s_word, tmask, acc); break;
+    default: tiled_run<R, NW, KIND, -1>(tile, v, tid, xl, w0, nw, s_word, tmask, acc); break;
+    }
+}
+template <typename R>
+__global__ void __launch_bounds__(kPTileThreads, 2) k_pauli_tiled(const C<R> *__restrict__ a, PauliTiledP p,
+                                                                  double *partials) {
+    constexpr int PER = (1 << kPTileBits) / kPTileThreads;  // 16 registers a thread
+    extern __shared__ __align__(16) unsigned char pt_raw[];
+    C<R> *tile = reinterpret_cast<C<R> *>(pt_raw);
+    __shared__ uint8_t s_lbits[kPTileBits], s_gbits[52];
+    __shared__ uint64_t s_hi[PER];
+    __shared__ double s_acc[kPTileThreads / 32][kPTileMaxWords];
+    __shared__ uint32_t s_word[kPTileMaxWords], s_run[kPTileMaxWords];
+    __shared__ uint32_t s_tmask;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (tid < kPTileBits) s_lbits[tid] = p.lbits[tid];
+    if (tid < 52) s_gbits[tid] = p.gbits[tid];
+    if (tid < p.nterms) s_word[tid] = tiled_word_bits(p.zl[tid], p.ny[tid]);
+    if (tid < p.nruns)
+        s_run[tid] = p.xl[tid] | ((uint32_t)p.run_begin[tid] << 12) |
+                     ((uint32_t)(p.run_begin[tid + 1] - p.run_begin[tid]) << 18) | ((uint32_t)p.run_kinds[tid] << 21);
+    static_assert(kPTileThreads == (kPTileThreads / 32) * kPTileMaxWords, "one accumulator per thread");
+    (&s_acc[0][0])[tid] = 0.0;
+    __syncthreads();
+    if (tid < PER) s_hi[tid] = deposit_bits_u8((uint64_t)tid * kPTileThreads, s_lbits, kPTileBits);
+    __syncthreads();
+    const uint64_t lo = deposit_bits_u8(tid, s_lbits, 8);
+    const uint64_t zg = lane < p.nterms ? p.zg[lane] : 0;
+    for (uint64_t tt = blockIdx.x; tt < p.ntiles; tt += gridDim.x) {
+        const uint64_t tbase = deposit_bits_u8(tt, s_gbits, p.ng);
+        C<R> v[PER];
+#pragma unroll
+        for (int j = 0; j < PER; ++j) v[j] = a[tbase | lo | s_hi[j]];
+        __syncthreads();  // the previous tile has been read
+#pragma unroll
+        for (int j = 0; j < PER; ++j) tile[tid + j * kPTileThreads] = v[j];
+        if (warp == 0) {  // parity of each word's Z factors outside the tile, one bit per word
+            const uint32_t m = __ballot_sync(0xffffffffu, __popcll(tbase & zg) & 1);
+            if (lane == 0) s_tmask = m;
+        }
+        __syncthreads();
+        const uint32_t tmask = s_tmask;
+        for (int run = 0; run < p.nruns; ++run) {
+            const uint32_t rd = s_run[run];
+            const uint32_t xl = rd & 0xfffu;
+            const int w0 = (rd >> 12) & 63, nw = (rd >> 18) & 7, kinds = (rd >> 21) & 3;
+            const uint32_t xj = xl >> 8;
+            const int tb = xj ? 31 - __clz(xj) : -1;
+            double *acc = s_acc[warp];
+            if (nw == 1) {
+                if (kinds == 2) tiled_run_tb<R, 1, 1>(tb, tile, v, tid, xl, w0, nw, s_word, tmask, acc);
+                else tiled_run_tb<R, 1, 0>(tb, tile, v, tid, xl, w0, nw, s_word, tmask, acc);
+            } else if (nw == 2) {
+                tiled_run_tb<R, 2, 2>(tb, tile, v, tid, xl, w0, nw, s_word, tmask, acc);
+            } else {
+                tiled_run_tb<R, 4, 2>(tb, tile, v, tid, xl, w0, nw, s_word, tmask, acc);
+            }
+        }
+    }
+    __syncthreads();
+    if (tid < p.nterms) {
+        double s = 0.0;
+#pragma unroll
+        for (int w = 0; w < kPTileThreads / 32; ++w) s += s_acc[w][tid];
+        partials[(size_t)tid * gridDim.x + blockIdx.x] = s;
+    }
+}
+
+uint64_t pauli_tile_bits(uint64_t xunion, uint32_t nq, size_t amp_bytes) {
+    const int low = kPTileLowBits[amp_bytes == 16 ? 1 : 0];
+    uint64_t in = xunion | ((uint64_t(1) << std::min<uint32_t>(low, nq)) - 1);
+    if (nq < (uint32_t)kPTileBits || __builtin_popcountll(in) > kPTileBits) return 0;
+    for (uint32_t b = 0; b < nq && __builtin_popcountll(in) < kPTileBits; ++b) in |= uint64_t(1) << b;
+    return in;
+}
+
+template <typename R>
+void reduce_pauli_tiled(const void *psi, uint32_t nq, const PauliWord *terms, int nterms, double *partials,
+                        double *out, cudaStream_t st) {
+    if (nterms <= 0) return;
+    if (nterms > kPTileMaxWords) throw ArgError("at most 32 Pauli words per tiled pass");
+    uint64_t xu = 0;
+    for (int t = 0; t < nterms; ++t) {
+        if (!terms[t].xmask) throw ArgError("tiled Pauli pass takes words with X factors");
+        if (t && terms[t].xmask < terms[t - 1].xmask) throw ArgError("tiled Pauli pass takes words sorted by X mask");
+        xu |= terms[t].xmask;
+    }
+    const uint64_t in = pauli_tile_bits(xu, nq, sizeof(C<R>));
+    if (!in) throw ArgError("Pauli X masks do not fit one tile");
+    PauliTiledP p{};
+    int loc[64];
+    int nl = 0, ng = 0;
+    for (uint32_t b = 0; b < nq; ++b) {
+        loc[b] = -1;
+        if ((in >> b) & 1) {
+            loc[b] = nl;
+            p.lbits[nl++] = (uint8_t)b;
+        } else {
+            p.gbits[ng++] = (uint8_t)b;
+        }
+    }
+    p.ng = ng;
+    p.ntiles = uint64_t(1) << (nq - kPTileBits);
+    p.nterms = nterms;
+    auto local = [&](uint64_t m) {
+        uint32_t r = 0;
+        for (uint32_t b = 0; b < nq; ++b)
+            if (((m >> b) & 1) && loc[b] >= 0) r |= 1u << loc[b];
+        return r;
+    };
+    int nr = 0;
+    for (int t = 0; t < nterms; ++t) {
+        if (t == 0 || terms[t].xmask != terms[t - 1].xmask || t - p.run_begin[nr - 1] == 4) {
+            p.run_begin[nr] = (uint8_t)t;
+            p.xl[nr++] = local(terms[t].xmask);
+        }
+        p.zl[t] = local(terms[t].zmask);
+        p.zg[t] = terms[t].zmask & ~in;
+        p.ny[t] = (uint8_t)(terms[t].ny & 3);
+        p.run_kinds[nr - 1] |= (p.ny[t] & 1) ? 2 : 1;
+    }
+    p.run_begin[nr] = (uint8_t)nterms;
+    p.nruns = nr;
+    const size_t smem = sizeof(C<R>) << kPTileBits;
+    const uint64_t nb = std::min<uint64_t>(p.ntiles, std::min<uint64_t>((uint64_t)sm_count() * 2, kMaxRedBlocks));
+    B200SV_CUDA(cudaFuncSetAttribute(k_pauli_tiled<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_pauli_tiled<R><<<(unsigned)nb, kPTileThreads, smem, st>>>(static_cast<const C<R> *>(psi), p, partials);
+    B200SV_CUDA(cudaGetLastError());
+    finalize(partials, (int)nb, nterms, out, 1, 1.0, st);
+}
+
 // ---- diagonal Pauli words (Z and I factors only), any number in one pass -----------------
 // Per tile of 4096 consecutive amplitudes (state bits 0-11), the Walsh-Hadamard transform of
 // the probabilities, W[k] = sum_m (-1)^popcount(m & k) p_(base + m), holds every diagonal
@@ -1011,6 +1271,8 @@ template <typename R> void axpy(void *acc, const void *x, uint32_t nq, double c,
                                             double, double *, double *, int, cudaStream_t, unsigned int *);     \
     template void reduce_generator_inner_complex<R>(const void *, const void *, uint32_t, const GateDesc &,     \
                                                     double *, double *, cudaStream_t);                          \
+    template void reduce_pauli_tiled<R>(const void *, uint32_t, const PauliWord *, int, double *, double *,     \
+                                        cudaStream_t);                                                          \
     template void adjoint_rot_step<R>(void *, void *const *, int, uint32_t, uint32_t, const cd(&)[4],          \
                                       const cd(&)[4], double, double *, double *, int, unsigned int *,         \
                                       cudaStream_t);                                                           \

@@ -120,6 +120,52 @@ def test_pauli_passes_near_and_far(capi, dtype):
         assert abs(sv.var(terms) - O.var(st64, terms)) < tol * 10
 
 
+def _jw_words(rng, n, count):
+    """Jordan-Wigner-shaped words: X/Y on 1, 2 or 4 wires with Z strings between them."""
+    words = []
+    for _ in range(count):
+        k = int(rng.choice([1, 2, 2, 4]))
+        ws = sorted(int(w) for w in rng.choice(n, k, replace=False))
+        letters = {w: "XY"[int(rng.integers(2))] for w in ws}
+        for lo, hi in zip(ws[0::2], ws[1::2]):
+            for w in range(lo + 1, hi):
+                letters[w] = "Z"
+        wires = sorted(letters)
+        words.append(("".join(letters[w] for w in wires), wires))
+    return words
+
+
+@pytest.mark.parametrize("dtype", [np.complex128, np.complex64])
+@pytest.mark.parametrize("n", [12, 13, 20, 22])
+def test_pauli_tiled_passes(capi, dtype, n):
+    """Words with X factors packed into tiled passes (12 tile bits: the words' X bits and the
+    lowest state bits, one state read for up to 32 words): one-wire X/Y words on every wire,
+    Jordan-Wigner strings, 8 words on one 4-wire X mask (runs of 4 sharing the partner reads),
+    40 words on one mask (chunks of 32), masks whose highest bit is a thread bit, a register bit
+    or outside the tile's low bits, and words whose masks do not fit a tile with others (multi
+    and pair passes), on one tile (12 qubits) and up; per word against the oracle."""
+    import lq_oracle as O
+    rng = np.random.default_rng(60 + n)
+    st = random_state(rng, n, dtype)
+    sv = capi.StateVector(n, dtype)
+    sv.upload(st)
+    st64 = st.astype(np.complex128)
+    words = [("X", [q]) for q in range(n)] + [("YZ", [q, (q + 3) % n]) for q in range(n)]
+    words += _jw_words(rng, n, 60)
+    quad = [0, 3, n // 2, n - 1]
+    words += [("".join(p), quad) for p in ("XXXX", "XXYY", "XYXY", "XYYX", "YXXY", "YXYX", "YYXX", "YYYY")]
+    words += [("XXZ", [1, n - 3, 5 + q % 4]) for q in range(40)]
+    wide = sorted(int(w) for w in rng.choice(n, 10, replace=False))
+    words += [("XXXXXXXX", list(range(n - 8, n))), ("YXYXYXYXYX", wide), ("ZZ", [0, n - 1]), ("Z", [4])]
+    coeffs = rng.normal(size=len(words))
+    per, tot = sv.expval_pauli(words, coeffs)
+    want = np.array([O.pauli_expval(st64, wd, ws) for wd, ws in words])
+    tol = TOL[dtype] * (1 if dtype == np.complex128 else 10)
+    err = np.abs(per - want)
+    assert err.max() < tol, (int(err.argmax()), words[int(err.argmax())], err.max())
+    assert abs(tot - float(np.dot(coeffs, want))) < tol * 20
+
+
 @pytest.mark.parametrize("n", [12, 13, 15])
 def test_diagonal_pauli_words_one_pass(capi, n):
     """Many diagonal words (Z and I factors, masks on low, high and both halves of the
