@@ -319,7 +319,9 @@ int b200sv_vjp_state(b200sv_handle psi, const b200sv_op *ops, uint32_t nops,
  * persistent kernel per step (optionally replayed as a CUDA graph).  Each circuit
  * is an op list over its own wires 0..n_c-1 starting from |0...0>, followed by
  * an observable given as a Pauli-word sum.  Parameters live in one device array
- * so steps can change angles without rebuilding the batch. */
+ * so steps can change angles without rebuilding the batch.  Ops: every gate with at
+ * most one parameter (the double excitations included) and B200SV_OP_MATRIX on 1 to 4
+ * wires; Rot and CRot are given as their RZ RY RZ decomposition. */
 typedef struct b200sv_batch *b200sv_batch_handle;
 
 typedef struct b200sv_batch_circuit {

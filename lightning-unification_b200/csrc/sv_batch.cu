@@ -31,8 +31,14 @@
 namespace b200sv {
 namespace batch {
 
-enum Form : uint8_t { F_MAT1 = 1, F_MAT2 = 2, F_DIAG = 3, F_SWAP = 4, F_PARITY = 5, F_NOOP = 6 };
-enum GForm : uint8_t { G_NONE = 0, G_MAT = 1, G_PARITY = 2 };
+// F_PAIR4: the double-excitation family, a 2x2 block on rows 0011 / 1100 of each 16-row group of
+// four target bits, the other rows scaled by gamma.  F_MATK: a constant dense matrix on 3 or 4
+// target bits.  For both, off[j] holds the single bit of target j (matrix order, j = 0 the most
+// significant) instead of row offsets.
+enum Form : uint8_t { F_MAT1 = 1, F_MAT2 = 2, F_DIAG = 3, F_SWAP = 4, F_PARITY = 5, F_NOOP = 6, F_PAIR4 = 7, F_MATK = 8 };
+// G_PAIR4: generator of a double excitation, Y on rows 0011 / 1100 and gk (0: 0, 1: +1, 2: -1)
+// times the identity on the other rows
+enum GForm : uint8_t { G_NONE = 0, G_MAT = 1, G_PARITY = 2, G_PAIR4 = 3 };
 constexpr uint8_t kConstGate = 255;
 constexpr int kMaxKt = 14;
 constexpr int kObsPerPass = 16;  // observables whose expectation values one forward pass accumulates
@@ -176,12 +182,15 @@ __device__ __forceinline__ void op_coeffs(const DOp &op, const double4 *__restri
         const double2 *c = consts + (size_t)op.cidx * 16;
         // NM == 4: D is 2 at compile time; NM == 16 serves every form (D chosen at run time)
         const int D = (NM == 16 && op.form == F_MAT2) ? 4 : 2;
-        if (op.form == F_MAT1 || (NM == 16 && op.form == F_MAT2)) {
+        if (op.form == F_MAT1 || (NM == 16 && (op.form == F_MAT2 || op.form == F_PAIR4))) {
             for (int r = 0; r < D; ++r)
                 for (int q = 0; q < D; ++q) {
                     const double2 z = adj ? c[q * D + r] : c[r * D + q];
                     m[r * D + q] = mk<R>((R)z.x, (R)(adj ? -z.y : z.y));
                 }
+            if constexpr (NM == 16) {
+                if (op.form == F_PAIR4) m[4] = mk<R>((R)c[4].x, (R)(adj ? -c[4].y : c[4].y));  // gamma
+            }
         } else {
             for (int r = 0; r < 4; ++r) m[r] = mk<R>((R)c[r].x, (R)(adj ? -c[r].y : c[r].y));
         }
@@ -201,6 +210,14 @@ __device__ __forceinline__ void op_coeffs(const DOp &op, const double4 *__restri
         m[0] = mk<R>((R)q.z, (R)(sg * q.w)); break;
     case B200SV_IsingZZ:
         m[0] = mk<R>(cr, -sr); m[1] = mk<R>(cr, sr); m[2] = mk<R>(cr, sr); m[3] = mk<R>(cr, -sr); break;
+    case B200SV_DoubleExcitation: case B200SV_DoubleExcitationMinus: case B200SV_DoubleExcitationPlus:
+        if constexpr (NM == 16) {  // block on rows (0011, 1100), gamma on the others
+            m[0] = mk<R>(cr, z); m[1] = mk<R>(-sr, z); m[2] = mk<R>(sr, z); m[3] = mk<R>(cr, z);
+            m[4] = op.gate == B200SV_DoubleExcitationMinus  ? mk<R>(cr, -sr)
+                   : op.gate == B200SV_DoubleExcitationPlus ? mk<R>(cr, sr)
+                                                            : mk<R>(one, z);
+        }
+        break;
     default: {
         if constexpr (NM == 16) {  // two-wire dense gates (F_MAT2)
 #pragma unroll
@@ -385,6 +402,86 @@ __device__ __forceinline__ void apply_op(C<R> *const (&s)[NS], int kt, int wl, b
     }
 }
 
+// offset of row r of a group of K target bits whose single bits are off[0..K-1] (off[0] the most
+// significant matrix-index bit)
+template <int K>
+__device__ __forceinline__ uint32_t row_offset(const uint32_t *off, int r) {
+    uint32_t o = 0;
+#pragma unroll
+    for (int j = 0; j < K; ++j)
+        if ((r >> (K - 1 - j)) & 1) o |= off[j];
+    return o;
+}
+
+// double-excitation step (F_PAIR4): m[0..3] on rows 0011 / 1100 of each 16-row group, the
+// other 14 rows times gamma = m[4] (skipped when gamma is exactly 1)
+template <typename R, int NS>
+__device__ __forceinline__ void apply_pair4(C<R> *const (&s)[NS], int kt, int wl, bool wloc, const DOp &op,
+                                            const C<R> (&m)[16]) {
+    const Range rg = groups(kt, wl, 4, wloc);
+    const uint32_t opa = op.off[2] | op.off[3], opb = op.off[0] | op.off[1];
+    const bool phase = !(m[4].x == (R)1 && m[4].y == (R)0);
+    for (uint32_t g = rg.g0; g < rg.g1; g += rg.gs) {
+        const uint32_t base = ins_local(g, op.low, 4) | op.cmask;
+#pragma unroll
+        for (int q = 0; q < NS; ++q) {
+            C<R> *t = s[q];
+            const C<R> a = t[base + opa], b = t[base + opb];
+            CAcc<R> x, y;
+            x.set(m[0], a); x.add(m[1], b);
+            y.set(m[2], a); y.add(m[3], b);
+            t[base + opa] = x.get();
+            t[base + opb] = y.get();
+            if (phase) {
+#pragma unroll
+                for (int r = 0; r < 16; ++r) {
+                    if (r == 3 || r == 12) continue;
+                    const uint32_t o = base + row_offset<4>(op.off, r);
+                    CAcc<R> w;
+                    w.set(m[4], t[o]);
+                    t[o] = w.get();
+                }
+            }
+        }
+    }
+}
+
+// constant dense matrix on K = 3 or 4 target bits (F_MATK), coefficients read from the constant
+// pool (row-major, 4^K entries), conjugate-transposed for the adjoint
+template <typename R, int NS, int K>
+__device__ __forceinline__ void apply_matk_k(C<R> *const (&s)[NS], int kt, int wl, bool wloc, const DOp &op,
+                                             const double2 *__restrict__ consts, bool adj) {
+    constexpr int D = 1 << K;
+    const double2 *cm = consts + (size_t)op.cidx * 16;
+    const Range rg = groups(kt, wl, op.nb, wloc);
+    for (uint32_t g = rg.g0; g < rg.g1; g += rg.gs) {
+        const uint32_t base = ins_local(g, op.low, op.nb) | op.cmask;
+#pragma unroll 1
+        for (int q = 0; q < NS; ++q) {
+            C<R> *t = s[q];
+            C<R> v[D];
+#pragma unroll
+            for (int c = 0; c < D; ++c) v[c] = t[base + row_offset<K>(op.off, c)];
+#pragma unroll 1
+            for (int r = 0; r < D; ++r) {
+                CAcc<R> a;
+#pragma unroll
+                for (int c = 0; c < D; ++c) {
+                    const double2 z = adj ? cm[c * D + r] : cm[r * D + c];
+                    cacc_term<R>(a, c, mk<R>((R)z.x, (R)(adj ? -z.y : z.y)), v[c]);
+                }
+                t[base + row_offset<K>(op.off, r)] = a.get();
+            }
+        }
+    }
+}
+template <typename R, int NS>
+__device__ __forceinline__ void apply_matk(C<R> *const (&s)[NS], int kt, int wl, bool wloc, const DOp &op,
+                                           const double2 *__restrict__ consts, bool adj) {
+    if (op.nt == 3) apply_matk_k<R, NS, 3>(s, kt, wl, wloc, op, consts, adj);
+    else apply_matk_k<R, NS, 4>(s, kt, wl, wloc, op, consts, adj);
+}
+
 // apply a step of any form with coefficients in a 16-entry array (kernels built with the
 // two-wire dense paths); the parity phase is picked by index, as those kernels keep the
 // array in local memory anyway
@@ -393,6 +490,10 @@ __device__ __forceinline__ void apply_op_general(C<R> *const (&s)[NS], int kt, i
                                                  const C<R> (&m)[16]) {
     if (op.form == F_MAT2) {
         apply_mat2<R, NS>(s, kt, wl, wloc, op, m);
+        return;
+    }
+    if (op.form == F_PAIR4) {
+        apply_pair4<R, NS>(s, kt, wl, wloc, op, m);
         return;
     }
     if (op.form == F_PARITY) {
@@ -411,6 +512,9 @@ __device__ __forceinline__ void apply_op_general(C<R> *const (&s)[NS], int kt, i
     const C<R>(&m4)[4] = reinterpret_cast<const C<R>(&)[4]>(m);
     apply_op<R, NS>(s, kt, wl, wloc, op, m4);
 }
+
+template <typename R, int CODE>
+__device__ __forceinline__ double pair_gen_im_k(C<R> a0, C<R> a1, C<R> b0, C<R> b1);
 
 // per-thread part of Im<bra|G|ket> on one tile, FP64
 // sum over groups of Im(conj(bra) . G ket) for a 2^K x 2^K generator G (FP64)
@@ -453,6 +557,30 @@ __device__ __forceinline__ double gen_inner(const C<R> *bra, const C<R> *ket, in
             acc += sg * (b.x * k.y - b.y * k.x);
         }
         return acc;
+    }
+    if constexpr (FULL) {
+        if (op.gform == G_PAIR4) {
+            // Y on rows (0011, 1100); gamma_g times the identity on the other rows
+            const Range rg = groups(kt, wl, 4, wloc);
+            const uint32_t opa = op.off[2] | op.off[3], opb = op.off[0] | op.off[1];
+            const double gg = op.gk == 1 ? 1.0 : op.gk == 2 ? -1.0 : 0.0;
+            for (uint32_t g = rg.g0; g < rg.g1; g += rg.gs) {
+                const uint32_t base = ins_local(g, op.low, 4) | op.cmask;
+                acc += pair_gen_im_k<R, 2>(ket[base + opa], ket[base + opb], bra[base + opa], bra[base + opb]);
+                if (gg != 0.0) {
+                    double o = 0.0;
+#pragma unroll
+                    for (int r = 0; r < 16; ++r) {
+                        if (r == 3 || r == 12) continue;
+                        const uint32_t i = base + row_offset<4>(op.off, r);
+                        const double2 k = widen<R>(ket[i]), b = widen<R>(bra[i]);
+                        o += b.x * k.y - b.y * k.x;
+                    }
+                    acc += gg * o;
+                }
+            }
+            return acc;
+        }
     }
     const double2 *G = consts + (size_t)op.gcidx * 16;
     const Range rg = groups(kt, wl, op.gnb, wloc);
@@ -1012,9 +1140,13 @@ __device__ void exec_segment(const KArgs &A, C<R> *const (&tiles)[NS], int kt, c
                 else __syncthreads();
             }
             if constexpr (FULL) {
-                C<R> m[16];
-                op_coeffs<R, 16>(op, A.cs, A.consts, REV, m);
-                apply_op_general<R, NS>(tiles, kt, wl, wloc, op, m);
+                if (op.form == F_MATK) {
+                    apply_matk<R, NS>(tiles, kt, wl, wloc, op, A.consts, REV);
+                } else {
+                    C<R> m[16];
+                    op_coeffs<R, 16>(op, A.cs, A.consts, REV, m);
+                    apply_op_general<R, NS>(tiles, kt, wl, wloc, op, m);
+                }
             } else {
                 C<R> m[4];
 #pragma unroll
@@ -1044,7 +1176,7 @@ __device__ __forceinline__ const DSeg &stage_segment(DSeg *s_seg, DOp *s_ops, C<
     for (uint32_t i = threadIdx.x; i < words; i += blockDim.x) reinterpret_cast<uint32_t *>(s_ops)[i] = src[i];
     for (uint32_t o = threadIdx.x; o < g.nops; o += blockDim.x) {
         const DOp &op = A.ops[g.op_begin + o];
-        if (op.form == F_MAT2) continue;  // sixteen coefficients: formed where they are used
+        if (op.form == F_MAT2 || op.form == F_PAIR4 || op.form == F_MATK) continue;  // formed where they are used
         C<R> t[4];
         op_coeffs<R, 4>(op, A.cs, A.consts, adj, t);
 #pragma unroll
@@ -1334,7 +1466,7 @@ HostOp make_hostop(const b200sv_op &o, int64_t pslot, uint32_t nq, int dtype) {
     std::vector<uint32_t> b(w.size());
     for (size_t i = 0; i < w.size(); ++i) b[i] = bitpos(w[i], nq);
     if (o.gate == B200SV_OP_MATRIX) {
-        if (o.nwires < 1 || o.nwires > 2 || !o.matrix) throw Unsupported("batch: matrix ops act on 1 or 2 wires");
+        if (o.nwires < 1 || o.nwires > 4 || !o.matrix) throw Unsupported("batch: matrix ops act on 1 to 4 wires");
         const size_t d = size_t(1) << o.nwires;
         h.cmat.resize(d * d);
         for (size_t i = 0; i < d * d; ++i) {
@@ -1348,7 +1480,7 @@ HostOp make_hostop(const b200sv_op &o, int64_t pslot, uint32_t nq, int dtype) {
         }
         if (h.inv) h.cmat = dagger(h.cmat, d);
         h.gate = kConstGate;
-        h.form = o.nwires == 1 ? F_MAT1 : F_MAT2;
+        h.form = o.nwires == 1 ? F_MAT1 : o.nwires == 2 ? F_MAT2 : F_MATK;
         h.nt = (int)o.nwires;
         h.bits = b;
         return h;
@@ -1392,7 +1524,8 @@ HostOp make_hostop(const b200sv_op &o, int64_t pslot, uint32_t nq, int dtype) {
             return constant(F_DIAG, g.k, ph);
         }
         case Kind::Pair: {
-            if (g.k != 2) throw Unsupported("batch: four-wire gates are not supported");
+            if (g.k == 4) return constant(F_PAIR4, 4, {g.m2[0], g.m2[1], g.m2[2], g.m2[3], g.gamma});
+            if (g.k != 2) throw Unsupported("batch: pair gate width not supported");
             std::vector<cd> m(16, 0.0);
             for (int r = 0; r < 4; ++r) m[r * 4 + r] = g.gamma;
             m[g.pa * 4 + g.pa] = g.m2[0];
@@ -1425,6 +1558,8 @@ HostOp make_hostop(const b200sv_op &o, int64_t pslot, uint32_t nq, int dtype) {
     case B200SV_SingleExcitationMinus: case B200SV_SingleExcitationPlus: h.form = F_MAT2; h.nt = 2; break;
     case B200SV_IsingZZ: h.form = F_DIAG; h.nt = 2; break;
     case B200SV_MultiRZ: h.form = F_PARITY; h.nt = 0; break;
+    case B200SV_DoubleExcitation: case B200SV_DoubleExcitationMinus: case B200SV_DoubleExcitationPlus:
+        h.form = F_PAIR4; h.nt = 4; break;
     default: throw Unsupported(std::string("batch: parameterised gate not supported: ") + gi.name);
     }
     return h;
@@ -1444,10 +1579,12 @@ struct Planned {
     int max_kt = 1;
 };
 
+// coefficients in whole slots of 16 (a 4-wire matrix takes 16 consecutive slots)
 uint32_t push_const(Planned &P, const std::vector<cd> &m) {
     const uint32_t idx = (uint32_t)(P.consts.size() / 16);
-    for (int i = 0; i < 16; ++i) {
-        const cd z = i < (int)m.size() ? m[i] : cd(0, 0);
+    const size_t n = std::max<size_t>(16, (m.size() + 15) / 16 * 16);
+    for (size_t i = 0; i < n; ++i) {
+        const cd z = i < m.size() ? m[i] : cd(0, 0);
         P.consts.push_back(make_double2(z.real(), z.imag()));
     }
     return idx;
@@ -1495,6 +1632,14 @@ DOp lower(Planned &P, const HostOp &h, const std::vector<int> &loc /* state bit 
     if (h.form == F_PARITY) {
         for (auto x : lb) d.pmask |= 1u << x;
         d.nb = 0;
+    } else if (h.form == F_PAIR4 || h.form == F_MATK) {
+        // every bit is a target; off[j] is target j's bit (matrix order)
+        std::vector<uint32_t> all = lb;
+        std::sort(all.begin(), all.end());
+        d.nb = (uint8_t)all.size();
+        for (size_t j = 0; j < all.size(); ++j) d.low[j] = (uint16_t)((1u << all[j]) - 1);
+        for (size_t j = 0; j < lb.size(); ++j) d.off[j] = 1u << lb[j];
+        d.nt = (uint8_t)lb.size();
     } else {
         std::vector<uint32_t> all = lb;
         std::sort(all.begin(), all.end());
@@ -1531,6 +1676,12 @@ DOp lower(Planned &P, const HostOp &h, const std::vector<int> &loc /* state bit 
         if (G.kind == Kind::Parity) {
             d.gform = G_PARITY;
             d.pmask = (uint32_t)G.pmask;
+        } else if (G.kind == Kind::Pair && G.k == 4) {
+            // same bits and rows as the gate (F_PAIR4): Y on rows (0011, 1100), gamma elsewhere
+            if (h.form != F_PAIR4 || G.tbits != lb || G.pa != 3 || G.pb != 12)
+                throw Unsupported("batch: four-wire generator layout");
+            d.gform = G_PAIR4;
+            d.gk = G.gamma == cd(1, 0) ? 1 : G.gamma == cd(-1, 0) ? 2 : 0;
         } else {
             // expand to a dense matrix over G.tbits (k <= 2)
             const int k = G.k;
@@ -1847,7 +1998,9 @@ void build_program(Batch &B, const Config &cfg) {
         throw Unsupported("batch: tile does not fit in shared memory; lower kt");
     B.full = false;
     for (const DOp &d : P.ops)
-        if (d.form == F_MAT2 || (d.gform == G_MAT && d.gk == 2)) B.full = true;
+        if (d.form == F_MAT2 || d.form == F_PAIR4 || d.form == F_MATK || (d.gform == G_MAT && d.gk == 2) ||
+            d.gform == G_PAIR4)
+            B.full = true;
     int per_sm = 1 << 30;
     for (int mode = 0; mode < 2; ++mode) {
         const void *k = batch_kernel(B.dtype, mode, B.full);

@@ -121,8 +121,9 @@ def rot_ring_batch(ncirc: int = 1024, n: int = 16, layers: int = 8, seed: int = 
 def bind(circuit, params):
     """Materialise a batch circuit's op list with concrete parameter values."""
     out = []
-    for (name, wires, inv, p), pi in zip(circuit["ops"], circuit["param_index"]):
-        out.append((name, wires, inv, [float(params[pi])] if pi >= 0 else list(p)))
+    for op, pi in zip(circuit["ops"], circuit["param_index"]):
+        name, wires, inv, p = op[:4]
+        out.append((name, wires, inv, [float(params[pi])] if pi >= 0 else list(p)) + tuple(op[4:]))
     return out
 
 

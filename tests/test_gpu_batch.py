@@ -116,6 +116,79 @@ def test_batch_forward_and_vjp(dtype, maker):
     assert np.abs(p.grad.cpu().numpy() - gwant).max() < GRAD_TOL[dtype]
 
 
+def wide_gate_batch(seed=31):
+    """Circuits with the four-wire double excitations (trainable, shared-slot and constant
+    angles, inverted) and constant matrices on 3 and 4 wires, between layers of rotations and
+    CNOTs; widths on both sides of the on-chip threshold."""
+    from lightning_b200.workloads import random_unitary
+    rng = np.random.default_rng(seed)
+    circuits, params = [], list(rng.uniform(0, 2 * np.pi, 4))
+    de = ["DoubleExcitation", "DoubleExcitationMinus", "DoubleExcitationPlus"]
+    for c in range(9):
+        n = [4, 6, 9, 12, 13, 14, 15, 5, 11][c]
+        ops, pidx = [], []
+        for layer in range(3):
+            for q in range(n):
+                ops.append((["RX", "RY"][(q + layer) % 2], [q], False, []))
+                pidx.append(len(params))
+                params.append(float(rng.uniform(0, 2 * np.pi)))
+            for _ in range(3):
+                w = [int(x) for x in rng.choice(n, 4, replace=False)]
+                r = rng.random()
+                if r < 0.5:
+                    ops.append((de[int(rng.integers(3))], w, bool(rng.random() < 0.3), []))
+                    pidx.append(len(params))
+                    params.append(float(rng.uniform(0, 2 * np.pi)))
+                elif r < 0.65:
+                    ops.append((de[int(rng.integers(3))], w, False, []))
+                    pidx.append(int(rng.integers(4)))  # shared slot
+                elif r < 0.8:
+                    ops.append((de[int(rng.integers(3))], w, bool(rng.random() < 0.5), [float(rng.uniform(0, 6))]))
+                    pidx.append(-1)  # constant angle
+                else:
+                    k = 3 if rng.random() < 0.5 else 4
+                    ops.append(("QubitUnitary", w[:k], bool(rng.random() < 0.5), [], random_unitary(rng, k)))
+                    pidx.append(-1)
+            for q in range(0, n - 1, 2):
+                ops.append(("CNOT", [q, q + 1], False, []))
+                pidx.append(-1)
+        obs = [[(1.0, "Z", [0])], [(0.7, "XY", [n - 1, 1]), (-0.4, "ZZ", [2, n - 1])], [(1.0, "Y", [n // 2])]]
+        circuits.append({"num_qubits": n, "ops": ops, "param_index": pidx, "observables": obs})
+    return circuits, np.array(params)
+
+
+@pytest.mark.parametrize("dtype", [np.complex128, np.complex64])
+def test_batch_double_excitations_and_wide_matrices(dtype):
+    """Four-wire double excitations (their generators in the VJP) and 3-/4-wire matrices in the
+    batched engine: forward outputs, the VJP and the full Jacobian against the FP64 oracle."""
+    import torch
+    from lightning_b200.batch import BatchedCircuits
+    circuits, params = wide_gate_batch()
+    eng = BatchedCircuits(circuits, len(params), dtype=dtype, use_graphs=False)
+    p = torch.tensor(params, dtype=torch.float64, device="cuda")
+    out = eng.forward(p).cpu().numpy()
+    tol = 1e-12 if dtype == np.complex128 else 2e-5
+    assert np.abs(out - oracle_outputs(circuits, params)).max() < tol
+    rng = np.random.default_rng(2)
+    dy = rng.normal(size=out.size)
+    g = eng.vjp(p, torch.tensor(dy, device="cuda")).cpu().numpy()
+    assert np.abs(g - oracle_vjp(circuits, params, dy)).max() < GRAD_TOL[dtype]
+    # Jacobian blocks [nobs x trainable ops] per circuit against the oracle's adjoint Jacobian
+    import lq_oracle as O
+    from lightning_b200.workloads import bind, obs_terms
+    jac = eng.jacobian(p).cpu().numpy()
+    k = 0
+    for c in circuits:
+        ops = bind(c, params)
+        pops = [i for i, op in enumerate(ops) if len(op[3]) > 0]
+        trainable = [j for j, i in enumerate(pops) if c["param_index"][i] >= 0]
+        want = O.adjoint_jacobian(O.run_circuit(c["num_qubits"], ops), ops,
+                                  [obs_terms(ob) for ob in c["observables"]], trainable)
+        got = jac[k:k + want.size].reshape(want.shape)
+        k += want.size
+        assert np.abs(got - want).max() < GRAD_TOL[dtype]
+
+
 @pytest.mark.parametrize("dtype", [np.complex128, np.complex64])
 def test_batch_graphs_and_autotune_repeatable(dtype):
     import torch
