@@ -665,31 +665,112 @@ __device__ __forceinline__ void run_fwd_fixed(C<R> *const (&s)[NS], const Range 
     }
 }
 
-// adjoint pair loop over (lambda, bra): per member (in reverse op order) the generator
-// product, then the member's inverse on both states
-template <typename R, int NS, int LEN, int K0, int G0, int K1, int G1, int K2, int G2>
-__device__ __forceinline__ void run_rev_fixed(C<R> *const (&s)[NS], const Range &rg, uint32_t low, uint32_t bit,
-                                              const C<R> (&m)[kMaxRun][4], double (&ip)[kMaxRun]) {
+// m0 v0 + m1 v1 with one rounding per FMA step (complex64: paired FP32 instructions)
+template <typename R> __device__ __forceinline__ C<R> mac2(C<R> m0, C<R> v0, C<R> m1, C<R> v1);
+template <> __device__ __forceinline__ float2 mac2<float>(float2 m0, float2 v0, float2 m1, float2 v1) {
+    const float2 t = cmul2(m0, v0);
+    const float2 w = __ffma2_rn(make_float2(m1.y, m1.y), make_float2(-v1.y, v1.x), t);
+    return __ffma2_rn(make_float2(m1.x, m1.x), v1, w);
+}
+template <> __device__ __forceinline__ double2 mac2<double>(double2 m0, double2 v0, double2 m1, double2 v1) {
+    CAcc<double> a;
+    a.set(m0, v0);
+    a.add(m1, v1);
+    return a.get();
+}
+
+// Adjoint sweep over a run, fused.  With A_k the product of the inverses undone before member k
+// (reverse order, A_0 = I), member k's generator product at its point of the sweep is
+// Im(b^dagger H_k a) on the run's input pair (a of lambda, b of the bra), H_k = A_k^dagger G_k A_k
+// Hermitian: h00 Im(b0* a0) + h11 Im(b1* a1) + Re h01 (Im(b0* a1) + Im(b1* a0))
+// + Im h01 (Re(b0* a1) - Re(b1* a0)).  The four cross terms are formed once per pair, each member
+// adds one FMA chain, and the run's inverse (the product of its members' inverses) is applied
+// to both states as one 2x2 (FMA chains, as the structured members of the forward runs).  H_k and the product are formed in FP64 per
+// segment (fuse_rev_run).
+template <typename R, int NS, int LEN, bool ALLG>
+__device__ __forceinline__ void run_rev_fused(C<R> *const (&s)[NS], const Range &rg, uint32_t low, uint32_t bit,
+                                              const C<R> (&M)[4], const R (&h)[kMaxRun][4],
+                                              const bool (&has)[kMaxRun], double (&ip)[kMaxRun]) {
     for (uint32_t g = rg.g0; g < rg.g1; g += rg.gs) {
         const uint32_t i0 = ((g & ~low) << 1) | (g & low), i1 = i0 | bit;
-        C<R> a0 = s[0][i0], a1 = s[0][i1], b0 = s[NS - 1][i0], b1 = s[NS - 1][i1];
-        if constexpr (G0 != 0) ip[0] += pair_gen_im_k<R, G0>(a0, a1, b0, b1);
-        apply_pair_k<R, K0>(m[0], a0, a1);
-        apply_pair_k<R, K0>(m[0], b0, b1);
-        if constexpr (LEN > 1) {
-            if constexpr (G1 != 0) ip[1] += pair_gen_im_k<R, G1>(a0, a1, b0, b1);
-            apply_pair_k<R, K1>(m[1], a0, a1);
-            apply_pair_k<R, K1>(m[1], b0, b1);
+        const C<R> a0 = s[0][i0], a1 = s[0][i1], b0 = s[NS - 1][i0], b1 = s[NS - 1][i1];
+        const R x1 = fma(b0.x, a0.y, -(b0.y * a0.x));
+        const R x2 = fma(b1.x, a1.y, -(b1.y * a1.x));
+        const R s1 = fma(b0.x, a1.y, -(b0.y * a1.x)) + fma(b1.x, a0.y, -(b1.y * a0.x));
+        const R s2 = fma(b0.x, a1.x, b0.y * a1.y) - fma(b1.x, a0.x, b1.y * a0.y);
+#pragma unroll
+        for (int k = 0; k < LEN; ++k)
+            if (ALLG || has[k]) ip[k] += (double)fma(h[k][0], x1, fma(h[k][1], x2, fma(h[k][2], s1, h[k][3] * s2)));
+        s[0][i0] = mac2<R>(M[0], a0, M[1], a1);
+        s[0][i1] = mac2<R>(M[2], a0, M[3], a1);
+        s[NS - 1][i0] = mac2<R>(M[0], b0, M[1], b1);
+        s[NS - 1][i1] = mac2<R>(M[2], b0, M[3], b1);
+    }
+}
+
+// Replace the adjoint coefficients of a run (slots cf[0..len-1], staged for the reverse sweep)
+// by its fused form: cf[0] the product of the members' inverses; cf[1] = (h00, h11), h01 of
+// members 0 and 1 of the sweep, cf[2] the same for member 2.  FP64 from the staged coefficients.
+template <typename R>
+__device__ void fuse_rev_run(const DOp *ops, C<R> (*cf)[4], int len) {
+    auto mul = [](double2 a, double2 b) { return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); };
+    auto add = [](double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); };
+    auto cj = [](double2 a) { return make_double2(a.x, -a.y); };
+    // member matrices (adjoints, sweep order), read before cf is overwritten
+    double2 m[kMaxRun][4];
+#pragma unroll
+    for (int k = 0; k < kMaxRun; ++k) {
+        if (k < len) {
+            C<R> t[4];
+            member_from<R>(ops[len - 1 - k], cf[len - 1 - k], t);
+#pragma unroll
+            for (int i = 0; i < 4; ++i) m[k][i] = make_double2((double)t[i].x, (double)t[i].y);
         }
-        if constexpr (LEN > 2) {
-            if constexpr (G2 != 0) ip[2] += pair_gen_im_k<R, G2>(a0, a1, b0, b1);
-            apply_pair_k<R, K2>(m[2], a0, a1);
-            apply_pair_k<R, K2>(m[2], b0, b1);
+    }
+    double2 A[4] = {make_double2(1, 0), make_double2(0, 0), make_double2(0, 0), make_double2(1, 0)};
+    double hv[kMaxRun][4];
+#pragma unroll
+    for (int k = 0; k < kMaxRun; ++k) {
+        hv[k][0] = hv[k][1] = hv[k][2] = hv[k][3] = 0.0;
+        if (k >= len) continue;
+        const DOp &op = ops[len - 1 - k];
+        const int code = op.gslot >= 0 ? op.gcode : 0;
+        if (code) {
+            const double2 z = make_double2(0, 0), one = make_double2(1, 0);
+            double2 G[4];
+            if (code == 1) { G[0] = z; G[1] = one; G[2] = one; G[3] = z; }
+            else if (code == 2) { G[0] = z; G[1] = make_double2(0, -1); G[2] = make_double2(0, 1); G[3] = z; }
+            else if (code == 3) { G[0] = one; G[1] = z; G[2] = z; G[3] = make_double2(-1, 0); }
+            else { G[0] = z; G[1] = z; G[2] = z; G[3] = one; }
+            double2 GA[4];
+#pragma unroll
+            for (int r = 0; r < 2; ++r)
+#pragma unroll
+                for (int c = 0; c < 2; ++c) GA[r * 2 + c] = add(mul(G[r * 2], A[c]), mul(G[r * 2 + 1], A[2 + c]));
+            // H = A^dagger (G A): h00, h11 and h01
+            hv[k][0] = add(mul(cj(A[0]), GA[0]), mul(cj(A[2]), GA[2])).x;
+            hv[k][1] = add(mul(cj(A[1]), GA[1]), mul(cj(A[3]), GA[3])).x;
+            const double2 h01 = add(mul(cj(A[0]), GA[1]), mul(cj(A[2]), GA[3]));
+            hv[k][2] = h01.x;
+            hv[k][3] = h01.y;
         }
-        s[0][i0] = a0;
-        s[0][i1] = a1;
-        s[NS - 1][i0] = b0;
-        s[NS - 1][i1] = b1;
+        double2 B[4];
+#pragma unroll
+        for (int r = 0; r < 2; ++r)
+#pragma unroll
+            for (int c = 0; c < 2; ++c) B[r * 2 + c] = add(mul(m[k][r * 2], A[c]), mul(m[k][r * 2 + 1], A[2 + c]));
+#pragma unroll
+        for (int i = 0; i < 4; ++i) A[i] = B[i];
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i) cf[0][i] = mk<R>((R)A[i].x, (R)A[i].y);
+    cf[1][0] = mk<R>((R)hv[0][0], (R)hv[0][1]);
+    cf[1][1] = mk<R>((R)hv[0][2], (R)hv[0][3]);
+    cf[1][2] = mk<R>((R)hv[1][0], (R)hv[1][1]);
+    cf[1][3] = mk<R>((R)hv[1][2], (R)hv[1][3]);
+    if (len > 2) {
+        cf[2][0] = mk<R>((R)hv[2][0], (R)hv[2][1]);
+        cf[2][1] = mk<R>((R)hv[2][2], (R)hv[2][3]);
     }
 }
 
@@ -780,49 +861,38 @@ __device__ void exec_run(C<R> *const (&s)[NS], int kt, int wl, bool wloc, const 
         return;
     }
     if constexpr (REV) {
-        // adjoint sweep: register copies in reverse order
-        C<R> m[kMaxRun][4];
+        // adjoint sweep, fused per pair (run_rev_fused; coefficients from fuse_rev_run)
+        C<R> M[4];
+        R h[kMaxRun][4];
+        bool has[kMaxRun];
         double ip[kMaxRun];
-        int gc[kMaxRun], mk_[kMaxRun];
+        int gc[kMaxRun];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) M[i] = cf[0][i];
+        h[0][0] = cf[1][0].x; h[0][1] = cf[1][0].y; h[0][2] = cf[1][1].x; h[0][3] = cf[1][1].y;
+        h[1][0] = cf[1][2].x; h[1][1] = cf[1][2].y; h[1][2] = cf[1][3].x; h[1][3] = cf[1][3].y;
+        h[2][0] = h[2][1] = h[2][2] = h[2][3] = (R)0;
+        if (len > 2) {
+            h[2][0] = cf[2][0].x; h[2][1] = cf[2][0].y; h[2][2] = cf[2][1].x; h[2][3] = cf[2][1].y;
+        }
+        bool all = true;
 #pragma unroll
         for (int kk = 0; kk < kMaxRun; ++kk) {
             ip[kk] = 0.0;
             gc[kk] = 0;
-            mk_[kk] = MK_GENERAL;
             if (kk < len) {
                 const DOp &op = ops[len - 1 - kk];
-                member_from<R>(op, cf[len - 1 - kk], m[kk]);
-                mk_[kk] = op.mkind;
                 if (op.gslot >= 0) gc[kk] = op.gcode;
             }
+            has[kk] = gc[kk] != 0;
+            all = all && (kk >= len || has[kk]);
         }
-        switch (run_sig(len, mk_[0], gc[0], mk_[1], gc[1], mk_[2], gc[2])) {
-        case run_sig(3, MK_DIAG, 3, MK_REAL, 2, MK_DIAG, 3):  // Rot = RZ RY RZ, every angle trained
-            run_rev_fixed<R, NS, 3, MK_DIAG, 3, MK_REAL, 2, MK_DIAG, 3>(s, rg, low, bit, m, ip);
-            break;
-        case run_sig(2, MK_DIAG, 3, MK_REAL, 2):  // RY then RZ
-            run_rev_fixed<R, NS, 2, MK_DIAG, 3, MK_REAL, 2, MK_GENERAL, 0>(s, rg, low, bit, m, ip);
-            break;
-        case run_sig(2, MK_REAL, 2, MK_DIAG, 3):  // RZ then RY
-            run_rev_fixed<R, NS, 2, MK_REAL, 2, MK_DIAG, 3, MK_GENERAL, 0>(s, rg, low, bit, m, ip);
-            break;
-        default:
-            for (uint32_t g = rg.g0; g < rg.g1; g += rg.gs) {
-                const uint32_t i0 = ((g & ~low) << 1) | (g & low), i1 = i0 | bit;
-                C<R> a0 = s[0][i0], a1 = s[0][i1], b0 = s[NS - 1][i0], b1 = s[NS - 1][i1];
-#pragma unroll
-                for (int kk = 0; kk < kMaxRun; ++kk) {
-                    if (kk < len) {
-                        if (gc[kk]) ip[kk] += pair_gen_im<R>(gc[kk], a0, a1, b0, b1);
-                        apply_pair<R>(mk_[kk], m[kk], a0, a1);
-                        apply_pair<R>(mk_[kk], m[kk], b0, b1);
-                    }
-                }
-                s[0][i0] = a0;
-                s[0][i1] = a1;
-                s[NS - 1][i0] = b0;
-                s[NS - 1][i1] = b1;
-            }
+        if (len == 3) {
+            if (all) run_rev_fused<R, NS, 3, true>(s, rg, low, bit, M, h, has, ip);
+            else run_rev_fused<R, NS, 3, false>(s, rg, low, bit, M, h, has, ip);
+        } else {
+            if (all) run_rev_fused<R, NS, 2, true>(s, rg, low, bit, M, h, has, ip);
+            else run_rev_fused<R, NS, 2, false>(s, rg, low, bit, M, h, has, ip);
         }
 #pragma unroll
         for (int kk = 0; kk < kMaxRun; ++kk)
@@ -1181,6 +1251,11 @@ __device__ __forceinline__ const DSeg &stage_segment(DSeg *s_seg, DOp *s_ops, C<
         op_coeffs<R, 4>(op, A.cs, A.consts, adj, t);
 #pragma unroll
         for (int r = 0; r < 4; ++r) s_cf[o][r] = t[r];
+    }
+    if (adj) {  // runs of the reverse sweep: fused coefficients, formed once per segment
+        __syncthreads();
+        for (uint32_t o = threadIdx.x; o < g.nops; o += blockDim.x)
+            if (s_ops[o].run >= 2) fuse_rev_run<R>(s_ops + o, s_cf + o, s_ops[o].run);
     }
     __syncthreads();
     return *s_seg;
