@@ -327,6 +327,8 @@ def rows_30q(nq: int, hbm_peak: float, cpu: bool, cpu_qubits: int = 26, steps: i
     h2 = (h2 + h2.conj().T) / 2
     ham = [("ZZ", [q, (q + 1) % nq]) for q in range(nq)] + [("ZZ", [q, (q + 2) % nq]) for q in range(nq)] + \
           [("X", [q]) for q in range(nq)]
+    from lightning_b200.workloads import jordan_wigner_words
+    jw = jordan_wigner_words(np.random.default_rng(5), nq, 400)
     # (label, call, algorithmic bytes, reference op or None)
     rows = [
         ("copy (A1)", lambda: other.copy_from(sv), 2 * S * N, None),
@@ -352,6 +354,7 @@ def rows_30q(nq: int, hbm_peak: float, cpu: bool, cpu_qubits: int = 26, steps: i
         ("expval Hermitian 2 wires (A14)", lambda: sv.expval([(1.0, [("Hermitian", [3, 17], h2)])]), S * N,
          ("expval", [(1.0, [("Hermitian", [3, 17], h2)])])),
         (f"expval_pauli {3 * nq}-term ZZ/X Hamiltonian (A14)", lambda: sv.expval_pauli(ham), S * N, None),
+        ("expval_pauli 400-word Jordan-Wigner sum (A14)", lambda: sv.expval_pauli(jw), S * N, None),
         ("var Y7 (A15)", lambda: sv.var([(1.0, [("PauliY", [7])])]), S * N, ("var", [(1.0, [("PauliY", [7])])])),
     ]
     out = {}
@@ -527,13 +530,16 @@ def run_case(args):
     from lightning_b200 import capi
     torch.cuda.set_device(0)
     if args.case == "gate":
+        # --gate on --wires (negative wires count from the last qubit), complex128
         sv = capi.StateVector(args.qubits, np.complex128)
         st = torch.cuda.current_stream()
         sv.set_stream(st.cuda_stream)
-        ms = timed(lambda: sv.apply("RX", [3], False, [0.3]), args.steps, args.warmup, st)
+        wires = [w % args.qubits for w in (int(x) for x in args.wires.split(","))]
+        par = [0.3] if args.gate in capi.GENERATOR_IDS else [0.1, 0.2, 0.3] if args.gate in ("Rot", "CRot") else []
+        ms = timed(lambda: sv.apply(args.gate, wires, False, par), args.steps, args.warmup, st)
         gbs = 2 * 16 * (1 << args.qubits) / (ms * 1e6)
-        print(json.dumps({"case": "gate", "kernel": "k_dense<double,1>", "qubits": args.qubits, "ms": ms,
-                          "gbs": gbs}))
+        print(json.dumps({"case": "gate", "gate": args.gate, "wires": wires, "qubits": args.qubits, "ms": ms,
+                          "gbs_full_state": gbs}))
         return
     if args.case == "matrix":
         # one random --k-wire unitary per step on a --qubits-qubit state (profiling)
@@ -548,6 +554,26 @@ def run_case(args):
         ms = timed(lambda: sv.apply_matrix(u, wires), args.steps, args.warmup, st)
         print(json.dumps({"case": "matrix", "qubits": args.qubits, "k": args.k, "dtype": args.dtype, "wires": wires,
                           "ms": ms, "tflops": 8 * (1 << args.k) * (1 << args.qubits) / (ms * 1e9)}))
+        return
+    if args.case == "pauli":
+        # Pauli sums on a --qubits state (--dtype): the 3n-term ZZ/X Hamiltonian and 400
+        # Jordan-Wigner words, one expval_pauli call each per step (profiling of the Pauli passes)
+        from lightning_b200.workloads import jordan_wigner_words
+        dt = np.complex64 if args.dtype == "c64" else np.complex128
+        n = args.qubits
+        sv = capi.StateVector(n, dt)
+        st = torch.cuda.current_stream()
+        sv.set_stream(st.cuda_stream)
+        sv.apply_ops([("RY", [q], False, [0.1 + 0.07 * q]) for q in range(n)] +
+                     [("CNOT", [q, q + 1], False, []) for q in range(n - 1)] +
+                     [("RX", [q], False, [0.3 - 0.01 * q]) for q in range(n)])
+        zzx = [("ZZ", [q, (q + 1) % n]) for q in range(n)] + [("ZZ", [q, (q + 2) % n]) for q in range(n)] + \
+              [("X", [q]) for q in range(n)]
+        jw = jordan_wigner_words(np.random.default_rng(5), n, 400)
+        res = {"case": "pauli", "qubits": n, "dtype": args.dtype}
+        for name, words in (("zzx_ms", zzx), ("jw400_ms", jw)):
+            res[name] = timed(lambda: sv.expval_pauli(words), args.steps, args.warmup, st)
+        print(json.dumps(res))
         return
     if args.case == "plain":
         print(json.dumps({"case": "plain", **plain_layered(not args.no_cpu)}))
@@ -866,11 +892,13 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--sweep-qubits", type=int, default=30)
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--case", default="full", choices=["full", "gate", "batch", "fused", "precision", "plain", "matrix", "rows", "next"],
+    ap.add_argument("--case", default="full", choices=["full", "gate", "batch", "fused", "precision", "plain", "matrix", "rows", "next", "pauli"],
                     help="gate / batch: one kernel family on a small case (profiling)")
     ap.add_argument("--qubits", type=int, default=28, help="--case gate: state width (complex128)")
+    ap.add_argument("--gate", default="RX", help="--case gate: gate name")
+    ap.add_argument("--wires", default="3", help="--case gate: comma-separated wires (negative: from the last)")
     ap.add_argument("--ncirc", type=int, default=148, help="--case batch: number of circuits")
-    ap.add_argument("--dtype", default="c128", choices=["c64", "c128"], help="--case fused / matrix: state precision")
+    ap.add_argument("--dtype", default="c128", choices=["c64", "c128"], help="--case fused / matrix / pauli: state precision")
     ap.add_argument("--k", type=int, default=5, help="--case matrix: wires of the unitary")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)

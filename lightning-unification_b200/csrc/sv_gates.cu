@@ -105,6 +105,34 @@ template <typename R, int K>
 __global__ void __launch_bounds__(kThreads) k_dense(States s, DenseP<R, K> p) {
     C<R> *__restrict__ sv = static_cast<C<R> *>(s.p[blockIdx.y]);
     constexpr int D = 1 << K;
+    if constexpr (K == 1) {
+        // one-wire steps: U pairs a trip, every load issued before the first store
+        constexpr int U = 4;
+        const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+        for (uint64_t g0 = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g0 < p.ngroups; g0 += U * stride) {
+            uint64_t base[U];
+            C<R> v0[U], v1[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const uint64_t g = g0 + u * stride;
+                base[u] = g < p.ngroups ? (p.ins(g) | p.cmask) : ~uint64_t(0);
+                if (g < p.ngroups) {
+                    v0[u] = sv[base[u] + p.off[0]];
+                    v1[u] = sv[base[u] + p.off[1]];
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                if (base[u] == ~uint64_t(0)) continue;
+                CAcc<R> a, b;
+                a.set(p.m[0], v0[u]); a.add(p.m[1], v1[u]);
+                b.set(p.m[2], v0[u]); b.add(p.m[3], v1[u]);
+                sv[base[u] + p.off[0]] = a.get();
+                sv[base[u] + p.off[1]] = b.get();
+            }
+        }
+        return;
+    }
     for (uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < p.ngroups;
          g += (uint64_t)gridDim.x * blockDim.x) {
         const uint64_t base = p.ins(g) | p.cmask;
@@ -334,16 +362,32 @@ template <typename R, int K> struct DiagP {
 };
 template <typename R, int K>
 __global__ void __launch_bounds__(kThreads) k_diag(States s, DiagP<R, K> p) {
+    // U groups a trip, every load issued before the first store (one multiply per amplitude
+    // covers little of the load latency)
+    constexpr int D = 1 << K, U = D >= 4 ? 2 : 4;
     C<R> *__restrict__ sv = static_cast<C<R> *>(s.p[blockIdx.y]);
-    for (uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < p.ngroups;
-         g += (uint64_t)gridDim.x * blockDim.x) {
-        const uint64_t base = p.ins(g) | p.cmask;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t g0 = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g0 < p.ngroups; g0 += U * stride) {
+        uint64_t base[U];
+        C<R> v[U][D];
 #pragma unroll
-        for (int r = 0; r < (1 << K); ++r) {
-            const C<R> v = sv[base + p.off[r]];
-            CAcc<R> a;
-            a.add(p.ph[r], v);
-            sv[base + p.off[r]] = a.get();
+        for (int u = 0; u < U; ++u) {
+            const uint64_t g = g0 + u * stride;
+            base[u] = g < p.ngroups ? (p.ins(g) | p.cmask) : ~uint64_t(0);
+            if (g < p.ngroups) {
+#pragma unroll
+                for (int r = 0; r < D; ++r) v[u][r] = sv[base[u] + p.off[r]];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            if (base[u] == ~uint64_t(0)) continue;
+#pragma unroll
+            for (int r = 0; r < D; ++r) {
+                CAcc<R> a;
+                a.set(p.ph[r], v[u][r]);
+                sv[base[u] + p.off[r]] = a.get();
+            }
         }
     }
 }
@@ -354,14 +398,29 @@ struct SwapP {
 };
 template <typename R>
 __global__ void __launch_bounds__(kThreads) k_swap(States s, SwapP p) {
+    // U groups a trip with every load issued before the first store: a swap has no arithmetic
+    // to cover the load latency, so the loads in flight per thread set its bandwidth
+    constexpr int U = 4;
     C<R> *__restrict__ sv = static_cast<C<R> *>(s.p[blockIdx.y]);
-    for (uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < p.ngroups;
-         g += (uint64_t)gridDim.x * blockDim.x) {
-        const uint64_t base = p.ins(g) | p.cmask;
-        const C<R> a = sv[base + p.oa];
-        const C<R> b = sv[base + p.ob];
-        sv[base + p.oa] = b;
-        sv[base + p.ob] = a;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t g0 = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g0 < p.ngroups; g0 += U * stride) {
+        uint64_t base[U];
+        C<R> a[U], b[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const uint64_t g = g0 + u * stride;
+            base[u] = g < p.ngroups ? (p.ins(g) | p.cmask) : ~uint64_t(0);
+            if (g < p.ngroups) {
+                a[u] = sv[base[u] + p.oa];
+                b[u] = sv[base[u] + p.ob];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            if (base[u] == ~uint64_t(0)) continue;
+            sv[base[u] + p.oa] = b[u];
+            sv[base[u] + p.ob] = a[u];
+        }
     }
 }
 
@@ -407,13 +466,23 @@ template <typename R> struct ParityP {
 };
 template <typename R>
 __global__ void __launch_bounds__(kThreads) k_parity(States s, ParityP<R> p) {
+    // U amplitudes a trip, every load issued before the first store
+    constexpr int U = 4;
     C<R> *__restrict__ sv = static_cast<C<R> *>(s.p[blockIdx.y]);
-    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < p.n;
-         i += (uint64_t)gridDim.x * blockDim.x) {
-        const C<R> v = sv[i];
-        CAcc<R> a;
-        a.add((__popcll(i & p.mask) & 1) ? p.ph[1] : p.ph[0], v);  // a select: an index would copy ph to local memory
-        sv[i] = a.get();
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i0 = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i0 < p.n; i0 += U * stride) {
+        C<R> v[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+            if (i0 + u * stride < p.n) v[u] = sv[i0 + u * stride];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const uint64_t i = i0 + u * stride;
+            if (i >= p.n) continue;
+            CAcc<R> a;
+            a.set((__popcll(i & p.mask) & 1) ? p.ph[1] : p.ph[0], v[u]);  // a select: an index would copy ph to local memory
+            sv[i] = a.get();
+        }
     }
 }
 
