@@ -8,6 +8,7 @@
 #include <memory>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/b200sv.h"
@@ -30,6 +31,8 @@ struct b200sv_state {
     void *d_matrix = nullptr;      // dense matrix staging
     size_t matrix_bytes = 0;
     void *d_scratch[2] = {nullptr, nullptr};  // two state-sized work buffers (lazy)
+    void *h_stage[2] = {nullptr, nullptr};    // pinned staging halves for host-array uploads (lazy)
+    cudaEvent_t stage_ev[2] = {nullptr, nullptr};
     cudaStream_t stream() const { return has_ext ? ext : own; }
     size_t amp_bytes() const { return dtype == B200SV_C64 ? 8 : 16; }
     size_t state_bytes() const { return amp_bytes() << nq; }
@@ -561,6 +564,10 @@ int b200sv_destroy(b200sv_handle h) {
         if (h->d_matrix) cudaFree(h->d_matrix);
         for (auto &s : h->d_scratch)
             if (s) cudaFree(s);
+        for (int k = 0; k < 2; ++k) {
+            if (h->h_stage[k]) cudaFreeHost(h->h_stage[k]);
+            if (h->stage_ev[k]) cudaEventDestroy(h->stage_ev[k]);
+        }
         cudaStreamDestroy(h->own);
         delete h;
     });
@@ -855,6 +862,67 @@ int b200sv_norm2(b200sv_handle h, double *out) {
     });
 }
 
+// ---- host-array uploads ----------------------------------------------------------------
+constexpr size_t kStageBytes = size_t(64) << 20;
+
+// memcpy split over nt host threads
+static void parallel_copy(char *dst, const char *src, size_t n, unsigned nt) {
+    if (nt <= 1 || n < (size_t(1) << 20)) {
+        std::memcpy(dst, src, n);
+        return;
+    }
+    const size_t per = (n + nt - 1) / nt;
+    std::vector<std::thread> th;
+    for (unsigned t = 1; t < nt; ++t) {
+        const size_t a = t * per;
+        if (a >= n) break;
+        const size_t b = std::min(n, a + per);
+        th.emplace_back([=] { std::memcpy(dst + a, src + a, b - a); });
+    }
+    std::memcpy(dst, src, std::min(n, per));
+    for (auto &x : th) x.join();
+}
+
+// Copy `bytes` from caller host memory to device memory on the state's stream.  Pinned (or
+// registered) host memory is copied directly.  Large pageable arrays go through two pinned
+// 64 MiB halves kept by the handle: host threads fill one half while the other half's copy
+// runs, so the transfer runs near the pinned link rate instead of the pageable path's.  A half
+// is refilled only after its previous copy has completed (an event per half), so the call may
+// return while the last copies are still in flight.
+static void upload_host(b200sv_state *h, void *dst, const void *src, size_t bytes) {
+    if (!bytes) return;
+    const cudaStream_t st = h->stream();
+    cudaPointerAttributes pa{};
+    const bool pinned = cudaPointerGetAttributes(&pa, src) == cudaSuccess && pa.type == cudaMemoryTypeHost;
+    cudaGetLastError();  // a failed query of plain host memory leaves no error behind
+    if (pinned || bytes <= (size_t(4) << 20)) {
+        B200SV_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st));
+        return;
+    }
+    for (int k = 0; k < 2; ++k) {
+        if (!h->h_stage[k]) {
+            if (cudaHostAlloc(&h->h_stage[k], kStageBytes, cudaHostAllocDefault) != cudaSuccess) {
+                cudaGetLastError();
+                h->h_stage[k] = nullptr;
+                B200SV_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st));  // no pinned memory
+                return;
+            }
+        }
+        if (!h->stage_ev[k]) B200SV_CUDA(cudaEventCreateWithFlags(&h->stage_ev[k], cudaEventDisableTiming));
+    }
+    const unsigned nt = std::max(1u, std::min(8u, std::thread::hardware_concurrency()));
+    const char *s = static_cast<const char *>(src);
+    char *d = static_cast<char *>(dst);
+    int k = 0;
+    for (size_t off = 0; off < bytes; off += kStageBytes, k ^= 1) {
+        const size_t n = std::min(kStageBytes, bytes - off);
+        B200SV_CUDA(cudaEventSynchronize(h->stage_ev[k]));  // the half's previous copy has completed
+        parallel_copy(static_cast<char *>(h->h_stage[k]), s + off, n, nt);
+        B200SV_CUDA(cudaMemcpyAsync(d + off, h->h_stage[k], n, cudaMemcpyHostToDevice, st));
+        B200SV_CUDA(cudaEventRecord(h->stage_ev[k], st));
+    }
+}
+
 // ---- sparse Hamiltonian: LQ/measurements/MeasurementsLQubit.hpp:197-214, :451-472 ----
 // out[0] = Re<psi|H psi>, out[1] = <H psi|H psi>.  The CSR arrays are checked on the host
 // (the reference reads them unchecked) so no launch reads outside them or the state.
@@ -888,10 +956,10 @@ static void sparse_impl(b200sv_state *h, const uint64_t *row_map, uint64_t row_m
             cudaFreeAsync(c, s);
         }
     } fr{d_rows, d_cols, d_vals, st};
-    B200SV_CUDA(cudaMemcpyAsync(d_rows, row_map, (N + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice, st));
+    upload_host(h, d_rows, row_map, (N + 1) * sizeof(uint64_t));
     if (used) {
-        B200SV_CUDA(cudaMemcpyAsync(d_cols, entries, used * sizeof(uint64_t), cudaMemcpyHostToDevice, st));
-        B200SV_CUDA(cudaMemcpyAsync(d_vals, values, used * S, cudaMemcpyHostToDevice, st));
+        upload_host(h, d_cols, entries, used * sizeof(uint64_t));
+        upload_host(h, d_vals, values, used * S);
     }
     sparse_device(h, d_rows, d_cols, d_vals, used, out);
 }

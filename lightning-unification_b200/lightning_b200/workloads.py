@@ -118,6 +118,22 @@ def rot_ring_batch(ncirc: int = 1024, n: int = 16, layers: int = 8, seed: int = 
     return circuits, np.array(params)
 
 
+def jordan_wigner_words(rng, n: int, count: int):
+    """Pauli words shaped like Jordan-Wigner fermion terms: X/Y on 1, 2 or 4 wires with Z
+    strings between the paired wires, as ("XZZY", [wires]) in ascending wire order."""
+    words = []
+    for _ in range(count):
+        k = int(rng.choice([1, 2, 2, 4]))
+        ws = sorted(int(w) for w in rng.choice(n, k, replace=False))
+        letters = {w: "XY"[int(rng.integers(2))] for w in ws}
+        for lo, hi in zip(ws[0::2], ws[1::2]):
+            for w in range(lo + 1, hi):
+                letters[w] = "Z"
+        wires = sorted(letters)
+        words.append(("".join(letters[w] for w in wires), wires))
+    return words
+
+
 def bind(circuit, params):
     """Materialise a batch circuit's op list with concrete parameter values."""
     out = []

@@ -120,21 +120,6 @@ def test_pauli_passes_near_and_far(capi, dtype):
         assert abs(sv.var(terms) - O.var(st64, terms)) < tol * 10
 
 
-def _jw_words(rng, n, count):
-    """Jordan-Wigner-shaped words: X/Y on 1, 2 or 4 wires with Z strings between them."""
-    words = []
-    for _ in range(count):
-        k = int(rng.choice([1, 2, 2, 4]))
-        ws = sorted(int(w) for w in rng.choice(n, k, replace=False))
-        letters = {w: "XY"[int(rng.integers(2))] for w in ws}
-        for lo, hi in zip(ws[0::2], ws[1::2]):
-            for w in range(lo + 1, hi):
-                letters[w] = "Z"
-        wires = sorted(letters)
-        words.append(("".join(letters[w] for w in wires), wires))
-    return words
-
-
 @pytest.mark.parametrize("dtype", [np.complex128, np.complex64])
 @pytest.mark.parametrize("n", [12, 13, 20, 22])
 def test_pauli_tiled_passes(capi, dtype, n):
@@ -151,7 +136,8 @@ def test_pauli_tiled_passes(capi, dtype, n):
     sv.upload(st)
     st64 = st.astype(np.complex128)
     words = [("X", [q]) for q in range(n)] + [("YZ", [q, (q + 3) % n]) for q in range(n)]
-    words += _jw_words(rng, n, 60)
+    from lightning_b200.workloads import jordan_wigner_words
+    words += jordan_wigner_words(rng, n, 60)
     quad = [0, 3, n // 2, n - 1]
     words += [("".join(p), quad) for p in ("XXXX", "XXYY", "XYXY", "XYYX", "YXXY", "YXYX", "YYXX", "YYYY")]
     words += [("XXZ", [1, n - 3, 5 + q % 4]) for q in range(40)]
