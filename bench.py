@@ -519,8 +519,8 @@ RX_DRAM_BYTES_26Q = 1.0737e9 + 1.0137e9
 # DRAM bytes (read + write) of the forward and VJP launches of the batched kernel on 148
 # circuits of the batched-adjoint workload, from an ncu capture of `bench.py --case batch`;
 # circuits are independent, so a step's traffic scales with the number of circuits.
-BATCH_DRAM_BYTES_148 = (0.0551e9 + 0.9862e9) + (3.1313e9 + 3.5045e9)
-BATCH_ISSUE_ACTIVE = 0.53  # scheduler cycles issuing, same capture (forward 52 %, VJP 53 %)
+BATCH_DRAM_BYTES_148 = (0.0900e9 + 0.9940e9) + (3.0908e9 + 3.5086e9)
+BATCH_ISSUE_ACTIVE = 0.48  # scheduler cycles issuing, same capture (forward 52 %, VJP 46 %, time-weighted)
 
 
 def run_case(args):
