@@ -392,7 +392,7 @@ def rows_30q(nq: int, hbm_peak: float, cpu: bool, cpu_qubits: int = 26, steps: i
     return out
 
 
-def next_rows(cpu: bool, reps: int = 3):
+def next_rows(cpu: bool, reps: int = 7):
     """The rows beside the core path, complex128: the state-return VJP (20 qubits, 2 layers of
     RX RY RZ + CNOT ladder, 120 parameters), a sparse Hamiltonian expectation value (22 qubits,
     the periodic tridiagonal CSR matrix of the reference's tests, 3 entries per row) and
@@ -682,7 +682,7 @@ def hea_forward(steps: int, warmup: int, ncirc: int = 4096, dtype=np.complex64, 
     return res
 
 
-def plain_layered(cpu: bool, reps: int = 3):
+def plain_layered(cpu: bool, reps: int = 7):
     """The plain single-circuit configuration: 20 qubits complex128, 10 layers of RX RY RZ on
     every qubit + CNOT ladder (790 gates), <Z0> and the 600-parameter adjoint Jacobian, through
     the C ABI (one launch per gate), timed as the host sees each call (median of `reps`);

@@ -142,7 +142,9 @@ __global__ void __launch_bounds__(kThreads) k_dense(States s, DenseP<R, K> p) {
         if constexpr (K >= 3) {
             // two output rows per trip of a rolled loop: two accumulators live instead of
             // 2^K, so more warps fit on an SM (72 vs 108 registers for complex128 at K = 3,
-            // which moves a 30-qubit 3-wire unitary from 4.5 to 6.1 TB/s); same FMA order
+            // which moves a 30-qubit 3-wire unitary from 4.5 to 6.1 TB/s); same FMA order.
+            // At K = 4 (complex128, 30 qubits) this takes 9.2 ms; four rows a trip 9.8 ms,
+            // every row unrolled 13.3 ms (172 registers)
 #pragma unroll 1
             for (int r = 0; r < D; r += 2) {
                 CAcc<R> a, b;
@@ -537,7 +539,10 @@ bool launch_dense_k(const States &S, int ns, uint32_t nq, const GateDesc &g, voi
             return true;
         }
     }
-    if constexpr (K <= 3) {
+    if constexpr (K <= 4) {
+        // the matrix as a kernel parameter (4^K entries; 4 KiB complex128 at K = 4): each
+        // coefficient is a warp-uniform constant-bank operand, where a matrix in device memory
+        // costs one L1 load per complex product
         DenseP<R, K> p{};
         p.ins = make_insert(all);
         p.cmask = ctrl_mask(g.cbits);
