@@ -145,7 +145,20 @@ struct alignas(16) RPhase {
     uint32_t rdep[16];       // tile offset of register g (g's bits deposited into the register bits)
     uint32_t srdep[16];      // swz(rdep[g]): the swizzle is linear over XOR, so a register's shared-memory
                              // position is swz(thread part) ^ srdep[g]
+    uint32_t ilow[4];        // (1 << register bit j) - 1, ascending: the thread part is the thread index
+                             // with zeros inserted at the register bits
 };
+
+// the thread part of a phase's tile offsets: the thread index with a zero inserted at each of
+// the phase's NA register bits (the thread index deposited into comp, in NA steps)
+template <int NA> __device__ __forceinline__ uint32_t phase_base(uint32_t x, const RPhase &ph) {
+#pragma unroll
+    for (int j = 0; j < NA; ++j) {
+        const uint32_t lo = x & ph.ilow[j];
+        x = ((x ^ lo) << 1) | lo;
+    }
+    return x;
+}
 
 // Register op codes: form and, for the forms with targets, the register mask of the targets
 // (index into the list of masks with that many bits).
@@ -373,17 +386,6 @@ __device__ __forceinline__ uint64_t deposit(uint64_t x, const uint8_t *pos, int 
     return r;
 }
 
-// x's low bits deposited into the set bits of mask (ascending)
-__device__ __forceinline__ uint32_t pdep32(uint32_t x, uint32_t mask) {
-    uint32_t r = 0;
-    while (mask) {
-        const uint32_t low = mask & (0u - mask);
-        if (x & 1u) r |= low;
-        x >>= 1;
-        mask ^= low;
-    }
-    return r;
-}
 
 struct SegArgs {
     const RPhase *phases;
@@ -442,25 +444,27 @@ __global__ void __launch_bounds__(kFThreads, 1) k_fused(C<R> *__restrict__ state
 
     uint64_t t = blockIdx.x;
     uint32_t cur = 0;
+    uint64_t tb_cur = 0;  // state offset of tile t (deposited once, when the tile is prefetched)
     if (t < ntiles) {
-        const uint64_t tb = deposit(t, s_gbits, a.ng);
+        tb_cur = deposit(t, s_gbits, a.ng);
 #pragma unroll
-        for (int j = 0; j < PER; ++j) cp_async16(buf0 + sw(j), state + (tb | lo | s_hi[j]));
+        for (int j = 0; j < PER; ++j) cp_async16(buf0 + sw(j), state + (tb_cur | lo | s_hi[j]));
     }
     cp_async_commit();
     for (; t < ntiles; t += gridDim.x) {
         const uint64_t tnext = t + gridDim.x;
+        uint64_t tb_next = 0;
         if (tnext < ntiles) {
-            const uint64_t tb = deposit(tnext, s_gbits, a.ng);
+            tb_next = deposit(tnext, s_gbits, a.ng);
             C<R> *dst = buf0 + (cur ^ 1u) * TN;
 #pragma unroll
-            for (int j = 0; j < PER; ++j) cp_async16(dst + sw(j), state + (tb | lo | s_hi[j]));
+            for (int j = 0; j < PER; ++j) cp_async16(dst + sw(j), state + (tb_next | lo | s_hi[j]));
         }
         cp_async_commit();
         cp_async_wait1();
         __syncthreads();
         C<R> *s = buf0 + cur * TN;
-        const uint64_t tbase = deposit(t, s_gbits, a.ng);
+        const uint64_t tbase = tb_cur;
         for (int p = 0; p < a.nph; ++p) {
             const RPhase &ph = sph[p];
             if (ph.fop >= 0) {
@@ -469,7 +473,7 @@ __global__ void __launch_bounds__(kFThreads, 1) k_fused(C<R> *__restrict__ state
                 __syncthreads();
                 continue;
             }
-            const uint32_t base = pdep32(threadIdx.x, ph.comp);
+            const uint32_t base = phase_base<Geo<R>::a>(threadIdx.x, ph);
             const uint32_t sbase = swz<R>(base);
             uint32_t l[A];
             C<R> v[A];
@@ -496,6 +500,7 @@ __global__ void __launch_bounds__(kFThreads, 1) k_fused(C<R> *__restrict__ state
         }
         __syncthreads();  // the buffer is refilled next iteration
         cur ^= 1u;
+        tb_cur = tb_next;
     }
     cp_async_wait0();
 }
@@ -732,6 +737,7 @@ void lower_phase(SegCode<R> &sc, uint32_t rmask, const std::vector<const GateDes
     ph.op_begin = (int32_t)sc.rops.size();
     ph.fop = -1;
     ph.comp = ((1u << KT) - 1) & ~rmask;
+    for (int j = 0; j < a; ++j) ph.ilow[j] = (1u << rb[j]) - 1;
     for (int g = 0; g < A; ++g) {
         uint32_t o = 0;
         for (int j = 0; j < a; ++j)
@@ -1028,7 +1034,7 @@ void run_fused(void *state, uint32_t nq, const std::vector<GateDesc> &descs,
     size_t smem_max = 0;
     for (const Piece &p : pieces)
         if (p.seg) smem_max = std::max(smem_max, seg_smem(p.s));
-    // at most 192 ops per segment: 128 KiB of tiles + 192 x (144 + 48) B + 32 KiB of coefficients
+    // at most 192 ops per segment: 128 KiB of tiles + 192 x (160 + 48) B + 32 KiB of coefficients
     // (+ 160 B per double excitation)
     if (smem_max > 227 * 1024) throw Unsupported("fused segment records exceed shared memory");
     B200SV_CUDA(cudaFuncSetAttribute(k_fused<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_max));
@@ -1216,7 +1222,7 @@ __global__ void __launch_bounds__(kFThreads, 1) k_fused_adj(C<R> *__restrict__ l
         const uint64_t tbase = deposit(t, s_gbits, a.ng);
         for (int p = 0; p < a.nph; ++p) {
             const RPhase &ph = sph[p];
-            const uint32_t base = pdep32(threadIdx.x, ph.comp);
+            const uint32_t base = phase_base<GeoA<R>::a>(threadIdx.x, ph);
             const uint32_t sbase = swz<R>(base);
             uint32_t l[A];
             C<R> v[A], w[A];
