@@ -517,6 +517,27 @@ int b200sv_device_count(int *count) {
     });
 }
 
+// The calls allocate their work buffers (lambda and bras of the adjoint, sampling and segment
+// tables) stream-ordered from the device's default pool.  With the pool's default release
+// threshold of 0, every synchronisation hands the freed memory back and the next call maps it
+// again; keeping up to 1 GiB of freed memory in the pool (a setting of this process only) lets
+// repeated calls reuse it.  A larger threshold set by the application is left as it is.
+static void keep_pool_memory(int device) {
+    static std::once_flag flags[64];
+    if (device < 0 || device >= 64) return;
+    std::call_once(flags[device], [device] {
+        cudaMemPool_t pool;
+        if (cudaDeviceGetDefaultMemPool(&pool, device) != cudaSuccess) {
+            cudaGetLastError();
+            return;
+        }
+        uint64_t cur = 0, want = uint64_t(1) << 30;
+        if (cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &cur) == cudaSuccess && cur < want)
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &want);
+        cudaGetLastError();
+    });
+}
+
 int b200sv_create(uint32_t num_qubits, int dtype, b200sv_handle *out) {
     return guard([&] {
         need(out != nullptr, "NULL output handle");
@@ -531,6 +552,7 @@ int b200sv_create(uint32_t num_qubits, int dtype, b200sv_handle *out) {
         h->nq = num_qubits;
         h->dtype = dtype;
         B200SV_CUDA(cudaGetDevice(&h->device));
+        keep_pool_memory(h->device);
         try {
             B200SV_CUDA(cudaStreamCreateWithFlags(&h->own, cudaStreamNonBlocking));
             B200SV_CUDA(cudaMalloc(&h->d_state, h->state_bytes()));
