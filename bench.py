@@ -514,7 +514,7 @@ def matrix_sweep(nq: int, hbm_peak: float, kmax: int = 8, steps: int = 3):
 # DRAM bytes (read + write) of one k_dense<double,1> launch (RX) on a 26-qubit complex128
 # state, from an ncu capture; the kernel streams each amplitude once, so the traffic
 # grows in proportion to the state.
-RX_DRAM_BYTES_26Q = 1.0737e9 + 1.0137e9
+RX_DRAM_BYTES_26Q = 1.0738e9 + 1.0144e9
 
 # DRAM bytes (read + write) of the forward and VJP launches of the batched kernel on 148
 # circuits of the batched-adjoint workload, from an ncu capture of `bench.py --case batch`;
