@@ -79,9 +79,12 @@ uint64_t ctrl_mask(const std::vector<uint32_t> &cb) {
     return m;
 }
 
-dim3 grid_for(uint64_t work, int nstates) {
+// per_thread: work items a thread takes per trip (the kernels that batch their loads), so a
+// small state gets one wave of threads that each keep several loads in flight
+dim3 grid_for(uint64_t work, int nstates, int per_thread = 1) {
     const uint64_t cap = uint64_t(sm_count()) * 16;
-    uint64_t b = (work + kThreads - 1) / kThreads;
+    const uint64_t per_block = uint64_t(kThreads) * (uint64_t)per_thread;
+    uint64_t b = (work + per_block - 1) / per_block;
     if (b > cap) b = cap;
     if (b == 0) b = 1;
     return dim3((unsigned)b, (unsigned)nstates);
@@ -549,7 +552,7 @@ bool launch_dense_k(const States &S, int ns, uint32_t nq, const GateDesc &g, voi
         p.ngroups = ngroups;
         fill_offsets(p.off, g.tbits);
         for (int i = 0; i < (1 << K) * (1 << K); ++i) p.m[i] = cvt<R>(g.m[i]);
-        k_dense<R, K><<<grid_for(ngroups, ns), kThreads, 0, st>>>(S, p);
+        k_dense<R, K><<<grid_for(ngroups, ns, K == 1 ? 4 : 1), kThreads, 0, st>>>(S, p);
     } else if constexpr (K <= 6) {
         DenseDevP<R, K> p{};
         p.ins = make_insert(all);
@@ -576,7 +579,7 @@ void launch_diag_k(const States &S, int ns, uint32_t nq, const GateDesc &g, cuda
     p.ngroups = uint64_t(1) << (nq - all.size());
     fill_offsets(p.off, g.tbits);
     for (int i = 0; i < (1 << K); ++i) p.ph[i] = cvt<R>(g.m[i]);
-    k_diag<R, K><<<grid_for(p.ngroups, ns), kThreads, 0, st>>>(S, p);
+    k_diag<R, K><<<grid_for(p.ngroups, ns, K >= 2 ? 2 : 4), kThreads, 0, st>>>(S, p);
 }
 
 template <typename R, int K>
@@ -665,7 +668,7 @@ void launch_gate(void *const *states, int nstates, uint32_t nq, const GateDesc &
         fill_offsets(off, g.tbits);
         p.oa = off[g.sa];
         p.ob = off[g.sb];
-        k_swap<R><<<grid_for(p.ngroups, nstates), kThreads, 0, st>>>(S, p);
+        k_swap<R><<<grid_for(p.ngroups, nstates, 4), kThreads, 0, st>>>(S, p);
         break;
     }
     case Kind::Pair:
@@ -682,7 +685,7 @@ void launch_gate(void *const *states, int nstates, uint32_t nq, const GateDesc &
         p.mask = g.pmask;
         p.ph[0] = cvt<R>(g.pphase[0]);
         p.ph[1] = cvt<R>(g.pphase[1]);
-        k_parity<R><<<grid_for(p.n, nstates), kThreads, 0, st>>>(S, p);
+        k_parity<R><<<grid_for(p.n, nstates, 4), kThreads, 0, st>>>(S, p);
         break;
     }
     default: break;
