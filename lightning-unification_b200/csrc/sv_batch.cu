@@ -1087,6 +1087,7 @@ struct KArgs {
     double *gradw;        // VJP: [ngslots * nwarps]
     void *pool_a, *pool_b;
     const int *reuse;     // VJP: nonzero when pool A still holds this step's forward states
+    const void *rcf;      // VJP: per op, the reverse sweep's coefficients (k_rev_coeffs)
     int max_kt;
 };
 
@@ -1244,18 +1245,18 @@ __device__ __forceinline__ const DSeg &stage_segment(DSeg *s_seg, DOp *s_ops, C<
     const uint32_t words = g.nops * (uint32_t)(sizeof(DOp) / 4);
     const uint32_t *src = reinterpret_cast<const uint32_t *>(A.ops + g.op_begin);
     for (uint32_t i = threadIdx.x; i < words; i += blockDim.x) reinterpret_cast<uint32_t *>(s_ops)[i] = src[i];
-    for (uint32_t o = threadIdx.x; o < g.nops; o += blockDim.x) {
-        const DOp &op = A.ops[g.op_begin + o];
-        if (op.form == F_MAT2 || op.form == F_PAIR4 || op.form == F_MATK) continue;  // formed where they are used
-        C<R> t[4];
-        op_coeffs<R, 4>(op, A.cs, A.consts, adj, t);
+    if (adj) {  // the reverse sweep's coefficients, formed once per launch by k_rev_coeffs
+        const C<R> *src = static_cast<const C<R> *>(A.rcf) + (size_t)g.op_begin * 4;
+        for (uint32_t i = threadIdx.x; i < g.nops * 4; i += blockDim.x) (&s_cf[0][0])[i] = src[i];
+    } else {
+        for (uint32_t o = threadIdx.x; o < g.nops; o += blockDim.x) {
+            const DOp &op = A.ops[g.op_begin + o];
+            if (op.form == F_MAT2 || op.form == F_PAIR4 || op.form == F_MATK) continue;  // formed where they are used
+            C<R> t[4];
+            op_coeffs<R, 4>(op, A.cs, A.consts, adj, t);
 #pragma unroll
-        for (int r = 0; r < 4; ++r) s_cf[o][r] = t[r];
-    }
-    if (adj) {  // runs of the reverse sweep: fused coefficients, formed once per segment
-        __syncthreads();
-        for (uint32_t o = threadIdx.x; o < g.nops; o += blockDim.x)
-            if (s_ops[o].run >= 2) fuse_rev_run<R>(s_ops + o, s_cf + o, s_ops[o].run);
+            for (int r = 0; r < 4; ++r) s_cf[o][r] = t[r];
+        }
     }
     __syncthreads();
     return *s_seg;
@@ -1311,6 +1312,28 @@ __device__ void run_forward(const KArgs &A, const DCirc &c, C<R> *sm, C<R> *pa, 
             store_tile<R>(pa, sm, sg, tbase, tn);
             __syncthreads();
         }
+    }
+}
+
+// The reverse sweep's coefficients of every op, once per VJP launch (after k_trig): the
+// adjoint coefficients of single ops and, for a run of single-wire gates, the fused form of
+// fuse_rev_run in the run's slots.  Two-wire dense, double-excitation and k-wire matrix steps
+// form theirs where they are used.  Kept out of k_batch, whose registers it would otherwise
+// share.
+template <typename R>
+__global__ void k_rev_coeffs(const DOp *__restrict__ ops, uint32_t nops, const double4 *__restrict__ cs,
+                             const double2 *__restrict__ consts, C<R> (*rcf)[4]) {
+    for (uint32_t o = blockIdx.x * blockDim.x + threadIdx.x; o < nops; o += gridDim.x * blockDim.x) {
+        const DOp &op = ops[o];
+        if (op.back != 0) continue;  // a run member: written by its run's head
+        if (op.form == F_MAT2 || op.form == F_PAIR4 || op.form == F_MATK) continue;
+        const int len = op.run >= 2 ? op.run : 1;
+        for (int k = 0; k < len; ++k) {
+            C<R> t[4];
+            op_coeffs<R, 4>(ops[o + k], cs, consts, true, t);
+            for (int r = 0; r < 4; ++r) rcf[o + k][r] = t[r];
+        }
+        if (len >= 2) fuse_rev_run<R>(ops + o, rcf + o, len);
     }
 }
 
@@ -1492,6 +1515,8 @@ struct Batch {
     double *d_params_in = nullptr, *d_dy_in = nullptr, *d_out = nullptr, *d_grad = nullptr;
     double *d_params_fwd = nullptr;   // parameters of the last forward
     double4 *d_cs = nullptr;          // per-parameter trigonometry
+    void *d_rcf = nullptr;            // per op: the reverse sweep's coefficients (k_rev_coeffs)
+    uint32_t nops_total = 0;
     int *d_fwd_valid = nullptr;       // pool A holds the last forward's states
     int *d_reuse = nullptr;           // per-VJP decision
     uint32_t ngslots = 0;
@@ -2057,6 +2082,8 @@ void build_program(Batch &B, const Config &cfg) {
     B.d_params_in = B.dalloc<double>(B.nparams);
     B.d_params_fwd = B.dalloc<double>(B.nparams);
     B.d_cs = B.dalloc<double4>(B.nparams);
+    B.nops_total = (uint32_t)P.ops.size();
+    B.d_rcf = B.dalloc<unsigned char>(std::max<size_t>(1, P.ops.size()) * 4 * B.amp());
     B.d_fwd_valid = B.dalloc<int>(1);
     B.d_reuse = B.dalloc<int>(1);
     B200SV_CUDA(cudaMemset(B.d_fwd_valid, 0, sizeof(int)));
@@ -2114,6 +2141,17 @@ void launch_main(Batch &B, int mode, const double *dy, double *out, const int *r
     A.pool_a = B.d_pool_a;
     A.pool_b = B.d_pool_b;
     A.reuse = reuse;
+    A.rcf = B.d_rcf;
+    if (mode == 1 && B.nops_total) {
+        const unsigned nb = std::max(1u, std::min(4096u, (B.nops_total + 255) / 256));
+        if (B.dtype == B200SV_C64)
+            k_rev_coeffs<float><<<nb, 256, 0, st>>>(B.d_ops, B.nops_total, B.d_cs, B.d_consts,
+                                                     static_cast<C<float>(*)[4]>(B.d_rcf));
+        else
+            k_rev_coeffs<double><<<nb, 256, 0, st>>>(B.d_ops, B.nops_total, B.d_cs, B.d_consts,
+                                                      static_cast<C<double>(*)[4]>(B.d_rcf));
+        B200SV_CUDA(cudaGetLastError());
+    }
     int mk = 1;
     for (auto &c : B.h_circs) mk = std::max<int>(mk, (int)c.kt);
     A.max_kt = mk;
@@ -2315,7 +2353,7 @@ int b200sv_batch_vjp(b200sv_batch_handle bh, const double *params, const double 
         run_maybe_graph(B, B.g_vjp, [&](cudaStream_t s) { enqueue_vjp(B, s); });
         if (B.nparams)
             B200SV_CUDA(cudaMemcpyAsync(grad, B.d_grad, B.nparams * sizeof(double), cudaMemcpyDeviceToDevice, st));
-        B.last_launches = 4;  // k_trig, k_params_equal, k_batch, k_grad_params
+        B.last_launches = 5;  // k_trig, k_params_equal, k_rev_coeffs, k_batch, k_grad_params
     });
 }
 
@@ -2341,7 +2379,7 @@ int b200sv_batch_jacobian(b200sv_batch_handle bh, const double *params, double *
                     B.d_gscale, B.d_gradw, nw, B.ngslots, o, B.d_gslot_circ, B.d_circs, B.d_jac_base,
                     B.d_gslot_col, B.d_circ_ncols, jac);
             B200SV_CUDA(cudaGetLastError());
-            launches += 3;
+            launches += 4;  // k_onehot_dy, k_rev_coeffs, k_batch, k_grad_scatter
         }
         B.last_launches = launches;
     });
