@@ -277,7 +277,8 @@ void apply_observable(b200sv_state *h, const ObsRec &o, const void *psi, void *o
 // per-term Pauli values of an all-Pauli observable (host vector, term order).  Words sorted by
 // X mask.  Diagonal words (two or more, 12+ qubits) share Walsh-Hadamard passes of
 // reduce_pauli_diag, up to 256 per pass.  The other words are packed, first fit in X-mask
-// order, into tiles (pauli_tile_bits): a tile holding two or more distinct X masks is one
+// order, into tiles of 12 or 13 bits (pauli_tile_bits): a tile holding two or more distinct X
+// masks is one
 // tiled pass of reduce_pauli_tiled (up to 32 words).  The rest: words whose X mask stays below
 // 4 MiB of amplitudes share passes of reduce_pauli_multi, up to 32 per pass, their partner
 // amplitudes coming from L2; each wider X mask gets pair passes of reduce_pauli_group, where a

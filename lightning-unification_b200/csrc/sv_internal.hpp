@@ -86,7 +86,7 @@ void reduce_pauli_multi(const void *psi, uint32_t nq, const PauliWord *terms, in
                         double *partials, double *out_dev, cudaStream_t st);
 // tile bits (state positions) of a tiled Pauli pass over words whose X masks OR to xunion:
 // those bits, the lowest 3 (complex128) or 4 (complex64) state bits, then the lowest others up
-// to 12 bits; 0 when they do not fit
+// to 12 (complex128) or 13 (complex64) bits; 0 when they do not fit
 uint64_t pauli_tile_bits(uint64_t xunion, uint32_t nq, size_t amp_bytes);
 // words with X factors, sorted by X mask, whose X masks fit one tile (pauli_tile_bits): one
 // read of the state for the group (<= 32 words)

@@ -625,28 +625,36 @@ void reduce_pauli_group(const void *psi, uint32_t nq, const PauliWord *terms, in
 // ---- Pauli words with wide X masks, one pass over tiles -------------------------------------
 // A word whose X mask reaches beyond the shared passes' partner distance costs one read of
 // the state as a pair pass.  A group of words whose X bits, together with the lowest state
-// bits, fit in 12 tile bits is evaluated per tile instead: a tile is the 4096 amplitudes that
-// share the values of the other bits, staged in shared memory, so the group reads the state
-// once.  Tile element r = t + 256 j is thread t's register j.
+// bits, fit in the tile bits is evaluated per tile instead: a tile is the 4096 (complex128) or
+// 8192 (complex64) amplitudes that share the values of the other bits, 64 KiB staged in shared
+// memory, so the group reads the state once.  Tile element r = t + 256 j is thread t's register j
+// (16 or 32 registers).
 //
 // For P = i^ny X^x Z^z the expectation value is sum_k Re(conj(psi_(k^x)) i^ny (-1)^(k.z) psi_k),
 // and because P is Hermitian the terms of k and k^x have equal real parts, so either member
 // of a pair may stand for it (counted twice).  A thread takes its register element as k and
 // reads the partner from shared memory, for one member of each pair:
-//  * x reaches a register bit (tile bits 8..11): the registers j whose copy of the highest such
-//    bit is 0 — the same 8 registers in every thread;
+//  * x reaches a register bit (tile bits 8 and up): the registers j whose copy of the highest
+//    such bit is 0 — the same half of the registers in every thread;
 //  * x lies in the thread bits only: registers j with (j & 1) equal to the thread's bit under
 //    the highest bit of x — a pair's two owners differ in that bit, so each pair is taken once,
-//    and every thread takes 8.
+//    and every thread takes half its registers.
 // Words sharing an X mask form runs of up to 4 that share the partner read and the products.
-constexpr int kPTileBits = 12;
+constexpr int kPTileMaxBits = 13;
 constexpr int kPTileThreads = 256;
 constexpr int kPTileMaxWords = 32;
 constexpr int kPTileLowBits[2] = {4, 3};  // state bits always in the tile: 128-byte runs (c64, c128)
+// tile shape per precision: 64 KiB of amplitudes, 8 thread bits and 4 (complex128) or 5
+// (complex64) register bits
+template <typename R> struct PTile {
+    static constexpr int bits = sizeof(R) == 4 ? 13 : 12;
+    static constexpr int per = (1 << bits) / kPTileThreads;  // registers a thread
+    static constexpr int rbits = bits - 8;
+};
 struct PauliTiledP {
     uint64_t ntiles;
     int nterms, ng, nruns;
-    uint8_t lbits[kPTileBits];          // state position of tile bit b (ascending)
+    uint8_t lbits[kPTileMaxBits];       // state position of tile bit b (ascending)
     uint8_t gbits[52];                  // state positions of the other bits (ascending)
     uint8_t run_begin[kPTileMaxWords + 1];
     uint32_t xl[kPTileMaxWords];        // tile-local X mask of each run
@@ -655,8 +663,8 @@ struct PauliTiledP {
     uint8_t ny[kPTileMaxWords];         // number of Y factors mod 4 of each word
     uint8_t run_kinds[kPTileMaxWords];  // bit 0: a word of the run has even ny, bit 1: odd
 };
-// parity of bit b of the register index j, as a 16-bit table over j
-__constant__ const uint32_t kRegParity[4] = {0xAAAAu, 0xCCCCu, 0xF0F0u, 0xFF00u};
+// parity of bit b of the register index j, as a table over the 32 registers j
+__constant__ const uint32_t kRegParity[5] = {0xAAAAAAAAu, 0xCCCCCCCCu, 0xF0F0F0F0u, 0xFF00FF00u, 0xFFFF0000u};
 __device__ __forceinline__ uint64_t deposit_bits_u8(uint64_t x, const uint8_t *pos, int nbits) {
     uint64_t r = 0;
     for (int i = 0; i < nbits; ++i) r |= ((x >> i) & 1u) << pos[i];
@@ -667,16 +675,19 @@ __device__ __forceinline__ double warp_sum(double v) {
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     return v;
 }
-// Per word, packed once per block: bits 0-7 the Z mask on the thread bits, 8-23 the parity of
-// (j & Z) over the 16 registers j as a table, bit 24 the word takes Im (odd ny), bit 25 the
-// i^ny factor is negative (ny = 1, 2).  Per run: bits 0-11 the tile-local X mask, 12-17 the
-// first word, 18-20 the number of words, 21-22 which parts its words take (bit 0 Re, bit 1 Im).
+// Per word, packed once per block: bits 0-7 the Z mask on the thread bits, bit 8 the word takes
+// Im (odd ny), bit 9 the i^ny factor is negative (ny = 1, 2); beside it the parity of (j & Z)
+// over the registers j as a 32-bit table.  Per run: bits 0-12 the tile-local X mask, 13-18 the
+// first word, 19-21 the number of words, 22-23 which parts its words take (bit 0 Re, bit 1 Im).
 __device__ __forceinline__ uint32_t tiled_word_bits(uint32_t zl, int ny) {
+    return (zl & 255u) | ((uint32_t)(ny & 1) << 8) | ((uint32_t)(ny == 1 || ny == 2) << 9);
+}
+__device__ __forceinline__ uint32_t tiled_reg_parity(uint32_t zl) {
     uint32_t m = 0;
 #pragma unroll
-    for (int b = 0; b < 4; ++b)
+    for (int b = 0; b < 5; ++b)
         if ((zl >> (8 + b)) & 1) m ^= kRegParity[b];
-    return (zl & 255u) | (m << 8) | ((uint32_t)(ny & 1) << 24) | ((uint32_t)(ny == 1 || ny == 2) << 25);
+    return m;
 }
 
 // One run of words over a tile.  NW words (1, 2 or 4; a run of 3 carries a fourth word whose
@@ -686,8 +697,10 @@ __device__ __forceinline__ uint32_t tiled_word_bits(uint32_t zl, int ny) {
 // load, the product and one signed add per word.  The run's sums go, signed, into the warp's
 // accumulators.
 template <typename R, int NW, int KIND, int TB>
-__device__ __forceinline__ void tiled_run(const C<R> *tile, const C<R> (&v)[16], int tid, uint32_t xl, int w0, int nw,
-                                          const uint32_t *s_word, uint32_t tmask, double *s_acc_warp) {
+__device__ __forceinline__ void tiled_run(const C<R> *tile, const C<R> (&v)[PTile<R>::per], int tid, uint32_t xl,
+                                          int w0, int nw, const uint32_t *s_word, const uint32_t *s_jpar,
+                                          uint32_t tmask, double *s_acc_warp) {
+    constexpr int PER = PTile<R>::per;
     uint32_t jpar[NW];
     bool im[NW];
     double sg[NW];
@@ -695,9 +708,9 @@ __device__ __forceinline__ void tiled_run(const C<R> *tile, const C<R> (&v)[16],
     for (int w = 0; w < NW; ++w) {
         const int t = w0 + (w < nw ? w : nw - 1);
         const uint32_t wb = s_word[t];
-        jpar[w] = (wb >> 8) & 0xffffu;
-        im[w] = (wb >> 24) & 1u;
-        const int odd = (__popc(tid & wb & 255u) + (tmask >> t) + (wb >> 25)) & 1;
+        jpar[w] = s_jpar[t];
+        im[w] = (wb >> 8) & 1u;
+        const int odd = (__popc(tid & wb & 255u) + (tmask >> t) + (wb >> 9)) & 1;
         sg[w] = odd ? -2.0 : 2.0;  // 2: each pair is taken once for both of its terms
     }
     double acc[2][NW];
@@ -719,9 +732,14 @@ __device__ __forceinline__ void tiled_run(const C<R> *tile, const C<R> (&v)[16],
         const uint32_t xj = xl >> 8;
         int k = 0;
 #pragma unroll
-        for (int j = 0; j < 16; ++j) {
+        for (int j = 0; j < PER; ++j) {
             if (j & (1 << TB)) continue;
-            step(widen<R>(v[j]), widen<R>(pb[((uint32_t)j ^ xj) << 8]), j, jpar, (k++) & 1);
+            // complex64 (32 registers of the tile a thread): the own element is read back from
+            // shared memory, so the tile's registers are free once it is stored
+            C<R> own;
+            if constexpr (sizeof(R) == 4) own = tile[tid + (j << 8)];
+            else own = v[j];
+            step(widen<R>(own), widen<R>(pb[((uint32_t)j ^ xj) << 8]), j, jpar, (k++) & 1);
         }
     } else {
         // registers j = 2m + hb (own element read back from shared memory); partner in the same
@@ -733,7 +751,7 @@ __device__ __forceinline__ void tiled_run(const C<R> *tile, const C<R> (&v)[16],
 #pragma unroll
         for (int w = 0; w < NW; ++w) jp[w] = jpar[w] >> hb;
 #pragma unroll
-        for (int m = 0; m < 8; ++m) step(widen<R>(po[m << 9]), widen<R>(pb[m << 9]), 2 * m, jp, m & 1);
+        for (int m = 0; m < PER / 2; ++m) step(widen<R>(po[m << 9]), widen<R>(pb[m << 9]), 2 * m, jp, m & 1);
     }
     const int lane = tid & 31;
 #pragma unroll
@@ -744,38 +762,45 @@ __device__ __forceinline__ void tiled_run(const C<R> *tile, const C<R> (&v)[16],
     }
 }
 template <typename R, int NW, int KIND>
-__device__ __forceinline__ void tiled_run_tb(int tb, const C<R> *tile, const C<R> (&v)[16], int tid, uint32_t xl,
-                                             int w0, int nw, const uint32_t *s_word, uint32_t tmask, double *acc) {
+__device__ __forceinline__ void tiled_run_tb(int tb, const C<R> *tile, const C<R> (&v)[PTile<R>::per], int tid,
+                                             uint32_t xl, int w0, int nw, const uint32_t *s_word,
+                                             const uint32_t *s_jpar, uint32_t tmask, double *acc) {
     switch (tb) {
-    case 0: tiled_run<R, NW, KIND, 0>(tile, v, tid, xl, w0, nw, s_word, tmask, acc); break;
-    case 1: tiled_run<R, NW, KIND, 1>(tile, v, tid, xl, w0, nw, s_word, tmask, acc); break;
-    case 2: tiled_run<R, NW, KIND, 2>(tile, v, tid, xl, w0, nw, s_word, tmask, acc); break;
-    case 3: tiled_run<R, NW, KIND, 3>(tile, v, tid, xl, w0, nw, s_word, tmask, acc); break;
-    default: tiled_run<R, NW, KIND, -1>(tile, v, tid, xl, w0, nw, s_word, tmask, acc); break;
+    case 0: tiled_run<R, NW, KIND, 0>(tile, v, tid, xl, w0, nw, s_word, s_jpar, tmask, acc); break;
+    case 1: tiled_run<R, NW, KIND, 1>(tile, v, tid, xl, w0, nw, s_word, s_jpar, tmask, acc); break;
+    case 2: tiled_run<R, NW, KIND, 2>(tile, v, tid, xl, w0, nw, s_word, s_jpar, tmask, acc); break;
+    case 3: tiled_run<R, NW, KIND, 3>(tile, v, tid, xl, w0, nw, s_word, s_jpar, tmask, acc); break;
+    case 4:
+        if constexpr (PTile<R>::rbits > 4) tiled_run<R, NW, KIND, 4>(tile, v, tid, xl, w0, nw, s_word, s_jpar, tmask, acc);
+        break;
+    default: tiled_run<R, NW, KIND, -1>(tile, v, tid, xl, w0, nw, s_word, s_jpar, tmask, acc); break;
     }
 }
 template <typename R>
 __global__ void __launch_bounds__(kPTileThreads, 2) k_pauli_tiled(const C<R> *__restrict__ a, PauliTiledP p,
                                                                   double *partials) {
-    constexpr int PER = (1 << kPTileBits) / kPTileThreads;  // 16 registers a thread
+    constexpr int TILE = PTile<R>::bits, PER = PTile<R>::per;
     extern __shared__ __align__(16) unsigned char pt_raw[];
     C<R> *tile = reinterpret_cast<C<R> *>(pt_raw);
-    __shared__ uint8_t s_lbits[kPTileBits], s_gbits[52];
+    __shared__ uint8_t s_lbits[kPTileMaxBits], s_gbits[52];
     __shared__ uint64_t s_hi[PER];
     __shared__ double s_acc[kPTileThreads / 32][kPTileMaxWords];
-    __shared__ uint32_t s_word[kPTileMaxWords], s_run[kPTileMaxWords];
+    __shared__ uint32_t s_word[kPTileMaxWords], s_jpar[kPTileMaxWords], s_run[kPTileMaxWords];
     __shared__ uint32_t s_tmask;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    if (tid < kPTileBits) s_lbits[tid] = p.lbits[tid];
+    if (tid < TILE) s_lbits[tid] = p.lbits[tid];
     if (tid < 52) s_gbits[tid] = p.gbits[tid];
-    if (tid < p.nterms) s_word[tid] = tiled_word_bits(p.zl[tid], p.ny[tid]);
+    if (tid < p.nterms) {
+        s_word[tid] = tiled_word_bits(p.zl[tid], p.ny[tid]);
+        s_jpar[tid] = tiled_reg_parity(p.zl[tid]);
+    }
     if (tid < p.nruns)
-        s_run[tid] = p.xl[tid] | ((uint32_t)p.run_begin[tid] << 12) |
-                     ((uint32_t)(p.run_begin[tid + 1] - p.run_begin[tid]) << 18) | ((uint32_t)p.run_kinds[tid] << 21);
+        s_run[tid] = p.xl[tid] | ((uint32_t)p.run_begin[tid] << 13) |
+                     ((uint32_t)(p.run_begin[tid + 1] - p.run_begin[tid]) << 19) | ((uint32_t)p.run_kinds[tid] << 22);
     static_assert(kPTileThreads == (kPTileThreads / 32) * kPTileMaxWords, "one accumulator per thread");
     (&s_acc[0][0])[tid] = 0.0;
     __syncthreads();
-    if (tid < PER) s_hi[tid] = deposit_bits_u8((uint64_t)tid * kPTileThreads, s_lbits, kPTileBits);
+    if (tid < PER) s_hi[tid] = deposit_bits_u8((uint64_t)tid * kPTileThreads, s_lbits, TILE);
     __syncthreads();
     const uint64_t lo = deposit_bits_u8(tid, s_lbits, 8);
     const uint64_t zg = lane < p.nterms ? p.zg[lane] : 0;
@@ -795,18 +820,18 @@ __global__ void __launch_bounds__(kPTileThreads, 2) k_pauli_tiled(const C<R> *__
         const uint32_t tmask = s_tmask;
         for (int run = 0; run < p.nruns; ++run) {
             const uint32_t rd = s_run[run];
-            const uint32_t xl = rd & 0xfffu;
-            const int w0 = (rd >> 12) & 63, nw = (rd >> 18) & 7, kinds = (rd >> 21) & 3;
+            const uint32_t xl = rd & 0x1fffu;
+            const int w0 = (rd >> 13) & 63, nw = (rd >> 19) & 7, kinds = (rd >> 22) & 3;
             const uint32_t xj = xl >> 8;
             const int tb = xj ? 31 - __clz(xj) : -1;
             double *acc = s_acc[warp];
             if (nw == 1) {
-                if (kinds == 2) tiled_run_tb<R, 1, 1>(tb, tile, v, tid, xl, w0, nw, s_word, tmask, acc);
-                else tiled_run_tb<R, 1, 0>(tb, tile, v, tid, xl, w0, nw, s_word, tmask, acc);
+                if (kinds == 2) tiled_run_tb<R, 1, 1>(tb, tile, v, tid, xl, w0, nw, s_word, s_jpar, tmask, acc);
+                else tiled_run_tb<R, 1, 0>(tb, tile, v, tid, xl, w0, nw, s_word, s_jpar, tmask, acc);
             } else if (nw == 2) {
-                tiled_run_tb<R, 2, 2>(tb, tile, v, tid, xl, w0, nw, s_word, tmask, acc);
+                tiled_run_tb<R, 2, 2>(tb, tile, v, tid, xl, w0, nw, s_word, s_jpar, tmask, acc);
             } else {
-                tiled_run_tb<R, 4, 2>(tb, tile, v, tid, xl, w0, nw, s_word, tmask, acc);
+                tiled_run_tb<R, 4, 2>(tb, tile, v, tid, xl, w0, nw, s_word, s_jpar, tmask, acc);
             }
         }
     }
@@ -821,9 +846,10 @@ __global__ void __launch_bounds__(kPTileThreads, 2) k_pauli_tiled(const C<R> *__
 
 uint64_t pauli_tile_bits(uint64_t xunion, uint32_t nq, size_t amp_bytes) {
     const int low = kPTileLowBits[amp_bytes == 16 ? 1 : 0];
+    const int tbits = amp_bytes == 16 ? PTile<double>::bits : PTile<float>::bits;
     uint64_t in = xunion | ((uint64_t(1) << std::min<uint32_t>(low, nq)) - 1);
-    if (nq < (uint32_t)kPTileBits || __builtin_popcountll(in) > kPTileBits) return 0;
-    for (uint32_t b = 0; b < nq && __builtin_popcountll(in) < kPTileBits; ++b) in |= uint64_t(1) << b;
+    if (nq < (uint32_t)tbits || __builtin_popcountll(in) > tbits) return 0;
+    for (uint32_t b = 0; b < nq && __builtin_popcountll(in) < tbits; ++b) in |= uint64_t(1) << b;
     return in;
 }
 
@@ -853,7 +879,7 @@ void reduce_pauli_tiled(const void *psi, uint32_t nq, const PauliWord *terms, in
         }
     }
     p.ng = ng;
-    p.ntiles = uint64_t(1) << (nq - kPTileBits);
+    p.ntiles = uint64_t(1) << (nq - PTile<R>::bits);
     p.nterms = nterms;
     auto local = [&](uint64_t m) {
         uint32_t r = 0;
@@ -874,7 +900,7 @@ void reduce_pauli_tiled(const void *psi, uint32_t nq, const PauliWord *terms, in
     }
     p.run_begin[nr] = (uint8_t)nterms;
     p.nruns = nr;
-    const size_t smem = sizeof(C<R>) << kPTileBits;
+    const size_t smem = sizeof(C<R>) << PTile<R>::bits;
     const uint64_t nb = std::min<uint64_t>(p.ntiles, std::min<uint64_t>((uint64_t)sm_count() * 2, kMaxRedBlocks));
     B200SV_CUDA(cudaFuncSetAttribute(k_pauli_tiled<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     k_pauli_tiled<R><<<(unsigned)nb, kPTileThreads, smem, st>>>(static_cast<const C<R> *>(psi), p, partials);

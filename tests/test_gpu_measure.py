@@ -123,7 +123,7 @@ def test_pauli_passes_near_and_far(capi, dtype):
 @pytest.mark.parametrize("dtype", [np.complex128, np.complex64])
 @pytest.mark.parametrize("n", [12, 13, 20, 22])
 def test_pauli_tiled_passes(capi, dtype, n):
-    """Words with X factors packed into tiled passes (12 tile bits: the words' X bits and the
+    """Words with X factors packed into tiled passes (12 or 13 tile bits: the words' X bits and the
     lowest state bits, one state read for up to 32 words): one-wire X/Y words on every wire,
     Jordan-Wigner strings, 8 words on one 4-wire X mask (runs of 4 sharing the partner reads),
     40 words on one mask (chunks of 32), masks whose highest bit is a thread bit, a register bit
