@@ -519,8 +519,8 @@ RX_DRAM_BYTES_26Q = 1.0738e9 + 1.0144e9
 # DRAM bytes (read + write) of the forward and VJP launches of the batched kernel on 148
 # circuits of the batched-adjoint workload, from an ncu capture of `bench.py --case batch`;
 # circuits are independent, so a step's traffic scales with the number of circuits.
-BATCH_DRAM_BYTES_148 = (0.0900e9 + 0.9940e9) + (3.0908e9 + 3.5086e9)
-BATCH_ISSUE_ACTIVE = 0.48  # scheduler cycles issuing, same capture (forward 52 %, VJP 46 %, time-weighted)
+BATCH_DRAM_BYTES_148 = (0.0397e9 + 0.9832e9) + (3.1324e9 + 3.5031e9)
+BATCH_ISSUE_ACTIVE = 0.47  # scheduler cycles issuing, same capture (forward 52 %, VJP 45 %, time-weighted)
 
 
 def run_case(args):
