@@ -134,8 +134,7 @@ __global__ void __launch_bounds__(kThreads) k_dense(States s, DenseP<R, K> p) {
                 sv[base[u] + p.off[1]] = b.get();
             }
         }
-        return;
-    }
+    } else {
     for (uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < p.ngroups;
          g += (uint64_t)gridDim.x * blockDim.x) {
         const uint64_t base = p.ins(g) | p.cmask;
@@ -169,6 +168,7 @@ __global__ void __launch_bounds__(kThreads) k_dense(States s, DenseP<R, K> p) {
             }
         }
     }
+    }
 }
 
 // A one-wire matrix on state bit 0: the pair of a group is two adjacent amplitudes, which the
@@ -194,6 +194,40 @@ __global__ void __launch_bounds__(kThreads) k_dense1_low(States s, Dense1LowP<R>
         a.set(hi ? p.m[2] : p.m[0], hi ? o : v);
         a.add(hi ? p.m[3] : p.m[1], hi ? v : o);
         sv[i] = a.get();
+    }
+}
+
+// A complex64 two-wire matrix on state bits 0 and 1 (no controls): a group's four amplitudes
+// are 32 contiguous bytes, which the group-per-thread kernel reads with four 8-byte loads at a
+// 32-byte stride across the warp.  Here each thread moves its group with two 16-byte loads and
+// stores.  Matrix row r sits at memory slot r, or with rows 1 and 2 exchanged when the first
+// target is bit 0 (SWAPMID); the sums run over the matrix columns in order, as in k_dense.
+template <typename R> struct Dense2LowP {
+    uint64_t ngroups;
+    C<R> m[16];
+};
+template <bool SWAPMID>
+__device__ __forceinline__ constexpr int slot2(int r) {
+    return SWAPMID ? (r == 1 ? 2 : r == 2 ? 1 : r) : r;
+}
+template <bool SWAPMID>
+__global__ void __launch_bounds__(kThreads) k_dense2_low(States s, Dense2LowP<float> p) {
+    float4 *__restrict__ sv = static_cast<float4 *>(s.p[blockIdx.y]);
+    for (uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < p.ngroups;
+         g += (uint64_t)gridDim.x * blockDim.x) {
+        const float4 lo = sv[2 * g], hi = sv[2 * g + 1];
+        const float2 x[4] = {make_float2(lo.x, lo.y), make_float2(lo.z, lo.w), make_float2(hi.x, hi.y),
+                             make_float2(hi.z, hi.w)};
+        float2 y[4];
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            CAcc<float> a;
+#pragma unroll
+            for (int c = 0; c < 4; ++c) cacc_term<float>(a, c, p.m[r * 4 + c], x[slot2<SWAPMID>(c)]);
+            y[slot2<SWAPMID>(r)] = a.get();
+        }
+        sv[2 * g] = make_float4(y[0].x, y[0].y, y[1].x, y[1].y);
+        sv[2 * g + 1] = make_float4(y[2].x, y[2].y, y[3].x, y[3].y);
     }
 }
 
@@ -532,6 +566,17 @@ bool launch_dense_k(const States &S, int ns, uint32_t nq, const GateDesc &g, voi
             return true;
         }
         if constexpr (K > 6) return false;
+    }
+    if constexpr (sizeof(R) == 4 && K == 2) {
+        const bool low2 = g.cbits.empty() && ((g.tbits[0] == 1 && g.tbits[1] == 0) || (g.tbits[0] == 0 && g.tbits[1] == 1));
+        if (low2) {
+            Dense2LowP<float> p{};
+            p.ngroups = ngroups;
+            for (int i = 0; i < 16; ++i) p.m[i] = cvt<float>(g.m[i]);
+            if (g.tbits[0] == 0) k_dense2_low<true><<<grid_for(ngroups, ns), kThreads, 0, st>>>(S, p);
+            else k_dense2_low<false><<<grid_for(ngroups, ns), kThreads, 0, st>>>(S, p);
+            return true;
+        }
     }
     if constexpr (K == 1) {
         if (g.cbits.empty() && g.tbits[0] == 0 && nq >= 5) {

@@ -68,6 +68,35 @@ def test_gate_every_wire_placement(capi, name):
         assert np.abs(sv.download() - want).max() < 1e-12, wires
 
 
+@pytest.mark.parametrize("n", [2, 5, 20])
+def test_c64_two_wire_dense_on_lowest_bits(capi, n):
+    """complex64 two-wire dense steps on state bits 0 and 1 (the last two wires, either order)
+    move each group with two 16-byte accesses; results against the oracle, beside the same
+    matrices on other wires and with a control added."""
+    import lq_oracle as O
+    from lightning_b200.workloads import random_unitary
+    rng = np.random.default_rng(90 + n)
+    st = random_state(rng, n, np.complex64)
+    sv = capi.StateVector(n, np.complex64)
+    placements = [[n - 2, n - 1], [n - 1, n - 2]] + ([[0, n - 1], [1, 0]] if n > 2 else [])
+    for wires in placements:
+        u = random_unitary(rng, 2)
+        sv.upload(st)
+        sv.apply_matrix(u.astype(np.complex64), wires)
+        want = O.apply_op(st.astype(np.complex128), "QubitUnitary", wires, False, [], u)
+        assert np.abs(sv.download() - want).max() < TOL[np.complex64], wires
+        for name in ("IsingXX", "IsingXY", "SingleExcitation"):
+            sv.upload(st)
+            sv.apply(name, wires, False, [0.37])
+            want = O.apply_op(st.astype(np.complex128), name, wires, False, [0.37])
+            assert np.abs(sv.download() - want).max() < TOL[np.complex64], (name, wires)
+    if n > 2:  # controlled: the general kernel
+        sv.upload(st)
+        sv.apply("CRY", [0, n - 1], False, [0.7])
+        want = O.apply_op(st.astype(np.complex128), "CRY", [0, n - 1], False, [0.7])
+        assert np.abs(sv.download() - want).max() < TOL[np.complex64]
+
+
 @pytest.mark.parametrize("n", [1, 2, 14, 21])
 def test_low_and_high_wires(capi, n):
     import lq_oracle as O
